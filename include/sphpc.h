@@ -1,0 +1,172 @@
+/*
+ * sphpc.h -- host C API of libsphpc_cuda.so, the B200 replacement for
+ * SPHPC's per-step particle pipeline.
+ *
+ * The reference keeps its particle arrays on the GPU with OpenACC data
+ * directives and calls its step functions on the "present" copies.  This
+ * library does the same with an explicit mirror: AllocInitParticles (or
+ * sphpc_enter_data) creates the device copy of a struct Particles, every
+ * step function below works on that copy, and sphpc_update_host /
+ * sphpc_update_device play the role of `#pragma acc update`.  The device
+ * copy is FP32 in cell-sorted order; the host arrays stay FP64 in the
+ * reference's original-index order.
+ *
+ * Every function returns 0 on success and a negative SPHPC_E* code on
+ * failure (the reference exits the process instead); sphpc_last_error()
+ * describes the last failure of the calling thread.  Nothing here falls
+ * back to the CPU: without a usable CUDA device every device call fails
+ * with SPHPC_ECUDA.
+ */
+#ifndef SPHPC_H_
+#define SPHPC_H_
+
+#include "sphpc_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPHPC_OK 0
+#define SPHPC_EINVAL (-1)   /* bad argument or unsupported configuration */
+#define SPHPC_EIO (-2)      /* file missing or malformed */
+#define SPHPC_ECUDA (-3)    /* CUDA runtime error / no device */
+#define SPHPC_ENOMEM (-4)   /* host or device allocation failed */
+#define SPHPC_ENOTREADY (-5)/* object not initialised (no device copy) */
+#define SPHPC_EKERNEL (-6)  /* a kernel reported an error (see message) */
+
+const char *sphpc_last_error(void);
+const char *sphpc_version(void);
+
+/* ---------------- configuration ---------------- */
+
+/* Reference values of every hard-coded constant. */
+void sphpc_default_solver(struct SphpcSolver *solver);
+/* Solver settings used by the next AllocInitParticles / sphpc_enter_data
+ * (the configuration loaders set them too). */
+void sphpc_set_default_solver(const struct SphpcSolver *solver);
+
+/* ReadParameters, input_parser.h:16-20: reads ./sim-config.ini.  The
+ * [Obstacle] section is optional here (required by the reference). */
+int ReadParameters(struct Params *parameters, struct Particles *particles,
+                   struct AABB *boundary_volume, struct AABB *initial_fluid_volume,
+                   struct Obstacle *obstacle);
+
+/* SetParameters, simulation.h:28-33 / simulation.c:130-178: ReadParameters
+ * plus particle spacing, h = 2 spacing, dq = 0.1 h and kernel norms. */
+int SetParameters(struct Params *params, struct Particles *particles,
+                  struct Neighbors *neighbors, struct AABB *boundary_global,
+                  struct AABB *water_volume_global, struct Obstacle *obstacle);
+
+/* SetParameters for an INI file at `path`, also reading the optional
+ * extension keys into `solver` (may be NULL). */
+int sphpc_load_config(const char *path, struct Params *params, struct Particles *particles,
+                      struct AABB *boundary_global, struct AABB *water_volume_global,
+                      struct Obstacle *obstacle, struct SphpcSolver *solver);
+
+/* SetParticleNumbers, geometry.h:21-24 (the communication argument of the
+ * reference is accepted and ignored: single rank). */
+int SetParticleNumbers(const struct AABB *fluid_global, struct Particles *particles,
+                       struct Params *params, void *communication);
+
+/* ConstructFluidVolume, geometry.h:16-18: cell-centred lattice plus the
+ * solver's seeded jitter; sets local_count, global_count, fluid_volume. */
+int ConstructFluidVolume(struct Particles *particles, struct Params *params,
+                         const struct AABB *fluid);
+
+/* ---------------- particles (particles.h:44-108) ---------------- */
+
+/* Host arrays (max_local each), lattice, rest state, device copy. */
+int AllocInitParticles(struct Particles *particles, struct Params *params,
+                       struct AABB *fluid_volume_initial);
+int FinalizeParticles(struct Particles *particles);
+
+/* Device copy of host arrays that were filled by the caller (acc enter data
+ * copyin); uses x, y, z, v, x_star (when non-NULL) and density. */
+int sphpc_enter_data(struct Particles *particles, const struct Params *params);
+int sphpc_exit_data(struct Particles *particles);
+int sphpc_update_host(struct Particles *particles);    /* device -> host, all fields */
+int sphpc_update_device(struct Particles *particles);  /* host -> device, all fields */
+/* Solver settings of this particle set (copied). */
+int sphpc_set_solver(struct Particles *particles, const struct SphpcSolver *solver);
+int sphpc_get_solver(const struct Particles *particles, struct SphpcSolver *solver);
+/* CUDA stream (cudaStream_t) the particle set's kernels run on. */
+int sphpc_set_stream(struct Particles *particles, void *cuda_stream);
+
+int ApplyGravity(struct Particles *fluid_particles, const struct Params *params);
+int PredictPositions(struct Particles *particles, const struct Params *params,
+                     const struct AABB *boundary_global);
+int ComputeDensities(struct Particles *fluid_particles, const struct Params *params,
+                     const struct Neighbors *neighbors);
+int ComputeLambda(struct Particles *fluid_particles, const struct Params *params,
+                  const struct Neighbors *neighbors);
+int UpdateDPs(struct Particles *fluid_particles, const struct Params *params,
+              const struct Neighbors *neighbors, const int substep);
+int UpdatePositionStars(struct Particles *particles, const struct AABB *boundary_global,
+                        const struct Obstacle *obstacle, const struct Params *params);
+int UpdateVelocities(struct Particles *fluid_particles, const struct Params *params);
+int ComputeSurfaceTension(struct Particles *particles, const struct Params *params,
+                          const struct Neighbors *neighbors);
+int ApplyViscosity(struct Particles *fluid_particles, const struct Params *params,
+                   const struct Neighbors *neighbors);
+int ComputeVorticity(struct Particles *particles, const struct Params *params,
+                     const struct Neighbors *neighbors);
+int ApplyVorticityConfinement(struct Particles *fluid_particles, const struct Params *params,
+                              const struct Neighbors *neighbors);
+int UpdatePositions(struct Particles *fluid_particles);
+
+/* ---------------- neighbours (neighbors.h:30-47) ---------------- */
+
+int AllocInitNeighbors(struct Neighbors *neighbors, const struct Particles *particles,
+                       const struct Params *params, const struct AABB *boundary_global);
+int FinalizeNeighbors(struct Neighbors *neighbors);
+/* HashParticles + SortHash + FindCellBounds + FillNeighbors on the device
+ * copy of `particles` (also reorders the device copy by cell). */
+int FindAllNeighbors(const struct Particles *particles, const struct Params *params,
+                     struct Neighbors *neighbors);
+/* The current neighbour buckets in the reference's layout and index space:
+ * indices[id*60 + j] (original indices), counts[id]. */
+int sphpc_get_neighbor_buckets(const struct Particles *particles, unsigned int *indices,
+                               int *counts);
+/* Sorted hash keys, sorted original ids (SortHash result) and the cell start
+ * table (FindLowerBounds over all cells, plus the trailing count), as the
+ * reference holds hash_values / particle_ids / start_indices. */
+int sphpc_get_cell_data(const struct Particles *particles, unsigned int *hash_values,
+                        unsigned int *particle_ids, unsigned int *start_indices);
+
+/* ---------------- obstacle (obstacle.h:32-33) ---------------- */
+
+/* Reads the SDFGen ASCII file named in obstacle->SDF_file_name
+ * (obstacle.c:13-79), fixes world_bounds' aspect ratio and uploads the SDF. */
+int AllocInitObstacle(struct Obstacle *obstacle);
+int FinalizeObstacle(struct Obstacle *obstacle);
+/* The file-reading half of AllocInitObstacle (host only, no device):
+ * fills SDF_dim_*, origin, SDF_spacing, SDF_buffer (malloc'd) and the
+ * world_bounds aspect fix. */
+int sphpc_read_sdf(struct Obstacle *obstacle);
+
+/* ---------------- whole step ---------------- */
+
+/* `steps` repetitions of the loop body of main (simulation.c:56-116):
+ * gravity, predict, neighbours, the constraint loop with SDF collisions,
+ * velocities, surface tension, XSPH viscosity, vorticity confinement,
+ * positions -- fused into the pipeline's kernels.  obstacle may be NULL. */
+int sphpc_step(struct Particles *particles, const struct Params *params,
+               struct Neighbors *neighbors, const struct AABB *boundary_global,
+               const struct Obstacle *obstacle, int steps);
+
+/* FP64 diagnostics of the device copy (density error from the last density
+ * evaluation, energy, centre of mass, momentum). */
+int sphpc_diagnostics(const struct Particles *particles, struct SphpcDiag *diag);
+/* Kernel-reported error bits since the last call (0 = none); clears them. */
+int sphpc_device_errors(const struct Particles *particles, unsigned int *bits);
+
+/* Per-kernel CUDA-event timing of the particle set's launches. */
+int sphpc_profile(struct Particles *particles, int enable);
+int sphpc_profile_read(const struct Particles *particles, struct SphpcKernelTime *out,
+                       int max_entries, int *n_entries);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,407 @@
+// grid.cu -- uniform-grid hashing, particle reorder, cell-start table and the
+// neighbour build of the PBF pipeline.
+#include "kernels.cuh"
+
+namespace sphpc {
+
+namespace {
+
+// Canonical predicted position of one particle.  predict: ApplyGravity then
+// PredictPositions (particles.c:516-527, 766-782) evaluated in FP64 exactly
+// as the reference does, then the box clamp (particles.c:842-867); the
+// displacement d = x* - x is rounded to FP32 and x* := fl64(x + d).
+__device__ __forceinline__ void canonical_xstar(const DevParams& P, const float4 x,
+                                                const float4 v, const float4 dgiven,
+                                                bool predict, float4& d, double& xs,
+                                                double& ys, double& zs) {
+  if (predict) {
+    double vx = (double)v.x, vy = (double)v.y, vz = (double)v.z;
+    if (P.gaxis == 0) vx = __dadd_rn(vx, P.gdt_d);
+    else if (P.gaxis == 1) vy = __dadd_rn(vy, P.gdt_d);
+    else vz = __dadd_rn(vz, P.gdt_d);
+    xs = __dadd_rn((double)x.x, __dmul_rn(vx, P.dt_d));
+    ys = __dadd_rn((double)x.y, __dmul_rn(vy, P.dt_d));
+    zs = __dadd_rn((double)x.z, __dmul_rn(vz, P.dt_d));
+    xs = clamp_axis(xs, P.bmin[0], P.bmax[0], P.bmax_eps[0]);
+    ys = clamp_axis(ys, P.bmin[1], P.bmax[1], P.bmax_eps[1]);
+    zs = clamp_axis(zs, P.bmin[2], P.bmax[2], P.bmax_eps[2]);
+    d = make_float4(__double2float_rn(__dsub_rn(xs, (double)x.x)),
+                    __double2float_rn(__dsub_rn(ys, (double)x.y)),
+                    __double2float_rn(__dsub_rn(zs, (double)x.z)), 0.0f);
+  } else {
+    d = dgiven;
+  }
+  xs = xstar_d(x.x, d.x);
+  ys = xstar_d(x.y, d.y);
+  zs = xstar_d(x.z, d.z);
+}
+
+__device__ __forceinline__ void grid_cell(const DevParams& P, double xs, double ys, double zs,
+                                          int& cx, int& cy, int& cz) {
+  cx = grid_coord(xs, P.hd);
+  cy = grid_coord(ys, P.hd);
+  cz = grid_coord(zs, P.hd);
+}
+
+// HashVal, neighbors.c:94-95 (unsigned arithmetic)
+__device__ __forceinline__ uint32_t cell_key(const DevParams& P, int cx, int cy, int cz) {
+  return (uint32_t)P.nx * (uint32_t)P.ny * (uint32_t)cz +
+         ((uint32_t)cy * (uint32_t)P.nx + (uint32_t)cx);
+}
+
+__device__ __forceinline__ uint32_t pack_cell(const DevParams& P, int cx, int cy, int cz) {
+  return (uint32_t)cx | ((uint32_t)cy << P.bx) | ((uint32_t)cz << (P.bx + P.by));
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_hash(const DevParams P, const float4* __restrict__ pos, const float4* __restrict__ vel,
+           const float4* __restrict__ disp, const uint32_t* __restrict__ ids,
+           uint32_t* __restrict__ keys_by_id, uint32_t* __restrict__ loc_by_id,
+           uint32_t* __restrict__ hist, int passes, int predict, uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_hist[kMaxPasses * kRadix];
+  for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) s_hist[i] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < P.n) {
+    const float4 x = __ldg(pos + i);
+    const float4 v = predict ? __ldg(vel + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 dg = predict ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(disp + i);
+    float4 d;
+    double xs, ys, zs;
+    canonical_xstar(P, x, v, dg, predict != 0, d, xs, ys, zs);
+    int cx, cy, cz;
+    grid_cell(P, xs, ys, zs, cx, cy, cz);
+    uint32_t key = cell_key(P, cx, cy, cz);
+    if (key >= P.ncells || cx >= P.nx || cy >= P.ny || cz >= P.nz) {
+      atomicOr(err, kErrCellRange);
+      key = P.ncells - 1;
+    }
+    const uint32_t id = __ldg(ids + i);
+    keys_by_id[id] = key;
+    loc_by_id[id] = (uint32_t)i;
+    count_key_digits(s_hist, key, passes);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < passes * kRadix; k += blockDim.x)
+    if (s_hist[k]) atomicAdd(hist + k, s_hist[k]);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_hash_plain(const DevParams P, const float4* __restrict__ pos,
+                 const float4* __restrict__ disp, uint32_t* __restrict__ keys) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  const float4 x = __ldg(pos + i), d = __ldg(disp + i);
+  const double xs = xstar_d(x.x, d.x), ys = xstar_d(x.y, d.y), zs = xstar_d(x.z, d.z);
+  int cx, cy, cz;
+  grid_cell(P, xs, ys, zs, cx, cy, cz);
+  keys[i] = cell_key(P, cx, cy, cz);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_reorder(const DevParams P, const uint32_t* __restrict__ sorted_ids,
+              const uint32_t* __restrict__ loc_by_id, const float4* __restrict__ pos_in,
+              const float4* __restrict__ vel_in, const float4* __restrict__ disp_in,
+              float4* __restrict__ pos_out, float4* __restrict__ vel_out,
+              float4* __restrict__ disp_out, uint32_t* __restrict__ cellp, int predict,
+              int move_vel, ReorderExtra ex) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= P.n) return;
+  const uint32_t id = __ldg(sorted_ids + j);
+  const uint32_t src = __ldg(loc_by_id + id);
+  const float4 x = __ldg(pos_in + src);
+  float4 v = (predict || move_vel) ? __ldg(vel_in + src) : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 dg = predict ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(disp_in + src);
+  float4 d;
+  double xs, ys, zs;
+  canonical_xstar(P, x, v, dg, predict != 0, d, xs, ys, zs);
+  int cx, cy, cz;
+  grid_cell(P, xs, ys, zs, cx, cy, cz);
+  cx = min(cx, P.nx - 1);
+  cy = min(cy, P.ny - 1);
+  cz = min(cz, P.nz - 1);
+  pos_out[j] = x;
+  d.w = dg.w;
+  disp_out[j] = d;
+  cellp[j] = pack_cell(P, cx, cy, cz);
+  if (move_vel) {
+    if (predict) {
+      // the velocity after ApplyGravity, as the reference holds it
+      if (P.gaxis == 0) v.x = __fadd_rn(v.x, P.gdt_f);
+      else if (P.gaxis == 1) v.y = __fadd_rn(v.y, P.gdt_f);
+      else v.z = __fadd_rn(v.z, P.gdt_f);
+    }
+    vel_out[j] = v;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+    if (ex.in4[k]) ex.out4[k][j] = __ldg(ex.in4[k] + src);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (ex.in1[k]) ex.out1[k][j] = __ldg(ex.in1[k] + src);
+}
+
+constexpr int kSmallGap = 32;
+
+// start[c] = lower_bound(keys, c): the first slot j of every non-empty key
+// writes j into the cells (key[j-1], key[j]]; long runs of empty cells go to
+// a worklist filled by k_fill_gaps.
+__global__ void __launch_bounds__(kBlock)
+    k_cell_starts(const uint32_t* __restrict__ keys, int n, uint32_t ncells,
+                  uint32_t* __restrict__ cstart, uint4* __restrict__ gaps,
+                  uint32_t* __restrict__ gap_count, uint32_t* __restrict__ err) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int64_t k = (int64_t)__ldg(keys + j);
+  const int64_t kp = j > 0 ? (int64_t)__ldg(keys + j - 1) : -1;
+  if (k >= (int64_t)ncells) {
+    atomicOr(err, kErrCellRange);
+    return;
+  }
+  if (k != kp) {
+    const int64_t lo = kp + 1, hi = k;  // inclusive
+    if (hi - lo + 1 <= kSmallGap) {
+      for (int64_t c = lo; c <= hi; ++c) cstart[c] = (uint32_t)j;
+    } else {
+      const uint32_t g = atomicAdd(gap_count, 1u);
+      gaps[g] = make_uint4((uint32_t)lo, (uint32_t)hi, (uint32_t)j, 0u);
+    }
+  }
+  if (j == n - 1) {
+    const int64_t lo = k + 1, hi = (int64_t)ncells;  // includes the sentinel cstart[C]
+    if (hi - lo + 1 <= kSmallGap) {
+      for (int64_t c = lo; c <= hi; ++c) cstart[c] = (uint32_t)n;
+    } else {
+      const uint32_t g = atomicAdd(gap_count, 1u);
+      gaps[g] = make_uint4((uint32_t)lo, (uint32_t)hi, (uint32_t)n, 0u);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_fill_gaps(const uint4* __restrict__ gaps, const uint32_t* __restrict__ gap_count,
+                uint32_t* __restrict__ cstart) {
+  const uint32_t ng = *gap_count;
+  for (uint32_t g = blockIdx.x; g < ng; g += gridDim.x) {
+    const uint4 e = gaps[g];
+    for (uint64_t c = (uint64_t)e.x + threadIdx.x; c <= (uint64_t)e.y; c += blockDim.x)
+      cstart[c] = e.z;
+  }
+}
+
+// FillNeighbors' validity test and HashVal coordinate of one shifted axis
+// value (neighbors.c:252-263).
+__device__ __forceinline__ bool shifted_coord(double x, double h, int nmax, int& g) {
+  const double f = floor(__ddiv_rn(x, h));
+  if (f > (double)(nmax - 1) || x < 0.0) return false;
+  g = (int)(unsigned)f;
+  return true;
+}
+
+__device__ __forceinline__ bool axis_regular(double x, double h, int c, int nmax) {
+  int g;
+  const bool vm = shifted_coord(__dadd_rn(x, -h), h, nmax, g);
+  const bool okm = vm ? (g == c - 1) : (c == 0);
+  const bool vp = shifted_coord(__dadd_rn(x, h), h, nmax, g);
+  const bool okp = vp ? (g == c + 1) : (c == nmax - 1);
+  return okm && okp;
+}
+
+struct BuildCtx {
+  float4 xp, dp;
+  double xs, ys, zs;
+  float h2lo, h2hi;
+  double h2d;
+};
+
+// r^2 < h^2 exactly as neighbors.c:278-285 evaluates it on the canonical
+// double positions; an FP32 estimate decides all pairs outside a narrow band
+// around h^2.
+__device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const float4* __restrict__ pos,
+                                            const float4* __restrict__ disp, int j) {
+  const float4 xq = __ldg(pos + j), dq = __ldg(disp + j);
+  const float fx = (c.xp.x - xq.x) + (c.dp.x - dq.x);
+  const float fy = (c.xp.y - xq.y) + (c.dp.y - dq.y);
+  const float fz = (c.xp.z - xq.z) + (c.dp.z - dq.z);
+  const float r2f = fx * fx + fy * fy + fz * fz;
+  if (r2f < c.h2lo) return true;
+  if (r2f > c.h2hi) return false;
+  const double ddx = __dsub_rn(c.xs, xstar_d(xq.x, dq.x));
+  const double ddy = __dsub_rn(c.ys, xstar_d(xq.y, dq.y));
+  const double ddz = __dsub_rn(c.zs, xstar_d(xq.z, dq.z));
+  const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)),
+                              __dmul_rn(ddz, ddz));
+  return r2 < c.h2d;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_build_neighbors(const DevParams P, const NbrView V, const float4* __restrict__ pos,
+                      const float4* __restrict__ disp, uint32_t* __restrict__ cellp,
+                      uint32_t* __restrict__ mask, uint32_t* __restrict__ explist,
+                      uint32_t exp_cap, uint32_t* __restrict__ exp_count,
+                      uint8_t* __restrict__ ncount, uint32_t* __restrict__ err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  BuildCtx c;
+  c.xp = __ldg(pos + p);
+  c.dp = __ldg(disp + p);
+  c.xs = xstar_d(c.xp.x, c.dp.x);
+  c.ys = xstar_d(c.xp.y, c.dp.y);
+  c.zs = xstar_d(c.xp.z, c.dp.z);
+  c.h2lo = P.h2 * (1.0f - 1.0f / 16384.0f);
+  c.h2hi = P.h2 * (1.0f + 1.0f / 16384.0f);
+  c.h2d = P.h2d;
+  const uint32_t cp = cellp[p] & ~kExplicitFlag;
+  int cx, cy, cz;
+  unpack_cell(V, cp, cx, cy, cz);
+  bool regular = axis_regular(c.xs, P.hd, cx, P.nx) && axis_regular(c.ys, P.hd, cy, P.ny) &&
+                 axis_regular(c.zs, P.hd, cz, P.nz);
+  const int xlo = cx - (cx > 0);
+  const int xhi = cx + (cx < P.nx - 1);
+  if (regular) {
+    int L = 0;
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int z = cz + dz;
+      if ((unsigned)z >= (unsigned)P.nz) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = cy + dy;
+        if ((unsigned)y >= (unsigned)P.ny) continue;
+        const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
+        L += (int)(__ldg(V.cstart + rk + xhi + 1) - __ldg(V.cstart + rk + xlo));
+      }
+    }
+    if (L > 32 * kMaskWords) regular = false;
+  }
+  int count = 0;
+  if (regular) {
+    uint32_t word = 0;
+    int wbit = 0, widx = 0;
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int z = cz + dz;
+      if ((unsigned)z >= (unsigned)P.nz) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = cy + dy;
+        if ((unsigned)y >= (unsigned)P.ny) continue;
+        const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
+        const int b = (int)__ldg(V.cstart + rk + xlo);
+        const int e = (int)__ldg(V.cstart + rk + xhi + 1);
+        for (int j = b; j < e; ++j) {
+          if (count < kMaxNeighbors && j != p && is_neighbor(c, pos, disp, j)) {
+            word |= 1u << wbit;
+            ++count;
+          }
+          if (++wbit == 32) {
+            mask[(size_t)widx * P.n + p] = word;
+            ++widx;
+            word = 0;
+            wbit = 0;
+          }
+        }
+      }
+    }
+    if (wbit > 0) mask[(size_t)widx * P.n + p] = word;
+    cellp[p] = cp;
+  } else {
+    const uint32_t idx = atomicAdd(exp_count, 1u);
+    if (idx >= exp_cap) {
+      atomicOr(err, kErrExplicitOverflow);
+      for (int w = 0; w < kMaskWords; ++w) mask[(size_t)w * P.n + p] = 0u;
+      cellp[p] = cp;
+    } else {
+      uint32_t* lst = explist + (size_t)idx * kExplicitStride;
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            int gx, gy, gz;
+            if (!shifted_coord(__dadd_rn(c.xs, (double)dx * P.hd), P.hd, P.nx, gx)) continue;
+            if (!shifted_coord(__dadd_rn(c.ys, (double)dy * P.hd), P.hd, P.ny, gy)) continue;
+            if (!shifted_coord(__dadd_rn(c.zs, (double)dz * P.hd), P.hd, P.nz, gz)) continue;
+            const uint32_t key = (uint32_t)P.nx * (uint32_t)P.ny * (uint32_t)gz +
+                                 ((uint32_t)gy * (uint32_t)P.nx + (uint32_t)gx);
+            if (key >= P.ncells) continue;
+            const int b = (int)__ldg(V.cstart + key);
+            const int e = (int)__ldg(V.cstart + key + 1);
+            for (int j = b; j < e; ++j) {
+              if (j == p) continue;
+              if (count < kMaxNeighbors && is_neighbor(c, pos, disp, j)) {
+                lst[1 + count] = (uint32_t)j;
+                ++count;
+              }
+            }
+          }
+      lst[0] = (uint32_t)count;
+      mask[p] = idx;
+      cellp[p] = cp | kExplicitFlag;
+    }
+  }
+  ncount[p] = (uint8_t)count;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_export_buckets(const NbrView V, const uint32_t* __restrict__ ids,
+                     uint32_t* __restrict__ nbr, int32_t* __restrict__ count) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= V.n) return;
+  const uint32_t idp = __ldg(ids + p);
+  uint32_t* out = nbr + (size_t)idp * kMaxNeighbors;
+  int cnt = 0;
+  for_each_neighbor(V, p, [&](int q) {
+    if (cnt < kMaxNeighbors) out[cnt] = __ldg(ids + q);
+    ++cnt;
+  });
+  for (int j = cnt; j < kMaxNeighbors; ++j) out[j] = 0u;
+  count[idp] = cnt;
+}
+
+}  // namespace
+
+void launch_hash(const DevParams& P, const float4* pos, const float4* vel, const float4* disp,
+                 const uint32_t* ids, uint32_t* keys_by_id, uint32_t* loc_by_id, uint32_t* hist,
+                 int passes, bool predict, uint32_t* err, cudaStream_t st) {
+  k_hash<<<grid_for(P.n), kBlock, 0, st>>>(P, pos, vel, disp, ids, keys_by_id, loc_by_id, hist,
+                                           passes, predict ? 1 : 0, err);
+}
+
+void launch_hash_plain(const DevParams& P, const float4* pos, const float4* disp,
+                       uint32_t* keys, cudaStream_t st) {
+  k_hash_plain<<<grid_for(P.n), kBlock, 0, st>>>(P, pos, disp, keys);
+}
+
+void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
+                    const float4* pos_in, const float4* vel_in, const float4* disp_in,
+                    float4* pos_out, float4* vel_out, float4* disp_out, uint32_t* cellp,
+                    bool predict, bool move_vel, const ReorderExtra* extra, cudaStream_t st) {
+  ReorderExtra ex = {};
+  if (extra) ex = *extra;
+  k_reorder<<<grid_for(P.n), kBlock, 0, st>>>(P, sorted_ids, loc_by_id, pos_in, vel_in,
+                                              disp_in, pos_out, vel_out, disp_out, cellp,
+                                              predict ? 1 : 0, move_vel ? 1 : 0, ex);
+}
+
+void launch_cell_starts(const uint32_t* keys_sorted, int n, uint32_t ncells, uint32_t* cstart,
+                        uint4* gaps, uint32_t* gap_count, uint32_t* err, cudaStream_t st) {
+  if (n == 0) {
+    cudaMemsetAsync(cstart, 0, sizeof(uint32_t) * ((size_t)ncells + 1), st);
+    return;
+  }
+  cudaMemsetAsync(gap_count, 0, sizeof(uint32_t), st);
+  k_cell_starts<<<grid_for(n), kBlock, 0, st>>>(keys_sorted, n, ncells, cstart, gaps,
+                                                 gap_count, err);
+  k_fill_gaps<<<148 * 4, kBlock, 0, st>>>(gaps, gap_count, cstart);
+}
+
+void launch_build_neighbors(const DevParams& P, const NbrView& V, const float4* pos,
+                            const float4* disp, uint32_t* cellp, uint32_t* mask,
+                            uint32_t* explist, uint32_t exp_cap, uint32_t* exp_count,
+                            uint8_t* ncount, uint32_t* err, cudaStream_t st) {
+  cudaMemsetAsync(exp_count, 0, sizeof(uint32_t), st);
+  k_build_neighbors<<<grid_for(P.n), kBlock, 0, st>>>(P, V, pos, disp, cellp, mask, explist,
+                                                      exp_cap, exp_count, ncount, err);
+}
+
+void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr, int32_t* count,
+                           cudaStream_t st) {
+  k_export_buckets<<<grid_for(V.n), kBlock, 0, st>>>(V, ids, nbr, count);
+}
+
+}  // namespace sphpc

@@ -1,0 +1,493 @@
+// pbf.cu -- the neighbour passes and pointwise steps of one PBF time step.
+//
+// Every pass is one thread per particle in slot (cell-sorted) order; the
+// neighbour loop visits the bucket of the particle in the reference's order
+// (for_each_neighbor).  Sums are FP32 (density with Kahan compensation);
+// the box clamp, the SDF lookup and the position update are FP64 on the
+// canonical double x* = x + d.
+#include "kernels.cuh"
+
+namespace sphpc {
+
+namespace {
+
+struct Pair {
+  float dx, dy, dz, r2;
+};
+
+// x*_p - x*_q as (x_p - x_q) + (d_p - d_q): exact in the first term for any
+// box size, so the FP32 pair geometry keeps its relative precision.
+__device__ __forceinline__ Pair pair_geom(const float4 xp, const float4 dp, const float4 xq,
+                                          const float4 dq) {
+  Pair g;
+  g.dx = (xp.x - xq.x) + (dp.x - dq.x);
+  g.dy = (xp.y - xq.y) + (dp.y - dq.y);
+  g.dz = (xp.z - xq.z) + (dp.z - dq.z);
+  g.r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
+  return g;
+}
+
+// r_mag floored at 1e-4 h (particles.c:635-637): returns r and 1/r.
+__device__ __forceinline__ void floored_r(const DevParams& P, float r2, float& r, float& rinv) {
+  const float r2c = fmaxf(r2, P.rmin * P.rmin);
+  rinv = rsqrtf(r2c);
+  r = r2c * rinv;
+}
+
+__device__ __forceinline__ void block_resid(double e, double* resid) {
+  // max and sum of the per-particle density error over the block (FP64).
+  double m = e, s = e;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+  }
+  __shared__ double sm[kBlock / 32], ss[kBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sm[warp] = m;
+    ss[warp] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double bm = 0.0, bs = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) {
+      bm = fmax(bm, sm[w]);
+      bs += ss[w];
+    }
+    atomicMax(reinterpret_cast<unsigned long long*>(resid),
+              (unsigned long long)__double_as_longlong(bm));
+    atomicAdd(resid + 1, bs);
+  }
+}
+
+template <int MODE, bool RESID>
+__global__ void __launch_bounds__(kBlock)
+    k_density_lambda(const DevParams P, const NbrView V, const PassArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  double err = 0.0;
+  if (p < P.n) {
+    const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+    float rho = P.W0m, comp = 0.0f;
+    float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
+    for_each_neighbor(V, p, [&](int q) {
+      const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), __ldg(a.disp + q));
+      if (MODE != 2) {
+        const float t = P.h2 - g.r2;
+        const float w = t > 0.0f ? P.Wn_m * t * t * t : 0.0f;
+        const float y = w - comp;
+        const float s = rho + y;
+        comp = (s - rho) - y;
+        rho = s;
+      }
+      if (MODE != 1) {
+        float r, rinv;
+        floored_r(P, g.r2, r, rinv);
+        const float hm = P.h - r;
+        const float c = hm > 0.0f ? P.DWn_m * hm * hm * rinv : 0.0f;
+        const float gx = c * g.dx, gy = c * g.dy, gz = c * g.dz;
+        sgx += gx;
+        sgy += gy;
+        sgz += gz;
+        sC += gx * gx + gy * gy + gz * gz;
+      }
+    });
+    if (MODE == 2) rho = a.rho[p];
+    if (MODE != 2) a.rho[p] = rho;
+    if (MODE != 1) {
+      const float C = fmaxf(__fdiv_rn(rho, P.rho0) - 1.0f, 0.0f);
+      sC += sgx * sgx + sgy * sgy + sgz * sgz;
+      sC *= P.inv_rho0_sq;
+      const float lam = -C / (sC + P.lambda_eps);
+      a.disp_out[p] = make_float4(dp.x, dp.y, dp.z, lam);
+      if (a.lam) a.lam[p] = lam;
+    }
+    if (RESID) err = fmax((double)rho / (double)P.rho0 - 1.0, 0.0);
+  }
+  if (RESID) block_resid(err, a.resid);
+}
+
+template <int MODE, int SCORR_N, bool SDF>
+__global__ void __launch_bounds__(kBlock)
+    k_position(const DevParams P, const NbrView V, const PassArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  const float lp = dp.w;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  for_each_neighbor(V, p, [&](int q) {
+    const float4 dq = __ldg(a.disp + q);
+    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), dq);
+    float r, rinv;
+    floored_r(P, g.r2, r, rinv);
+    const float hm = P.h - r;
+    const float delW = hm > 0.0f ? P.DWn_m * hm * hm : 0.0f;
+    float sc = 0.0f;
+    if (SCORR_N != 0) {
+      const float t = P.h2 - r * r;
+      const float w = t > 0.0f ? P.Wn * t * t * t : 0.0f;
+      const float ratio = w * P.inv_Wdq;
+      if (SCORR_N == 4) {
+        const float r2_ = ratio * ratio;
+        sc = -P.scorr_k * (r2_ * r2_);
+      } else {
+        sc = -P.scorr_k;
+        for (int e = 0; e < P.scorr_n; ++e) sc *= ratio;
+      }
+    }
+    const float c = (lp + dq.w + sc) * delW * rinv;
+    ax += c * g.dx;
+    ay += c * g.dy;
+    az += c * g.dz;
+  });
+  const float s = a.stiffness * P.inv_rho0;
+  const float dpx = ax * s, dpy = ay * s, dpz = az * s;
+  if (MODE == 1) {
+    a.dp[p] = make_float4(dpx, dpy, dpz, 0.0f);
+    return;
+  }
+  double xs = __dadd_rn(xstar_d(xp.x, dp.x), (double)dpx);
+  double ys = __dadd_rn(xstar_d(xp.y, dp.y), (double)dpy);
+  double zs = __dadd_rn(xstar_d(xp.z, dp.z), (double)dpz);
+  xs = clamp_axis(xs, P.bmin[0], P.bmax[0], P.bmax_eps[0]);
+  ys = clamp_axis(ys, P.bmin[1], P.bmax[1], P.bmax_eps[1]);
+  zs = clamp_axis(zs, P.bmin[2], P.bmax[2], P.bmax_eps[2]);
+  if (SDF) sdf_collide(P, xs, ys, zs);
+  const double ex = __dsub_rn(xs, (double)xp.x), ey = __dsub_rn(ys, (double)xp.y),
+               ez = __dsub_rn(zs, (double)xp.z);
+  a.disp_out[p] = make_float4(__double2float_rn(ex), __double2float_rn(ey),
+                              __double2float_rn(ez), a.rho[p]);
+  if (a.last) {
+    // UpdateVelocities, particles.c:814-837
+    float vx = __double2float_rn(__ddiv_rn(ex, P.dt_d));
+    float vy = __double2float_rn(__ddiv_rn(ey, P.dt_d));
+    float vz = __double2float_rn(__ddiv_rn(ez, P.dt_d));
+    vx = fminf(fmaxf(vx, -P.v_max), P.v_max);
+    vy = fminf(fmaxf(vy, -P.v_max), P.v_max);
+    vz = fminf(fmaxf(vz, -P.v_max), P.v_max);
+    a.vel_out[p] = make_float4(vx, vy, vz, 0.0f);
+  }
+}
+
+template <bool SDF>
+__global__ void __launch_bounds__(kBlock) k_apply_dp(const DevParams P, const PassArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 xp = __ldg(a.pos + p), dp = a.disp_out[p], dd = __ldg(a.dp + p);
+  double xs = __dadd_rn(xstar_d(xp.x, dp.x), (double)dd.x);
+  double ys = __dadd_rn(xstar_d(xp.y, dp.y), (double)dd.y);
+  double zs = __dadd_rn(xstar_d(xp.z, dp.z), (double)dd.z);
+  xs = clamp_axis(xs, P.bmin[0], P.bmax[0], P.bmax_eps[0]);
+  ys = clamp_axis(ys, P.bmin[1], P.bmax[1], P.bmax_eps[1]);
+  zs = clamp_axis(zs, P.bmin[2], P.bmax[2], P.bmax_eps[2]);
+  if (SDF) sdf_collide(P, xs, ys, zs);
+  a.disp_out[p] = make_float4(__double2float_rn(__dsub_rn(xs, (double)xp.x)),
+                              __double2float_rn(__dsub_rn(ys, (double)xp.y)),
+                              __double2float_rn(__dsub_rn(zs, (double)xp.z)), dp.w);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_color(const DevParams P, const NbrView V, const PassArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  float cx = 0.f, cy = 0.f, cz = 0.f;
+  for_each_neighbor(V, p, [&](int q) {
+    const float4 dq = __ldg(a.disp + q);
+    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), dq);
+    float r, rinv;
+    floored_r(P, g.r2, r, rinv);
+    const float t = P.h2 - r * r;
+    const float grad = t > 0.0f ? P.DWPn * t * t * r : 0.0f;
+    const float c = grad * P.m / dq.w * rinv;
+    cx += c * g.dx;
+    cy += c * g.dy;
+    cz += c * g.dz;
+  });
+  a.color[p] = make_float4(P.h * cx, P.h * cy, P.h * cz, 0.0f);
+}
+
+__device__ __forceinline__ float cohesion(const DevParams& P, float r) {
+  // Akinci cohesion spline, particles.c:54-65
+  const float hr = P.h - r;
+  float c;
+  if (r > P.h)
+    c = 0.0f;
+  else if (r <= 0.5f * P.h) {
+    const float h3 = P.h * P.h * P.h;
+    c = 2.0f * hr * hr * hr * r * r * r - h3 * h3 * (1.0f / 64.0f);
+  } else
+    c = hr * hr * hr * r * r * r;
+  return P.C_norm * c;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_tension(const DevParams P, const NbrView V, const PassArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  const float4 cp = __ldg(a.color + p);
+  const float rp = dp.w;
+  const float kcoh = -20.0f * P.gamma * P.m * P.m;
+  const float kcur = -P.gamma * P.m;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  for_each_neighbor(V, p, [&](int q) {
+    const float4 dq = __ldg(a.disp + q);
+    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), dq);
+    float r, rinv;
+    floored_r(P, g.r2, r, rinv);
+    const float4 cq = __ldg(a.color + q);
+    const float coh = kcoh * cohesion(P, r) * rinv;
+    const float K = 2.0f * P.rho0 / (rp + dq.w);
+    fx += K * (coh * g.dx + kcur * (cp.x - cq.x));
+    fy += K * (coh * g.dy + kcur * (cp.y - cq.y));
+    fz += K * (coh * g.dz + kcur * (cp.z - cq.z));
+  });
+  float4 v = a.vel[p];
+  const float s = P.dt / rp;
+  v.x += s * fx;
+  v.y += s * fy;
+  v.z += s * fz;
+  a.vel[p] = v;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_xsph(const DevParams P, const NbrView V, const PassArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  const float4 vp = __ldg(a.vel + p);
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+  for_each_neighbor(V, p, [&](int q) {
+    const float4 dq = __ldg(a.disp + q);
+    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), dq);
+    // particles.c:439 evaluates x^2 + y^2 * z^2 (kept unless xsph_exact)
+    const float rr = P.xsph_exact ? g.r2 : g.dx * g.dx + g.dy * g.dy * g.dz * g.dz;
+    const float t = P.h2 - rr;
+    const float w = t > 0.0f ? P.Wn_m * t * t * t / dq.w : 0.0f;
+    const float4 vq = __ldg(a.vel + q);
+    sx += (vq.x - vp.x) * w;
+    sy += (vq.y - vp.y) * w;
+    sz += (vq.z - vp.z) * w;
+  });
+  a.vel_out[p] = make_float4(vp.x + P.c_xsph * sx, vp.y + P.c_xsph * sy,
+                             vp.z + P.c_xsph * sz, 0.0f);
+  if (a.write_pos)
+    a.pos_out[p] = make_float4(__double2float_rn(xstar_d(xp.x, dp.x)),
+                               __double2float_rn(xstar_d(xp.y, dp.y)),
+                               __double2float_rn(xstar_d(xp.z, dp.z)), 0.0f);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_vorticity(const DevParams P, const NbrView V, const PassArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  const float4 vp = __ldg(a.vel + p);
+  float wx = 0.f, wy = 0.f, wz = 0.f;
+  for_each_neighbor(V, p, [&](int q) {
+    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), __ldg(a.disp + q));
+    float r, rinv;
+    floored_r(P, g.r2, r, rinv);
+    const float hm = P.h - r;
+    const float c = hm > 0.0f ? P.DWn * hm * hm * rinv : 0.0f;
+    const float gx = c * g.dx, gy = c * g.dy, gz = c * g.dz;
+    const float4 vq = __ldg(a.vel + q);
+    const float ux = vq.x - vp.x, uy = vq.y - vp.y, uz = vq.z - vp.z;
+    wx += uy * gz - uz * gy;
+    wy += uz * gx - ux * gz;
+    wz += ux * gy - uy * gx;
+  });
+  a.omega[p] = make_float4(wx, wy, wz, sqrtf(wx * wx + wy * wy + wz * wz));
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_confinement(const DevParams P, const NbrView V, const PassArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  float ex = 0.f, ey = 0.f, ez = 0.f;
+  for_each_neighbor(V, p, [&](int q) {
+    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), __ldg(a.disp + q));
+    float r, rinv;
+    floored_r(P, g.r2, r, rinv);
+    const float hm = P.h - r;
+    const float wq = __ldg(a.omega + q).w;
+    const float c = hm > 0.0f ? P.DWn * hm * hm * rinv * wq : 0.0f;
+    ex += c * g.dx;
+    ey += c * g.dy;
+    ez += c * g.dz;
+  });
+  const float em = fmaxf(sqrtf(ex * ex + ey * ey + ez * ez), P.rmin);
+  const float nx = ex / em, ny = ey / em, nz = ez / em;
+  const float4 w = __ldg(a.omega + p);
+  const float s = P.dt * P.vort_eps / P.m;
+  float4 v = a.vel[p];
+  v.x += s * (ny * w.z - nz * w.y);
+  v.y += s * (nz * w.x - nx * w.z);
+  v.z += s * (nx * w.y - ny * w.x);
+  a.vel[p] = v;
+  if (a.write_pos)
+    a.pos_out[p] = make_float4(__double2float_rn(xstar_d(xp.x, dp.x)),
+                               __double2float_rn(xstar_d(xp.y, dp.y)),
+                               __double2float_rn(xstar_d(xp.z, dp.z)), 0.0f);
+}
+
+__global__ void __launch_bounds__(kBlock) k_gravity(const DevParams P, float4* vel) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  float4 v = vel[p];
+  if (P.gaxis == 0) v.x = __fadd_rn(v.x, P.gdt_f);
+  else if (P.gaxis == 1) v.y = __fadd_rn(v.y, P.gdt_f);
+  else v.z = __fadd_rn(v.z, P.gdt_f);
+  vel[p] = v;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_predict(const DevParams P, const float4* __restrict__ pos, const float4* __restrict__ vel,
+              float4* __restrict__ disp) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 x = pos[p], v = vel[p];
+  double xs = __dadd_rn((double)x.x, __dmul_rn((double)v.x, P.dt_d));
+  double ys = __dadd_rn((double)x.y, __dmul_rn((double)v.y, P.dt_d));
+  double zs = __dadd_rn((double)x.z, __dmul_rn((double)v.z, P.dt_d));
+  xs = clamp_axis(xs, P.bmin[0], P.bmax[0], P.bmax_eps[0]);
+  ys = clamp_axis(ys, P.bmin[1], P.bmax[1], P.bmax_eps[1]);
+  zs = clamp_axis(zs, P.bmin[2], P.bmax[2], P.bmax_eps[2]);
+  const float w = disp[p].w;
+  disp[p] = make_float4(__double2float_rn(__dsub_rn(xs, (double)x.x)),
+                        __double2float_rn(__dsub_rn(ys, (double)x.y)),
+                        __double2float_rn(__dsub_rn(zs, (double)x.z)), w);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_update_velocities(const DevParams P, const float4* __restrict__ disp,
+                        float4* __restrict__ vel) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 d = disp[p];
+  float vx = __double2float_rn(__ddiv_rn((double)d.x, P.dt_d));
+  float vy = __double2float_rn(__ddiv_rn((double)d.y, P.dt_d));
+  float vz = __double2float_rn(__ddiv_rn((double)d.z, P.dt_d));
+  vx = fminf(fmaxf(vx, -P.v_max), P.v_max);
+  vy = fminf(fmaxf(vy, -P.v_max), P.v_max);
+  vz = fminf(fmaxf(vz, -P.v_max), P.v_max);
+  vel[p] = make_float4(vx, vy, vz, 0.0f);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_update_positions(const DevParams P, const float4* __restrict__ pos, float4* disp,
+                       float4* pos_out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 x = pos[p];
+  const float4 d = disp[p];
+  const float nx = __double2float_rn(xstar_d(x.x, d.x));
+  const float ny = __double2float_rn(xstar_d(x.y, d.y));
+  const float nz = __double2float_rn(xstar_d(x.z, d.z));
+  pos_out[p] = make_float4(nx, ny, nz, 0.0f);
+  // keep x* unchanged: d' = x* - x_new (exactly representable residue)
+  disp[p] = make_float4(__double2float_rn(__dsub_rn(xstar_d(x.x, d.x), (double)nx)),
+                        __double2float_rn(__dsub_rn(xstar_d(x.y, d.y), (double)ny)),
+                        __double2float_rn(__dsub_rn(xstar_d(x.z, d.z), (double)nz)), d.w);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_pack_w(const DevParams P, float4* disp, const float* __restrict__ src) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  reinterpret_cast<float*>(disp)[4 * (size_t)p + 3] = src[p];
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_collisions_double(const DevParams P, double* x, double* y, double* z, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a = x[i], b = y[i], c = z[i];
+  if (sdf_collide(P, a, b, c)) {
+    x[i] = a;
+    y[i] = b;
+    z[i] = c;
+  }
+}
+
+}  // namespace
+
+void launch_density_lambda(const DevParams& P, const NbrView& V, const PassArgs& a, int mode,
+                           bool residual, cudaStream_t st) {
+  const int g = grid_for(P.n);
+  if (mode == 0) {
+    if (residual) k_density_lambda<0, true><<<g, kBlock, 0, st>>>(P, V, a);
+    else k_density_lambda<0, false><<<g, kBlock, 0, st>>>(P, V, a);
+  } else if (mode == 1) {
+    if (residual) k_density_lambda<1, true><<<g, kBlock, 0, st>>>(P, V, a);
+    else k_density_lambda<1, false><<<g, kBlock, 0, st>>>(P, V, a);
+  } else {
+    k_density_lambda<2, false><<<g, kBlock, 0, st>>>(P, V, a);
+  }
+}
+
+void launch_position(const DevParams& P, const NbrView& V, const PassArgs& a, int mode,
+                     cudaStream_t st) {
+  const int g = grid_for(P.n);
+  const int sn = P.scorr_k != 0.0f ? (P.scorr_n == 4 ? 4 : -1) : 0;
+  const bool sdf = P.has_sdf != 0;
+#define SPHPC_POS(M, N, S) k_position<M, N, S><<<g, kBlock, 0, st>>>(P, V, a)
+  if (mode == 0) {
+    if (sn == 0) { if (sdf) SPHPC_POS(0, 0, true); else SPHPC_POS(0, 0, false); }
+    else if (sn == 4) { if (sdf) SPHPC_POS(0, 4, true); else SPHPC_POS(0, 4, false); }
+    else { if (sdf) SPHPC_POS(0, -1, true); else SPHPC_POS(0, -1, false); }
+  } else {
+    if (sn == 0) SPHPC_POS(1, 0, false);
+    else if (sn == 4) SPHPC_POS(1, 4, false);
+    else SPHPC_POS(1, -1, false);
+  }
+#undef SPHPC_POS
+}
+
+void launch_apply_dp(const DevParams& P, const PassArgs& a, cudaStream_t st) {
+  if (P.has_sdf) k_apply_dp<true><<<grid_for(P.n), kBlock, 0, st>>>(P, a);
+  else k_apply_dp<false><<<grid_for(P.n), kBlock, 0, st>>>(P, a);
+}
+
+void launch_color(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
+  k_color<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
+}
+void launch_tension(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
+  k_tension<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
+}
+void launch_xsph(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
+  k_xsph<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
+}
+void launch_vorticity(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
+  k_vorticity<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
+}
+void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a,
+                        cudaStream_t st) {
+  k_confinement<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
+}
+void launch_gravity(const DevParams& P, float4* vel, cudaStream_t st) {
+  k_gravity<<<grid_for(P.n), kBlock, 0, st>>>(P, vel);
+}
+void launch_predict(const DevParams& P, const float4* pos, const float4* vel, float4* disp,
+                    cudaStream_t st) {
+  k_predict<<<grid_for(P.n), kBlock, 0, st>>>(P, pos, vel, disp);
+}
+void launch_update_velocities(const DevParams& P, const float4* disp, float4* vel,
+                              cudaStream_t st) {
+  k_update_velocities<<<grid_for(P.n), kBlock, 0, st>>>(P, disp, vel);
+}
+void launch_update_positions(const DevParams& P, const float4* pos, float4* disp,
+                             float4* pos_out, cudaStream_t st) {
+  k_update_positions<<<grid_for(P.n), kBlock, 0, st>>>(P, pos, disp, pos_out);
+}
+void launch_pack_w(const DevParams& P, float4* disp, const float* src, cudaStream_t st) {
+  k_pack_w<<<grid_for(P.n), kBlock, 0, st>>>(P, disp, src);
+}
+void launch_collisions_double(const DevParams& P, double* x, double* y, double* z, int n,
+                              cudaStream_t st) {
+  k_collisions_double<<<grid_for(n), kBlock, 0, st>>>(P, x, y, z, n);
+}
+
+}  // namespace sphpc

@@ -1,0 +1,285 @@
+// radix_sort.cu -- onesweep LSD radix sort and the cell-bounds seam kernels.
+#include "radix_sort.cuh"
+
+namespace sphpc {
+
+namespace {
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
+__device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) {
+  asm volatile("st.volatile.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__global__ void __launch_bounds__(256) k_digit_histogram(const uint32_t* __restrict__ keys,
+                                                         int n, int passes,
+                                                         uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_hist[kMaxPasses * kRadix];
+  for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) s_hist[i] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    count_key_digits(s_hist, __ldg(keys + i), passes);
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x)
+    if (s_hist[i]) atomicAdd(hist + i, s_hist[i]);
+}
+
+// Exclusive scan of each pass's 256 digit counts (one block, 256 threads).
+__global__ void __launch_bounds__(256) k_scan_digits(uint32_t* __restrict__ hist, int passes) {
+  __shared__ uint32_t s_warp[kRadix / 32];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int p = 0; p < passes; ++p) {
+    const uint32_t v = hist[p * kRadix + t];
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    uint32_t wsum = 0;
+    for (int w = 0; w < warp; ++w) wsum += s_warp[w];
+    hist[p * kRadix + t] = wsum + x - v;
+    __syncthreads();
+  }
+}
+
+// One digit pass.  vals_in == nullptr means the values are the input
+// indices (iota), which is how SortHash calls SortByKey (neighbors.c:123).
+__global__ void __launch_bounds__(kSortThreads)
+    k_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+               uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n,
+               int shift, const uint32_t* __restrict__ digit_offset,
+               uint32_t* __restrict__ lookback, uint32_t* __restrict__ tile_counter,
+               uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_whist[kSortWarps][kRadix + 1];
+  __shared__ uint32_t s_dstart[kRadix];
+  __shared__ uint32_t s_gbase[kRadix];
+  __shared__ uint32_t s_wsum[kRadix / 32];
+  __shared__ uint32_t s_keys[kSortTile];
+  __shared__ uint32_t s_vals[kSortTile];
+
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) s_tile = atomicAdd(tile_counter, 1u);
+  for (int i = t; i < kSortWarps * (kRadix + 1); i += kSortThreads)
+    (&s_whist[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const int64_t tile_base = (int64_t)tile * kSortTile;
+  const int64_t wbase = tile_base + (int64_t)warp * 32 * kSortItems;
+
+  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const int64_t idx = wbase + i * 32 + lane;
+    if (idx < n) {
+      key[i] = __ldg(keys_in + idx);
+      val[i] = vals_in ? __ldg(vals_in + idx) : (uint32_t)idx;
+    } else {
+      key[i] = 0xffffffffu;
+      val[i] = 0;
+    }
+  }
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const int64_t idx = wbase + i * 32 + lane;
+    const uint32_t d = idx < n ? ((key[i] >> shift) & (kRadix - 1)) : (uint32_t)kRadix;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const int leader = __ffs(peers) - 1;
+    uint32_t prev = 0;
+    if (lane == leader) {
+      prev = s_whist[warp][d];
+      s_whist[warp][d] = prev + __popc(peers);
+    }
+    prev = __shfl_sync(0xffffffffu, prev, leader);
+    rank[i] = prev + __popc(peers & lt);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Per digit: exclusive prefix over warps, the tile count, look-back.
+  {
+    const int d = t;  // kSortThreads == kRadix
+    uint32_t sum = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = s_whist[w][d];
+      s_whist[w][d] = sum;
+      sum += c;
+    }
+    const uint32_t cnt = sum;
+    uint32_t* my = lookback + (size_t)tile * kRadix + d;
+    if (tile == 0) {
+      st_volatile(my, kLbInc | cnt);
+    } else {
+      st_volatile(my, kLbAgg | cnt);
+    }
+    uint32_t excl = 0;
+    if (tile > 0) {
+      int64_t pt = (int64_t)tile - 1;
+      while (pt >= 0) {
+        const uint32_t* f = lookback + (size_t)pt * kRadix + d;
+        uint32_t v = ld_volatile(f);
+        int spins = 0;
+        while ((v & (kLbAgg | kLbInc)) == 0) {
+          if (++spins > kSpinLimit) {
+            atomicOr(err, 2u);  // kErrSortSpin
+            v = kLbInc;
+            break;
+          }
+          __nanosleep(32);
+          v = ld_volatile(f);
+        }
+        excl += v & kLbValue;
+        if (v & kLbInc) break;
+        --pt;
+      }
+      st_volatile(my, kLbInc | (excl + cnt));
+    }
+    s_gbase[d] = __ldg(digit_offset + d) + excl;
+    // tile-local exclusive scan of cnt over digits
+    uint32_t x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_wsum[warp] = x;
+    __syncthreads();
+    uint32_t wsum = 0;
+    for (int w = 0; w < warp; ++w) wsum += s_wsum[w];
+    s_dstart[d] = wsum + x - cnt;
+  }
+  __syncthreads();
+
+  // Stage the tile in digit order.
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const int64_t idx = wbase + i * 32 + lane;
+    if (idx < n) {
+      const uint32_t d = (key[i] >> shift) & (kRadix - 1);
+      const uint32_t lp = s_dstart[d] + s_whist[warp][d] + rank[i];
+      s_keys[lp] = key[i];
+      s_vals[lp] = val[i];
+    }
+  }
+  __syncthreads();
+  const int valid = (int)min((int64_t)kSortTile, (int64_t)n - tile_base);
+  for (int k = t; k < valid; k += kSortThreads) {
+    const uint32_t kk = s_keys[k];
+    const uint32_t d = (kk >> shift) & (kRadix - 1);
+    const uint32_t g = s_gbase[d] + (uint32_t)k - s_dstart[d];
+    keys_out[g] = kk;
+    vals_out[g] = s_vals[k];
+  }
+}
+
+__global__ void k_bounds(const uint32_t* __restrict__ keys, int n, int count,
+                         uint32_t* __restrict__ out, int upper) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < count;
+       c += gridDim.x * blockDim.x) {
+    int lo = 0, hi = n;
+    const uint32_t v = (uint32_t)c;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      const uint32_t k = __ldg(keys + mid);
+      const bool go_right = upper ? (k <= v) : (k < v);
+      if (go_right) lo = mid + 1; else hi = mid;
+    }
+    out[c] = (uint32_t)lo;
+  }
+}
+
+}  // namespace
+
+void launch_digit_histogram(const uint32_t* keys, int n, int passes, uint32_t* hist,
+                            cudaStream_t stream) {
+  if (n <= 0) return;
+  int blocks = (n + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_digit_histogram<<<blocks, 256, 0, stream>>>(keys, n, passes, hist);
+}
+
+cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, int n, int passes,
+                             const SortScratch& s, cudaStream_t stream, bool hist_ready,
+                             bool vals_iota, bool copy_back, uint32_t** keys_res,
+                             uint32_t** vals_res) {
+  if (passes < 1 || passes > kMaxPasses) return cudaErrorInvalidValue;
+  if (n < 0 || (uint64_t)n > kLbValue || vals == nullptr) return cudaErrorInvalidValue;
+  cudaError_t e;
+  if (n <= 1) {
+    if (n == 1 && vals_iota) {
+      e = cudaMemsetAsync(vals, 0, sizeof(uint32_t), stream);
+      if (e != cudaSuccess) return e;
+    }
+    if (keys_res) *keys_res = keys;
+    if (vals_res) *vals_res = vals;
+    return cudaSuccess;
+  }
+  const int tiles = sort_tiles(n);
+  if (!hist_ready) {
+    e = cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * kMaxPasses * kRadix, stream);
+    if (e != cudaSuccess) return e;
+    launch_digit_histogram(keys, n, passes, s.hist, stream);
+  }
+  e = cudaMemsetAsync(s.lookback, 0, sizeof(uint32_t) * (size_t)passes * tiles * kRadix,
+                      stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(s.counters, 0, sizeof(uint32_t) * kMaxPasses, stream);
+  if (e != cudaSuccess) return e;
+  k_scan_digits<<<1, kRadix, 0, stream>>>(s.hist, passes);
+  // Pass p reads the previous output and writes buffer set (p & 1):
+  // set 0 = scratch alternates, set 1 = the caller's arrays.
+  uint32_t* const bk[2] = {s.keys_alt, keys};
+  uint32_t* const bv[2] = {s.vals_alt, vals};
+  const uint32_t* kin = keys;
+  const uint32_t* vin = vals_iota ? nullptr : vals;
+  for (int p = 0; p < passes; ++p) {
+    uint32_t* kout = bk[p & 1];
+    uint32_t* vout = bv[p & 1];
+    k_onesweep<<<tiles, kSortThreads, 0, stream>>>(
+        kin, vin, kout, vout, n, p * kRadixBits, s.hist + p * kRadix,
+        s.lookback + (size_t)p * tiles * kRadix, s.counters + p, s.err);
+    kin = kout;
+    vin = vout;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  uint32_t* kres = const_cast<uint32_t*>(kin);
+  uint32_t* vres = const_cast<uint32_t*>(vin);
+  if (copy_back && kres != keys) {
+    e = cudaMemcpyAsync(keys, kres, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(vals, vres, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, stream);
+    if (e != cudaSuccess) return e;
+    kres = keys;
+    vres = vals;
+  }
+  if (keys_res) *keys_res = kres;
+  if (vals_res) *vals_res = vres;
+  return cudaSuccess;
+}
+
+cudaError_t launch_bounds(const uint32_t* keys, int n, int count, uint32_t* out, bool upper,
+                          cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  int blocks = (count + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_bounds<<<blocks, 256, 0, stream>>>(keys, n, count, out, upper ? 1 : 0);
+  return cudaGetLastError();
+}
+
+}  // namespace sphpc

@@ -1,0 +1,1326 @@
+// sim.cu -- device copy of a particle set and the C ABI of the pipeline.
+//
+// A DeviceSim is the device mirror of one struct Particles (the reference
+// keeps the same arrays resident with OpenACC `enter data`,
+// particles.c:1056-1078).  Its kernels run on one stream; the reference-named
+// step functions launch one stage each, sphpc_step launches the fused step.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+#include "host_internal.h"
+#include "kernels.cuh"
+#include "mlp.cuh"
+#include "../../include/sphpc_device.h"
+
+struct Obstacle_CUDA {
+  float* sdf;
+  size_t count;
+};
+
+namespace sphpc {
+
+#define SPHPC_CK(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return set_error(SPHPC_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                       __FILE__, __LINE__);                                             \
+  } while (0)
+
+#define SPHPC_RC(expr)      \
+  do {                      \
+    const int rc_ = (expr); \
+    if (rc_) return rc_;    \
+  } while (0)
+
+template <class T>
+static int dalloc(T** p, size_t n) {
+  if (n == 0) n = 1;
+  const cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_error(SPHPC_ENOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T),
+                     cudaGetErrorString(e));
+  }
+  return SPHPC_OK;
+}
+
+template <class T>
+static void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+static int bits_for(uint32_t v) {  // bits needed to hold values 0..v
+  int b = 0;
+  while (b < 32 && (v >> b) != 0) ++b;
+  return b > 0 ? b : 1;
+}
+
+class DeviceSim {
+ public:
+  int n = 0;
+  SphpcSolver solver{};
+  cudaStream_t stream = nullptr;
+  double rho0 = 1000.0, mass = 1.0;
+  int device = 0;
+
+  // grid
+  bool grid_ready = false;
+  int nx = 0, ny = 0, nz = 0;
+  uint32_t C = 0;
+  int bx = 0, by = 0, passes = 1;
+
+  // per-particle arrays, slot order
+  float4 *pos = nullptr, *pos_alt = nullptr, *disp = nullptr, *disp_alt = nullptr;
+  float4 *vel = nullptr, *vel_alt = nullptr, *color = nullptr, *omega = nullptr, *dp = nullptr;
+  float *rho = nullptr, *lam = nullptr;
+  // alternates for the full reorder of the per-function path
+  float4 *color_alt = nullptr, *omega_alt = nullptr, *dp_alt = nullptr;
+  float *rho_alt = nullptr, *lam_alt = nullptr;
+  uint32_t *ids = nullptr, *ids_spare = nullptr, *keys_by_id = nullptr, *loc_by_id = nullptr;
+  uint32_t* keys_sorted = nullptr;  // view into keys_by_id or sort.keys_alt
+  uint32_t *cellp = nullptr, *mask = nullptr, *explist = nullptr, *cstart = nullptr;
+  uint8_t* ncount = nullptr;
+  uint4* gaps = nullptr;
+  uint32_t* small = nullptr;  // [0] gap count, [1] explicit count, [2] error bits
+  double* resid = nullptr;    // [0] max (bits), [1] sum, [2..] diagnostics
+  uint32_t exp_cap = 0;
+  SortScratch sort{};
+  uint32_t* sort_aux = nullptr;
+  double* stage = nullptr;  // 20 * n doubles for host transfers
+  bool nbr_valid = false;
+  bool disp_zero_pending = false;
+
+  MlpState mlp{};
+
+  double last_iterations = 0.0;
+  double last_warm = 0.0;
+  double last_max_err = 0.0, last_mean_err = 0.0;
+
+  // profiling
+  bool prof = false;
+  struct Pending {
+    int name;
+    cudaEvent_t a, b;
+  };
+  std::vector<std::string> prof_names;
+  std::map<std::string, int> prof_index;
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<double> prof_ms;
+  std::vector<int> prof_count;
+
+  ~DeviceSim() { release(); }
+
+  uint32_t* gap_count() { return small; }
+  uint32_t* exp_count() { return small + 1; }
+  uint32_t* err() { return small + 2; }
+
+  void release() {
+    dfree(pos); dfree(pos_alt); dfree(disp); dfree(disp_alt); dfree(vel); dfree(vel_alt);
+    dfree(color); dfree(omega); dfree(dp); dfree(rho); dfree(lam);
+    dfree(color_alt); dfree(omega_alt); dfree(dp_alt); dfree(rho_alt); dfree(lam_alt);
+    dfree(ids); dfree(ids_spare); dfree(keys_by_id); dfree(loc_by_id); dfree(cellp);
+    dfree(mask); dfree(explist); dfree(cstart); dfree(ncount); dfree(gaps); dfree(small);
+    dfree(resid); dfree(sort.keys_alt); dfree(sort.vals_alt); dfree(sort_aux); dfree(stage);
+    mlp_release(mlp);
+    for (auto& p : pending) {
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+    pending.clear();
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    ev_pool.clear();
+  }
+
+  int alloc(int n_) {
+    n = n_;
+    SPHPC_RC(dalloc(&pos, n)); SPHPC_RC(dalloc(&pos_alt, n));
+    SPHPC_RC(dalloc(&disp, n)); SPHPC_RC(dalloc(&disp_alt, n));
+    SPHPC_RC(dalloc(&vel, n)); SPHPC_RC(dalloc(&vel_alt, n));
+    SPHPC_RC(dalloc(&color, n)); SPHPC_RC(dalloc(&omega, n)); SPHPC_RC(dalloc(&dp, n));
+    SPHPC_RC(dalloc(&rho, n)); SPHPC_RC(dalloc(&lam, n));
+    SPHPC_RC(dalloc(&ids, n)); SPHPC_RC(dalloc(&ids_spare, n));
+    SPHPC_RC(dalloc(&keys_by_id, n)); SPHPC_RC(dalloc(&loc_by_id, n));
+    SPHPC_RC(dalloc(&cellp, n)); SPHPC_RC(dalloc(&ncount, n));
+    SPHPC_RC(dalloc(&mask, (size_t)kMaskWords * n));
+    exp_cap = (uint32_t)(n / 16 + 1024);
+    SPHPC_RC(dalloc(&explist, (size_t)exp_cap * kExplicitStride));
+    SPHPC_RC(dalloc(&gaps, (size_t)n + 2));
+    SPHPC_RC(dalloc(&small, 8));
+    SPHPC_RC(dalloc(&resid, 16));
+    SPHPC_RC(dalloc(&sort.keys_alt, n));
+    SPHPC_RC(dalloc(&sort.vals_alt, n));
+    const size_t aux = sort_aux_words(n) + 4;
+    SPHPC_RC(dalloc(&sort_aux, aux));
+    sort.hist = sort_aux;
+    sort.counters = sort_aux + (size_t)kMaxPasses * kRadix;
+    sort.err = sort_aux + (size_t)kMaxPasses * kRadix + kMaxPasses;
+    sort.lookback = sort_aux + (size_t)kMaxPasses * kRadix + kMaxPasses + 4;
+    SPHPC_CK(cudaMemsetAsync(small, 0, 8 * sizeof(uint32_t), stream));
+    SPHPC_CK(cudaMemsetAsync(sort_aux, 0, aux * sizeof(uint32_t), stream));
+    SPHPC_CK(cudaMemsetAsync(disp, 0, sizeof(float4) * n, stream));
+    SPHPC_CK(cudaMemsetAsync(vel, 0, sizeof(float4) * n, stream));
+    SPHPC_CK(cudaMemsetAsync(color, 0, sizeof(float4) * n, stream));
+    SPHPC_CK(cudaMemsetAsync(omega, 0, sizeof(float4) * n, stream));
+    SPHPC_CK(cudaMemsetAsync(dp, 0, sizeof(float4) * n, stream));
+    SPHPC_CK(cudaMemsetAsync(lam, 0, sizeof(float) * n, stream));
+    return SPHPC_OK;
+  }
+
+  int ensure_full_alts() {
+    if (!color_alt) SPHPC_RC(dalloc(&color_alt, n));
+    if (!omega_alt) SPHPC_RC(dalloc(&omega_alt, n));
+    if (!dp_alt) SPHPC_RC(dalloc(&dp_alt, n));
+    if (!rho_alt) SPHPC_RC(dalloc(&rho_alt, n));
+    if (!lam_alt) SPHPC_RC(dalloc(&lam_alt, n));
+    return SPHPC_OK;
+  }
+
+  int ensure_stage() {
+    if (!stage) SPHPC_RC(dalloc(&stage, (size_t)20 * n));
+    return SPHPC_OK;
+  }
+
+  // Grid of the hash (neighbors.c:23-28).
+  int init_grid(const AABB& b, double h) {
+    const double nxd = ceil((b.max_x - b.min_x) / h) + 1;
+    const double nyd = ceil((b.max_y - b.min_y) / h) + 1;
+    const double nzd = ceil((b.max_z - b.min_z) / h) + 1;
+    if (!(nxd >= 1 && nyd >= 1 && nzd >= 1) || nxd * nyd * nzd >= 4294967295.0)
+      return set_error(SPHPC_EINVAL, "grid %.0f x %.0f x %.0f does not fit 32-bit keys", nxd,
+                       nyd, nzd);
+    const int nnx = (int)nxd, nny = (int)nyd, nnz = (int)nzd;
+    const int bxx = bits_for((uint32_t)nnx - 1), byy = bits_for((uint32_t)nny - 1),
+              bzz = bits_for((uint32_t)nnz - 1);
+    if (bxx + byy + bzz > 31)
+      return set_error(SPHPC_EINVAL, "grid %d x %d x %d needs %d bits of packed cell "
+                                     "coordinates (31 available)", nnx, nny, nnz,
+                       bxx + byy + bzz);
+    const uint32_t CC = (uint32_t)nnx * (uint32_t)nny * (uint32_t)nnz;
+    if (grid_ready && CC == C && nnx == nx && nny == ny && nnz == nz) return SPHPC_OK;
+    dfree(cstart);
+    nx = nnx; ny = nny; nz = nnz; C = CC; bx = bxx; by = byy;
+    passes = (bits_for(C - 1) + kRadixBits - 1) / kRadixBits;
+    if (passes > kMaxPasses) passes = kMaxPasses;
+    SPHPC_RC(dalloc(&cstart, (size_t)C + 1));
+    SPHPC_CK(cudaMemsetAsync(cstart, 0, sizeof(uint32_t) * ((size_t)C + 1), stream));
+    grid_ready = true;
+    nbr_valid = false;
+    return SPHPC_OK;
+  }
+
+  NbrView view() const {
+    NbrView v;
+    v.cellp = cellp;
+    v.mask = mask;
+    v.explist = explist;
+    v.cstart = cstart;
+    v.n = n;
+    v.nx = nx; v.ny = ny; v.nz = nz;
+    v.nxny = (uint32_t)nx * (uint32_t)ny;
+    v.bx = bx; v.by = by;
+    v.mx = (1u << bx) - 1u;
+    v.my = (1u << by) - 1u;
+    return v;
+  }
+
+  // ---- profiling ----
+  cudaEvent_t take_event() {
+    if (!ev_pool.empty()) {
+      cudaEvent_t e = ev_pool.back();
+      ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  int prof_begin(const char* name, cudaEvent_t* b) {
+    if (!prof) return -1;
+    auto it = prof_index.find(name);
+    int id;
+    if (it == prof_index.end()) {
+      id = (int)prof_names.size();
+      prof_names.push_back(name);
+      prof_index[name] = id;
+      prof_ms.push_back(0.0);
+      prof_count.push_back(0);
+    } else {
+      id = it->second;
+    }
+    *b = take_event();
+    cudaEventRecord(*b, stream);
+    return id;
+  }
+  void prof_end(int id, cudaEvent_t b) {
+    if (id < 0) return;
+    cudaEvent_t e = take_event();
+    cudaEventRecord(e, stream);
+    pending.push_back({id, b, e});
+  }
+  void prof_collect() {
+    if (pending.empty()) return;
+    cudaStreamSynchronize(stream);
+    for (auto& p : pending) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p.a, p.b);
+      prof_ms[p.name] += ms;
+      prof_count[p.name] += 1;
+      ev_pool.push_back(p.a);
+      ev_pool.push_back(p.b);
+    }
+    pending.clear();
+  }
+
+  struct Scope {
+    DeviceSim* s;
+    int id;
+    cudaEvent_t b;
+    Scope(DeviceSim* s_, const char* name) : s(s_), id(-1), b(nullptr) {
+      id = s->prof_begin(name, &b);
+    }
+    ~Scope() { s->prof_end(id, b); }
+  };
+
+  DevParams params(const Params& prm, const AABB* b, const Obstacle* ob) const;
+
+  int zero_disp_if_pending() {
+    if (disp_zero_pending) {
+      SPHPC_CK(cudaMemsetAsync(disp, 0, sizeof(float4) * n, stream));
+      disp_zero_pending = false;
+    }
+    return SPHPC_OK;
+  }
+
+  int find_neighbors(const DevParams& P, bool predict, bool full, bool move_vel);
+  int run_step(const DevParams& P, const Params& prm);
+};
+
+DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob) const {
+  DevParams P;
+  memset(&P, 0, sizeof(P));
+  const double h = prm.smoothing_radius;
+  const double m = mass;
+  P.n = n;
+  P.nx = nx; P.ny = ny; P.nz = nz;
+  P.nxny = (uint32_t)nx * (uint32_t)ny;
+  P.ncells = C;
+  P.bx = bx; P.by = by;
+  P.mx = (1u << bx) - 1u;
+  P.my = (1u << by) - 1u;
+  P.hd = h;
+  P.h2d = h * h;
+  P.h = (float)h;
+  P.h2 = (float)(h * h);
+  P.rmin = (float)(h * 0.0001);
+  const double W0 = prm.W_norm * (h * h) * (h * h) * (h * h);
+  P.W0m = (float)(m * W0);
+  P.Wn = (float)prm.W_norm;
+  P.Wn_m = (float)(m * prm.W_norm);
+  P.DWn = (float)prm.DelW_norm;
+  P.DWn_m = (float)(m * prm.DelW_norm);
+  P.DWPn = (float)prm.DelW_poly_norm;
+  P.m = (float)m;
+  P.rho0 = (float)rho0;
+  P.inv_rho0 = (float)(1.0 / rho0);
+  P.inv_rho0_sq = (float)(1.0 / (rho0 * rho0));
+  P.lambda_eps = (float)(solver.lambda_epsilon_mass_units
+                             ? solver.lambda_epsilon / (rho0 * rho0)
+                             : solver.lambda_epsilon);
+  P.scorr_k = (float)solver.scorr_k;
+  P.scorr_n = solver.scorr_n;
+  {
+    const double dq = solver.scorr_dq * h;
+    const double t = h * h - dq * dq;
+    const double Wdq = dq > h ? 0.0 : prm.W_norm * t * t * t;
+    P.inv_Wdq = Wdq > 0.0 ? (float)(1.0 / Wdq) : 0.0f;
+    if (Wdq <= 0.0) P.scorr_k = 0.0f;
+  }
+  P.c_xsph = (float)prm.c;
+  P.xsph_exact = solver.xsph_exact;
+  P.gamma = (float)prm.k;
+  P.C_norm = (float)(32.0 / (M_PI * pow(h, 9.0)));
+  P.vort_eps = (float)(solver.vorticity_epsilon < 0.0 ? 0.1 * h : solver.vorticity_epsilon);
+  P.dt = (float)prm.time_step;
+  P.inv_dt = (float)(1.0 / prm.time_step);
+  P.v_max = (float)solver.velocity_max;
+  P.dt_d = prm.time_step;
+  P.gdt_d = (-prm.g) * prm.time_step;
+  P.gdt_f = (float)P.gdt_d;
+  P.gaxis = solver.gravity_axis;
+  if (b) {
+    const double lo[3] = {b->min_x, b->min_y, b->min_z};
+    const double hi[3] = {b->max_x, b->max_y, b->max_z};
+    const double eps = h * 0.0001;
+    for (int k = 0; k < 3; ++k) {
+      P.bmin[k] = lo[k];
+      P.bmax[k] = hi[k];
+      P.bmax_eps[k] = hi[k] - eps;
+    }
+  }
+  if (ob && ob->obstacle_cuda && ob->obstacle_cuda->sdf) {
+    P.has_sdf = 1;
+    P.sdf = ob->obstacle_cuda->sdf;
+    P.sdim[0] = ob->SDF_dim_x;
+    P.sdim[1] = ob->SDF_dim_y;
+    P.sdim[2] = ob->SDF_dim_z;
+    const double lo[3] = {ob->world_bounds.min_x, ob->world_bounds.min_y, ob->world_bounds.min_z};
+    const double hi[3] = {ob->world_bounds.max_x, ob->world_bounds.max_y, ob->world_bounds.max_z};
+    for (int k = 0; k < 3; ++k) {
+      P.ob_min[k] = lo[k];
+      P.ob_max[k] = hi[k];
+      P.ob_len[k] = (float)(hi[k] - lo[k]);
+      P.tex_sp[k] = (float)(1.0 / (float)P.sdim[k]);
+    }
+    const float len_model = (float)(ob->SDF_dim_x * ob->SDF_spacing);
+    P.model_to_world = P.ob_len[0] / len_model;
+  }
+  return P;
+}
+
+int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool move_vel) {
+  if (!grid_ready) return set_error(SPHPC_ENOTREADY, "neighbour grid not initialised");
+  {
+    Scope sc(this, "hash");
+    SPHPC_CK(cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * kMaxPasses * kRadix, stream));
+    launch_hash(P, pos, vel, disp, ids, keys_by_id, loc_by_id, sort.hist, passes, predict, err(),
+                stream);
+  }
+  uint32_t *K = nullptr, *R = nullptr;
+  {
+    Scope sc(this, "radix_sort");
+    const cudaError_t e = radix_sort_pairs(keys_by_id, ids_spare, n, passes, sort, stream, true,
+                                           true, false, &K, &R);
+    if (e != cudaSuccess)
+      return set_error(SPHPC_ECUDA, "radix sort: %s", cudaGetErrorString(e));
+  }
+  keys_sorted = K;
+  {
+    Scope sc(this, "cell_starts");
+    launch_cell_starts(K, n, C, cstart, gaps, gap_count(), err(), stream);
+  }
+  {
+    Scope sc(this, "reorder");
+    ReorderExtra ex{};
+    if (full) {
+      SPHPC_RC(ensure_full_alts());
+      ex.in4[0] = color; ex.out4[0] = color_alt;
+      ex.in4[1] = omega; ex.out4[1] = omega_alt;
+      ex.in4[2] = dp; ex.out4[2] = dp_alt;
+      ex.in1[0] = rho; ex.out1[0] = rho_alt;
+      ex.in1[1] = lam; ex.out1[1] = lam_alt;
+    }
+    const bool mv = move_vel || full;
+    launch_reorder(P, R, loc_by_id, pos, vel, disp, pos_alt, vel_alt, disp_alt, cellp, predict,
+                   mv, &ex, stream);
+    std::swap(pos, pos_alt);
+    std::swap(disp, disp_alt);
+    if (mv) std::swap(vel, vel_alt);
+    if (full) {
+      std::swap(color, color_alt);
+      std::swap(omega, omega_alt);
+      std::swap(dp, dp_alt);
+      std::swap(rho, rho_alt);
+      std::swap(lam, lam_alt);
+    }
+    uint32_t* old = ids;
+    ids = R;
+    if (R == ids_spare) ids_spare = old;
+    else sort.vals_alt = old;
+  }
+  {
+    Scope sc(this, "build_neighbors");
+    launch_build_neighbors(P, view(), pos, disp, cellp, mask, explist, exp_cap, exp_count(),
+                           ncount, err(), stream);
+  }
+  SPHPC_CK(cudaGetLastError());
+  nbr_valid = true;
+  disp_zero_pending = false;
+  return SPHPC_OK;
+}
+
+static float stiffness_of(double k_stiff, int substep) {
+  // particles.c:693-694 (substep 0 gives 1/0 = inf and stiffness 1)
+  return (float)(1.0 - pow(1.0 - k_stiff, 1.0 / (double)substep));
+}
+
+int DeviceSim::run_step(const DevParams& P, const Params& prm) {
+  const bool warm = solver.warm_start && mlp.ready;
+  SPHPC_RC(find_neighbors(P, true, false, warm));
+  const NbrView V = view();
+  PassArgs a{};
+  a.pos = pos;
+  a.rho = rho;
+  a.vel = vel;
+  a.vel_out = vel;
+  a.resid = resid;
+  const int fixed_iters = solver.solve_iterations;
+  const bool adaptive = solver.adaptive != 0;
+  const int max_iters = adaptive ? solver.max_iterations : fixed_iters;
+  int k0 = 0;
+  last_warm = 0.0;
+  if (warm) {
+    // warm start: features -> MLP lambda0 -> one position pass (stiffness 1)
+    Scope sc(this, "mlp_warm_start");
+    SPHPC_RC(mlp_warm_start(mlp, P, V, pos, disp, disp_alt, vel, ncount, stream));
+    a.disp = disp_alt;
+    a.disp_out = disp;
+    a.stiffness = 1.0f;
+    a.last = 0;
+    launch_position(P, V, a, 0, stream);
+    last_warm = 1.0;
+  }
+  int iters = 0;
+  bool converged = false;
+  for (int k = k0; k < max_iters; ++k) {
+    {
+      Scope sc(this, "density_lambda");
+      SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
+      a.disp = disp;
+      a.disp_out = disp_alt;
+      a.lam = nullptr;
+      launch_density_lambda(P, V, a, 0, true, stream);
+    }
+    if (adaptive) {
+      double h_res[2];
+      SPHPC_CK(cudaMemcpyAsync(h_res, resid, sizeof(h_res), cudaMemcpyDeviceToHost, stream));
+      SPHPC_CK(cudaStreamSynchronize(stream));
+      last_max_err = h_res[0];
+      last_mean_err = h_res[1] / (n > 0 ? n : 1);
+      if (h_res[0] <= solver.density_tolerance) {
+        converged = true;
+        break;
+      }
+    }
+    {
+      Scope sc(this, "position");
+      a.disp = disp_alt;
+      a.disp_out = disp;
+      // the warm-started pass counts as substep 0; plain iterations continue
+      a.stiffness = stiffness_of(solver.stiffness_k, warm ? k + 1 : k);
+      a.last = (!adaptive && k == max_iters - 1) ? 1 : 0;
+      launch_position(P, V, a, 0, stream);
+    }
+    ++iters;
+  }
+  if (adaptive || max_iters == 0) {
+    // converged (or cap reached): velocities from x* and the freshest density
+    Scope sc(this, "velocity");
+    if (converged) launch_pack_w(P, disp, rho, stream);
+    else if (max_iters == 0) launch_pack_w(P, disp, rho, stream);
+    launch_update_velocities(P, disp, vel, stream);
+  }
+  last_iterations = iters + (warm ? 1 : 0);
+  // post-solve passes (simulation.c:93-106)
+  a.disp = disp;
+  a.pos_out = pos_alt;
+  if (solver.surface_tension) {
+    Scope sc(this, "surface_tension");
+    a.color = color;
+    launch_color(P, V, a, stream);
+    a.vel = vel;
+    launch_tension(P, V, a, stream);
+  }
+  {
+    Scope sc(this, "xsph");
+    a.vel = vel;
+    a.vel_out = vel_alt;
+    a.write_pos = solver.vorticity ? 0 : 1;
+    launch_xsph(P, V, a, stream);
+  }
+  if (solver.vorticity) {
+    Scope sc(this, "vorticity");
+    a.vel = vel_alt;
+    a.omega = omega;
+    a.write_pos = 0;
+    launch_vorticity(P, V, a, stream);
+    a.write_pos = 1;
+    launch_confinement(P, V, a, stream);
+  }
+  std::swap(vel, vel_alt);
+  std::swap(pos, pos_alt);
+  disp_zero_pending = true;  // UpdatePositions: x = x*, so x* - x = 0
+  SPHPC_CK(cudaGetLastError());
+  (void)prm;
+  return SPHPC_OK;
+}
+
+// ---- registry of device copies (the "present" table) ----
+static std::mutex g_mu;
+static std::unordered_map<const Particles*, DeviceSim*> g_sims;
+
+static DeviceSim* find_sim(const Particles* p) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_sims.find(p);
+  return it == g_sims.end() ? nullptr : it->second;
+}
+
+#define SPHPC_SIM(var, particles)                                                        \
+  DeviceSim* var = find_sim(particles);                                                  \
+  if (!var)                                                                              \
+    return set_error(SPHPC_ENOTREADY, "%s: particles have no device copy (call "         \
+                                      "AllocInitParticles or sphpc_enter_data)",         \
+                     __func__);
+
+// ---- host <-> device transfers ----
+
+__global__ void k_download(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ pos,
+                           const float4* __restrict__ disp, const float4* __restrict__ vel,
+                           const float4* __restrict__ dp, const float4* __restrict__ omega,
+                           const float4* __restrict__ color, const float* __restrict__ rho,
+                           const float* __restrict__ lam, int disp_zero, double* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const size_t N = (size_t)n;
+  const uint32_t id = ids[p];
+  const float4 x = pos[p];
+  const float4 d = disp_zero ? make_float4(0.f, 0.f, 0.f, 0.f) : disp[p];
+  const float4 v = vel[p], q = dp[p], w = omega[p], c = color[p];
+  out[0 * N + id] = xstar_d(x.x, d.x);
+  out[1 * N + id] = xstar_d(x.y, d.y);
+  out[2 * N + id] = xstar_d(x.z, d.z);
+  out[3 * N + id] = x.x; out[4 * N + id] = x.y; out[5 * N + id] = x.z;
+  out[6 * N + id] = v.x; out[7 * N + id] = v.y; out[8 * N + id] = v.z;
+  out[9 * N + id] = q.x; out[10 * N + id] = q.y; out[11 * N + id] = q.z;
+  out[12 * N + id] = w.x; out[13 * N + id] = w.y; out[14 * N + id] = w.z;
+  out[15 * N + id] = c.x; out[16 * N + id] = c.y; out[17 * N + id] = c.z;
+  out[18 * N + id] = rho[p];
+  out[19 * N + id] = lam[p];
+}
+
+__global__ void k_upload(int n, const uint32_t* __restrict__ ids, const double* __restrict__ in,
+                         unsigned mask, float4* pos, float4* disp, float4* vel, float4* dp,
+                         float4* omega, float4* color, float* rho, float* lam) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const size_t N = (size_t)n;
+  const uint32_t id = ids[p];
+  auto f = [&](int k) { return in[(size_t)k * N + id]; };
+  if (mask & (1u << 3)) {
+    const float x = (float)f(3), y = (float)f(4), z = (float)f(5);
+    pos[p] = make_float4(x, y, z, 0.f);
+    float4 d = make_float4(0.f, 0.f, 0.f, disp[p].w);
+    if (mask & (1u << 0)) {
+      d.x = (float)(f(0) - (double)x);
+      d.y = (float)(f(1) - (double)y);
+      d.z = (float)(f(2) - (double)z);
+    }
+    disp[p] = d;
+  }
+  if (mask & (1u << 6)) vel[p] = make_float4((float)f(6), (float)f(7), (float)f(8), 0.f);
+  if (mask & (1u << 9)) dp[p] = make_float4((float)f(9), (float)f(10), (float)f(11), 0.f);
+  if (mask & (1u << 12)) omega[p] = make_float4((float)f(12), (float)f(13), (float)f(14), 0.f);
+  if (mask & (1u << 15)) color[p] = make_float4((float)f(15), (float)f(16), (float)f(17), 0.f);
+  if (mask & (1u << 18)) rho[p] = (float)f(18);
+  if (mask & (1u << 19)) lam[p] = (float)f(19);
+}
+
+__global__ void k_iota(uint32_t* a, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = (uint32_t)i;
+}
+
+// FP64 diagnostics: [0] max err (u64 bits), [1] sum err, [2] sum |v|^2,
+// [3..5] sum x, [6..8] sum v
+__global__ void __launch_bounds__(kBlock)
+    k_diag(int n, float rho0, const float4* __restrict__ pos, const float4* __restrict__ vel,
+           const float* __restrict__ rho, double* __restrict__ out) {
+  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const double e = fmax((double)rho[p] / (double)rho0 - 1.0, 0.0);
+    v[0] = fmax(v[0], e);
+    v[1] += e;
+    const float4 u = vel[p], x = pos[p];
+    v[2] += (double)u.x * u.x + (double)u.y * u.y + (double)u.z * u.z;
+    v[3] += x.x; v[4] += x.y; v[5] += x.z;
+    v[6] += u.x; v[7] += u.y; v[8] += u.z;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    v[0] = fmax(v[0], __shfl_xor_sync(0xffffffffu, v[0], o));
+    for (int k = 1; k < 9; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(reinterpret_cast<unsigned long long*>(out),
+              (unsigned long long)__double_as_longlong(v[0]));
+    for (int k = 1; k < 9; ++k) atomicAdd(out + k, v[k]);
+  }
+}
+
+static int enter_data(Particles* particles, const Params* params, DeviceSim** out) {
+  if (!particles || !params) return set_error(SPHPC_EINVAL, "sphpc_enter_data: null argument");
+  if (particles->local_count <= 0 || !particles->x || !particles->y || !particles->z)
+    return set_error(SPHPC_EINVAL, "sphpc_enter_data: no particles");
+  if (find_sim(particles))
+    return set_error(SPHPC_EINVAL, "sphpc_enter_data: particles already have a device copy");
+  int ndev = 0;
+  const cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_error(SPHPC_ECUDA, "no CUDA device: %s", cudaGetErrorString(e));
+  }
+  DeviceSim* s = new DeviceSim();
+  cudaGetDevice(&s->device);
+  s->solver = current_solver();
+  s->rho0 = particles->rest_density;
+  s->mass = particles->rest_mass;
+  int rc = s->alloc(particles->local_count);
+  if (!rc) {
+    k_iota<<<grid_for(s->n), kBlock, 0, s->stream>>>(s->ids, s->n);
+    {
+      std::lock_guard<std::mutex> lk(g_mu);
+      g_sims[particles] = s;
+    }
+    rc = sphpc_update_device(particles);
+    if (rc) {
+      std::lock_guard<std::mutex> lk(g_mu);
+      g_sims.erase(particles);
+    }
+  }
+  if (rc) {
+    delete s;
+    return rc;
+  }
+  if (out) *out = s;
+  return SPHPC_OK;
+}
+
+// Device scratch of the SortByKey seam, one cache per device.
+struct SeamScratch {
+  SortScratch s{};
+  uint32_t* aux = nullptr;
+  int cap = 0;
+};
+static std::mutex g_seam_mu;
+static std::map<int, SeamScratch> g_seam;
+
+}  // namespace sphpc
+
+using namespace sphpc;
+
+extern "C" {
+
+int sphpc_enter_data(struct Particles* particles, const struct Params* params) {
+  clear_error();
+  return enter_data(particles, params, nullptr);
+}
+
+int sphpc_exit_data(struct Particles* particles) {
+  DeviceSim* s = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_sims.find(particles);
+    if (it == g_sims.end()) return set_error(SPHPC_ENOTREADY, "sphpc_exit_data: no device copy");
+    s = it->second;
+    g_sims.erase(it);
+  }
+  cudaStreamSynchronize(s->stream);
+  delete s;
+  return SPHPC_OK;
+}
+
+int sphpc_set_solver(struct Particles* particles, const struct SphpcSolver* solver) {
+  SPHPC_SIM(s, particles);
+  if (!solver) return set_error(SPHPC_EINVAL, "sphpc_set_solver: null");
+  s->solver = *solver;
+  return SPHPC_OK;
+}
+
+int sphpc_get_solver(const struct Particles* particles, struct SphpcSolver* solver) {
+  SPHPC_SIM(s, particles);
+  if (!solver) return set_error(SPHPC_EINVAL, "sphpc_get_solver: null");
+  *solver = s->solver;
+  return SPHPC_OK;
+}
+
+int sphpc_set_stream(struct Particles* particles, void* cuda_stream) {
+  SPHPC_SIM(s, particles);
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  s->stream = (cudaStream_t)cuda_stream;
+  return SPHPC_OK;
+}
+
+int sphpc_update_host(struct Particles* p) {
+  SPHPC_SIM(s, p);
+  SPHPC_RC(s->ensure_stage());
+  const int n = s->n;
+  k_download<<<grid_for(n), kBlock, 0, s->stream>>>(n, s->ids, s->pos, s->disp, s->vel, s->dp,
+                                                    s->omega, s->color, s->rho, s->lam,
+                                                    s->disp_zero_pending ? 1 : 0, s->stage);
+  SPHPC_CK(cudaGetLastError());
+  double* fields[20] = {p->x_star, p->y_star, p->z_star, p->x, p->y, p->z, p->v_x, p->v_y,
+                        p->v_z, p->dp_x, p->dp_y, p->dp_z, p->w_x, p->w_y, p->w_z,
+                        p->color_x, p->color_y, p->color_z, p->density, p->lambda};
+  for (int k = 0; k < 20; ++k)
+    if (fields[k])
+      SPHPC_CK(cudaMemcpyAsync(fields[k], s->stage + (size_t)k * n, sizeof(double) * n,
+                               cudaMemcpyDeviceToHost, s->stream));
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  if (p->id)
+    for (int i = 0; i < n; ++i) p->id[i] = i;
+  return SPHPC_OK;
+}
+
+int sphpc_update_device(struct Particles* p) {
+  SPHPC_SIM(s, p);
+  SPHPC_RC(s->ensure_stage());
+  const int n = s->n;
+  const double* fields[20] = {p->x_star, p->y_star, p->z_star, p->x, p->y, p->z, p->v_x,
+                              p->v_y, p->v_z, p->dp_x, p->dp_y, p->dp_z, p->w_x, p->w_y,
+                              p->w_z, p->color_x, p->color_y, p->color_z, p->density,
+                              p->lambda};
+  unsigned mask = 0;
+  const int groups[8][2] = {{0, 3}, {3, 3}, {6, 3}, {9, 3}, {12, 3}, {15, 3}, {18, 1}, {19, 1}};
+  for (auto& g : groups) {
+    bool all = true;
+    for (int k = g[0]; k < g[0] + g[1]; ++k) all = all && fields[k] != nullptr;
+    if (!all) continue;
+    mask |= 1u << g[0];
+    for (int k = g[0]; k < g[0] + g[1]; ++k)
+      SPHPC_CK(cudaMemcpyAsync(s->stage + (size_t)k * n, fields[k], sizeof(double) * n,
+                               cudaMemcpyHostToDevice, s->stream));
+  }
+  if (!(mask & (1u << 3)))
+    return set_error(SPHPC_EINVAL, "sphpc_update_device: x, y, z are required");
+  SPHPC_RC(s->zero_disp_if_pending());
+  k_upload<<<grid_for(n), kBlock, 0, s->stream>>>(n, s->ids, s->stage, mask, s->pos, s->disp,
+                                                  s->vel, s->dp, s->omega, s->color, s->rho,
+                                                  s->lam);
+  SPHPC_CK(cudaGetLastError());
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  return SPHPC_OK;
+}
+
+int AllocInitParticles(struct Particles* particles, struct Params* params,
+                       struct AABB* fluid_volume_initial) {
+  clear_error();
+  if (!particles || !params || !fluid_volume_initial)
+    return set_error(SPHPC_EINVAL, "AllocInitParticles: null argument");
+  if (particles->max_local <= 0)
+    SPHPC_RC(SetParticleNumbers(fluid_volume_initial, particles, params, nullptr));
+  const size_t n = (size_t)particles->max_local;
+  double* SPHPC_RESTRICT* dfields[20] = {&particles->x_star, &particles->y_star, &particles->z_star,
+                          &particles->x, &particles->y, &particles->z, &particles->v_x,
+                          &particles->v_y, &particles->v_z, &particles->dp_x, &particles->dp_y,
+                          &particles->dp_z, &particles->w_x, &particles->w_y, &particles->w_z,
+                          &particles->color_x, &particles->color_y, &particles->color_z,
+                          &particles->density, &particles->lambda};
+  for (auto f : dfields) {
+    *f = (double*)calloc(n, sizeof(double));
+    if (!*f) return set_error(SPHPC_ENOMEM, "AllocInitParticles: calloc of %zu doubles", n);
+  }
+  particles->id = (int*)calloc(n, sizeof(int));
+  if (!particles->id) return set_error(SPHPC_ENOMEM, "AllocInitParticles: calloc ids");
+  SPHPC_RC(ConstructFluidVolume(particles, params, fluid_volume_initial));
+  const SphpcSolver sv = current_solver();
+  const double spacing = 2.0 * particles->rest_radius;
+  if (sv.rest_density_lattice) {
+    particles->rest_mass = params->fluid_volume * 1000.0 / (double)particles->global_count;
+    particles->rest_density =
+        particles->rest_mass *
+        lattice_poly6_sum(params->smoothing_radius, params->W_norm, spacing);
+  } else {
+    // particles.c:1034-1037
+    particles->rest_density = 1000.0;
+    particles->rest_mass =
+        params->fluid_volume * particles->rest_density / (double)particles->global_count;
+    particles->rest_mass *= .991;
+  }
+  for (int i = 0; i < particles->local_count; ++i) {
+    particles->v_x[i] = 0.0;
+    particles->v_y[i] = 0.0;
+    particles->v_z[i] = 0.0;
+    particles->x_star[i] = particles->x[i];
+    particles->y_star[i] = particles->y[i];
+    particles->z_star[i] = particles->z[i];
+    particles->density[i] = particles->rest_density;
+  }
+  particles->halo_count_left = 0;
+  particles->halo_count_right = 0;
+  return enter_data(particles, params, nullptr);
+}
+
+int FinalizeParticles(struct Particles* particles) {
+  if (!particles) return set_error(SPHPC_EINVAL, "FinalizeParticles: null");
+  if (find_sim(particles)) sphpc_exit_data(particles);
+  double* SPHPC_RESTRICT* dfields[20] = {&particles->x_star, &particles->y_star, &particles->z_star,
+                          &particles->x, &particles->y, &particles->z, &particles->v_x,
+                          &particles->v_y, &particles->v_z, &particles->dp_x, &particles->dp_y,
+                          &particles->dp_z, &particles->w_x, &particles->w_y, &particles->w_z,
+                          &particles->color_x, &particles->color_y, &particles->color_z,
+                          &particles->density, &particles->lambda};
+  for (auto f : dfields) {
+    free(*f);
+    *f = nullptr;
+  }
+  free(particles->id);
+  particles->id = nullptr;
+  return SPHPC_OK;
+}
+
+// ---- neighbours ----
+
+int AllocInitNeighbors(struct Neighbors* neighbors, const struct Particles* particles,
+                       const struct Params* params, const struct AABB* boundary_global) {
+  if (!neighbors || !params || !boundary_global)
+    return set_error(SPHPC_EINVAL, "AllocInitNeighbors: null argument");
+  memset(neighbors, 0, sizeof(*neighbors));
+  const double h = params->smoothing_radius;
+  neighbors->hash_size_x = (int)(ceil((boundary_global->max_x - boundary_global->min_x) / h) + 1);
+  neighbors->hash_size_y = (int)(ceil((boundary_global->max_y - boundary_global->min_y) / h) + 1);
+  neighbors->hash_size_z = (int)(ceil((boundary_global->max_z - boundary_global->min_z) / h) + 1);
+  neighbors->hash_spacing = h;
+  SPHPC_SIM(s, particles);
+  return s->init_grid(*boundary_global, h);
+}
+
+int FinalizeNeighbors(struct Neighbors* neighbors) {
+  if (neighbors) memset(neighbors, 0, sizeof(*neighbors));
+  return SPHPC_OK;
+}
+
+int FindAllNeighbors(const struct Particles* particles, const struct Params* params,
+                     struct Neighbors* neighbors) {
+  (void)neighbors;
+  SPHPC_SIM(s, particles);
+  if (!params) return set_error(SPHPC_EINVAL, "FindAllNeighbors: null params");
+  SPHPC_RC(s->zero_disp_if_pending());
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  return s->find_neighbors(P, false, true, true);
+}
+
+int sphpc_get_neighbor_buckets(const struct Particles* particles, unsigned int* indices,
+                               int* counts) {
+  SPHPC_SIM(s, particles);
+  if (!s->nbr_valid) return set_error(SPHPC_ENOTREADY, "no neighbour lists built yet");
+  uint32_t* d_nbr = nullptr;
+  int32_t* d_cnt = nullptr;
+  SPHPC_RC(dalloc(&d_nbr, (size_t)s->n * kMaxNeighbors));
+  int rc = dalloc(&d_cnt, (size_t)s->n);
+  if (rc) {
+    dfree(d_nbr);
+    return rc;
+  }
+  launch_export_buckets(s->view(), s->ids, d_nbr, d_cnt, s->stream);
+  cudaError_t e = cudaMemcpyAsync(indices, d_nbr, sizeof(uint32_t) * s->n * kMaxNeighbors,
+                                  cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(counts, d_cnt, sizeof(int32_t) * s->n, cudaMemcpyDeviceToHost,
+                        s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  dfree(d_nbr);
+  dfree(d_cnt);
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "bucket export: %s", cudaGetErrorString(e));
+  return SPHPC_OK;
+}
+
+int sphpc_get_cell_data(const struct Particles* particles, unsigned int* hash_values,
+                        unsigned int* particle_ids, unsigned int* start_indices) {
+  SPHPC_SIM(s, particles);
+  if (!s->nbr_valid || !s->keys_sorted) return set_error(SPHPC_ENOTREADY, "no cell data yet");
+  if (hash_values)
+    SPHPC_CK(cudaMemcpyAsync(hash_values, s->keys_sorted, sizeof(uint32_t) * s->n,
+                             cudaMemcpyDeviceToHost, s->stream));
+  if (particle_ids)
+    SPHPC_CK(cudaMemcpyAsync(particle_ids, s->ids, sizeof(uint32_t) * s->n,
+                             cudaMemcpyDeviceToHost, s->stream));
+  if (start_indices)
+    SPHPC_CK(cudaMemcpyAsync(start_indices, s->cstart, sizeof(uint32_t) * ((size_t)s->C + 1),
+                             cudaMemcpyDeviceToHost, s->stream));
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  return SPHPC_OK;
+}
+
+// ---- step functions (one stage each) ----
+
+#define SPHPC_STAGE_BEGIN(particles, params)                               \
+  SPHPC_SIM(s, particles);                                                 \
+  if (!(params)) return set_error(SPHPC_EINVAL, "%s: null params", __func__); \
+  SPHPC_RC(s->zero_disp_if_pending());
+
+#define SPHPC_NEED_NBR()                                                                  \
+  if (!s->nbr_valid)                                                                      \
+    return set_error(SPHPC_ENOTREADY, "%s: call FindAllNeighbors first", __func__);
+
+#define SPHPC_LAUNCH_DONE() SPHPC_CK(cudaGetLastError()); return SPHPC_OK;
+
+int ApplyGravity(struct Particles* particles, const struct Params* params) {
+  SPHPC_STAGE_BEGIN(particles, params);
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  launch_gravity(P, s->vel, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+int PredictPositions(struct Particles* particles, const struct Params* params,
+                     const struct AABB* boundary_global) {
+  SPHPC_STAGE_BEGIN(particles, params);
+  if (!boundary_global) return set_error(SPHPC_EINVAL, "PredictPositions: null boundary");
+  const DevParams P = s->params(*params, boundary_global, nullptr);
+  launch_predict(P, s->pos, s->vel, s->disp, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+int ComputeDensities(struct Particles* particles, const struct Params* params,
+                     const struct Neighbors* neighbors) {
+  (void)neighbors;
+  SPHPC_STAGE_BEGIN(particles, params);
+  SPHPC_NEED_NBR();
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  PassArgs a{};
+  a.pos = s->pos;
+  a.disp = s->disp;
+  a.rho = s->rho;
+  a.resid = s->resid;
+  SPHPC_CK(cudaMemsetAsync(s->resid, 0, 2 * sizeof(double), s->stream));
+  launch_density_lambda(P, s->view(), a, 1, true, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+int ComputeLambda(struct Particles* particles, const struct Params* params,
+                  const struct Neighbors* neighbors) {
+  (void)neighbors;
+  SPHPC_STAGE_BEGIN(particles, params);
+  SPHPC_NEED_NBR();
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  PassArgs a{};
+  a.pos = s->pos;
+  a.disp = s->disp;
+  a.disp_out = s->disp_alt;
+  a.rho = s->rho;
+  a.lam = s->lam;
+  launch_density_lambda(P, s->view(), a, 2, false, s->stream);
+  std::swap(s->disp, s->disp_alt);
+  SPHPC_LAUNCH_DONE();
+}
+
+int UpdateDPs(struct Particles* particles, const struct Params* params,
+              const struct Neighbors* neighbors, const int substep) {
+  (void)neighbors;
+  SPHPC_STAGE_BEGIN(particles, params);
+  SPHPC_NEED_NBR();
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  launch_pack_w(P, s->disp, s->lam, s->stream);
+  PassArgs a{};
+  a.pos = s->pos;
+  a.disp = s->disp;
+  a.dp = s->dp;
+  a.rho = s->rho;
+  a.stiffness = stiffness_of(s->solver.stiffness_k, substep);
+  launch_position(P, s->view(), a, 1, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+int UpdatePositionStars(struct Particles* particles, const struct AABB* boundary_global,
+                        const struct Obstacle* obstacle, const struct Params* params) {
+  SPHPC_STAGE_BEGIN(particles, params);
+  if (!boundary_global) return set_error(SPHPC_EINVAL, "UpdatePositionStars: null boundary");
+  const DevParams P = s->params(*params, boundary_global, obstacle);
+  PassArgs a{};
+  a.pos = s->pos;
+  a.disp_out = s->disp;
+  a.dp = s->dp;
+  launch_apply_dp(P, a, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+int UpdateVelocities(struct Particles* particles, const struct Params* params) {
+  SPHPC_STAGE_BEGIN(particles, params);
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  launch_update_velocities(P, s->disp, s->vel, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+int ComputeSurfaceTension(struct Particles* particles, const struct Params* params,
+                          const struct Neighbors* neighbors) {
+  (void)neighbors;
+  SPHPC_STAGE_BEGIN(particles, params);
+  SPHPC_NEED_NBR();
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  launch_pack_w(P, s->disp, s->rho, s->stream);
+  PassArgs a{};
+  a.pos = s->pos;
+  a.disp = s->disp;
+  a.color = s->color;
+  a.vel = s->vel;
+  launch_color(P, s->view(), a, s->stream);
+  launch_tension(P, s->view(), a, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+int ApplyViscosity(struct Particles* particles, const struct Params* params,
+                   const struct Neighbors* neighbors) {
+  (void)neighbors;
+  SPHPC_STAGE_BEGIN(particles, params);
+  SPHPC_NEED_NBR();
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  launch_pack_w(P, s->disp, s->rho, s->stream);
+  PassArgs a{};
+  a.pos = s->pos;
+  a.disp = s->disp;
+  a.vel = s->vel;
+  a.vel_out = s->vel_alt;
+  launch_xsph(P, s->view(), a, s->stream);
+  std::swap(s->vel, s->vel_alt);
+  SPHPC_LAUNCH_DONE();
+}
+
+int ComputeVorticity(struct Particles* particles, const struct Params* params,
+                     const struct Neighbors* neighbors) {
+  (void)neighbors;
+  SPHPC_STAGE_BEGIN(particles, params);
+  SPHPC_NEED_NBR();
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  PassArgs a{};
+  a.pos = s->pos;
+  a.disp = s->disp;
+  a.vel = s->vel;
+  a.omega = s->omega;
+  launch_vorticity(P, s->view(), a, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+int ApplyVorticityConfinement(struct Particles* particles, const struct Params* params,
+                              const struct Neighbors* neighbors) {
+  (void)neighbors;
+  SPHPC_STAGE_BEGIN(particles, params);
+  SPHPC_NEED_NBR();
+  const DevParams P = s->params(*params, nullptr, nullptr);
+  PassArgs a{};
+  a.pos = s->pos;
+  a.disp = s->disp;
+  a.vel = s->vel;
+  a.omega = s->omega;
+  launch_confinement(P, s->view(), a, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+int UpdatePositions(struct Particles* particles) {
+  SPHPC_SIM(s, particles);
+  SPHPC_RC(s->zero_disp_if_pending());
+  DevParams P{};
+  P.n = s->n;
+  launch_update_positions(P, s->pos, s->disp, s->pos, s->stream);
+  SPHPC_LAUNCH_DONE();
+}
+
+// ---- whole step ----
+
+int sphpc_step(struct Particles* particles, const struct Params* params,
+               struct Neighbors* neighbors, const struct AABB* boundary_global,
+               const struct Obstacle* obstacle, int steps) {
+  (void)neighbors;
+  SPHPC_SIM(s, particles);
+  if (!params || !boundary_global) return set_error(SPHPC_EINVAL, "sphpc_step: null argument");
+  if (steps < 0) return set_error(SPHPC_EINVAL, "sphpc_step: negative step count");
+  if (!s->grid_ready) SPHPC_RC(s->init_grid(*boundary_global, params->smoothing_radius));
+  const DevParams P = s->params(*params, boundary_global, obstacle);
+  for (int k = 0; k < steps; ++k) SPHPC_RC(s->run_step(P, *params));
+  return SPHPC_OK;
+}
+
+int sphpc_diagnostics(const struct Particles* particles, struct SphpcDiag* diag) {
+  SPHPC_SIM(s, particles);
+  if (!diag) return set_error(SPHPC_EINVAL, "sphpc_diagnostics: null");
+  double* out = s->resid + 4;
+  SPHPC_CK(cudaMemsetAsync(out, 0, 9 * sizeof(double), s->stream));
+  k_diag<<<148 * 2, kBlock, 0, s->stream>>>(s->n, (float)s->rho0, s->pos, s->vel, s->rho, out);
+  double h[9];
+  SPHPC_CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  memset(diag, 0, sizeof(*diag));
+  const double n = s->n > 0 ? s->n : 1;
+  diag->max_density_error = h[0];
+  diag->mean_density_error = h[1] / n;
+  diag->kinetic_energy = 0.5 * s->mass * h[2];
+  for (int k = 0; k < 3; ++k) {
+    diag->com[k] = h[3 + k] / n;
+    diag->momentum[k] = s->mass * h[6 + k];
+  }
+  diag->iterations = s->last_iterations;
+  diag->warm_start_used = s->last_warm;
+  return SPHPC_OK;
+}
+
+int sphpc_device_errors(const struct Particles* particles, unsigned int* bits) {
+  SPHPC_SIM(s, particles);
+  uint32_t h[2] = {0, 0};
+  SPHPC_CK(cudaMemcpyAsync(&h[0], s->err(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+  SPHPC_CK(cudaMemcpyAsync(&h[1], s->sort.err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           s->stream));
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  SPHPC_CK(cudaMemsetAsync(s->err(), 0, sizeof(uint32_t), s->stream));
+  SPHPC_CK(cudaMemsetAsync(s->sort.err, 0, sizeof(uint32_t), s->stream));
+  if (bits) *bits = h[0] | h[1];
+  return SPHPC_OK;
+}
+
+int sphpc_profile(struct Particles* particles, int enable) {
+  SPHPC_SIM(s, particles);
+  s->prof_collect();
+  s->prof = enable != 0;
+  for (auto& v : s->prof_ms) v = 0.0;
+  for (auto& c : s->prof_count) c = 0;
+  return SPHPC_OK;
+}
+
+int sphpc_profile_read(const struct Particles* particles, struct SphpcKernelTime* out,
+                       int max_entries, int* n_entries) {
+  SPHPC_SIM(s, particles);
+  s->prof_collect();
+  const int m = (int)s->prof_names.size();
+  for (int i = 0; i < m && i < max_entries; ++i) {
+    memset(&out[i], 0, sizeof(out[i]));
+    strncpy(out[i].name, s->prof_names[i].c_str(), sizeof(out[i].name) - 1);
+    out[i].launches = s->prof_count[i];
+    out[i].total_ms = s->prof_ms[i];
+  }
+  if (n_entries) *n_entries = m;
+  return SPHPC_OK;
+}
+
+// ---- obstacle ----
+
+int AllocInitObstacle_CUDA(struct Obstacle* obstacle) {
+  if (!obstacle || !obstacle->SDF_buffer)
+    return set_error(SPHPC_EINVAL, "AllocInitObstacle_CUDA: no SDF buffer");
+  const size_t count =
+      (size_t)obstacle->SDF_dim_x * obstacle->SDF_dim_y * obstacle->SDF_dim_z;
+  if (count == 0) return set_error(SPHPC_EINVAL, "AllocInitObstacle_CUDA: empty SDF");
+  Obstacle_CUDA* oc = new Obstacle_CUDA{nullptr, count};
+  int rc = dalloc(&oc->sdf, count);
+  if (rc) {
+    delete oc;
+    return rc;
+  }
+  const cudaError_t e =
+      cudaMemcpy(oc->sdf, obstacle->SDF_buffer, count * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    dfree(oc->sdf);
+    delete oc;
+    return set_error(SPHPC_ECUDA, "SDF upload: %s", cudaGetErrorString(e));
+  }
+  obstacle->obstacle_cuda = oc;
+  return SPHPC_OK;
+}
+
+int FinalizeObstacle_CUDA(struct Obstacle_CUDA* obstacle_cuda) {
+  if (!obstacle_cuda) return SPHPC_OK;
+  dfree(obstacle_cuda->sdf);
+  delete obstacle_cuda;
+  return SPHPC_OK;
+}
+
+int AllocInitObstacle(struct Obstacle* obstacle) {
+  clear_error();
+  if (!obstacle) return set_error(SPHPC_EINVAL, "AllocInitObstacle: null");
+  SPHPC_RC(sphpc_read_sdf(obstacle));
+  return AllocInitObstacle_CUDA(obstacle);
+}
+
+int FinalizeObstacle(struct Obstacle* obstacle) {
+  if (!obstacle) return SPHPC_OK;
+  FinalizeObstacle_CUDA(obstacle->obstacle_cuda);
+  obstacle->obstacle_cuda = nullptr;
+  free(obstacle->SDF_buffer);
+  obstacle->SDF_buffer = nullptr;
+  return SPHPC_OK;
+}
+
+int CalculateParticleCollisions(double* x, double* y, double* z, const int particle_count,
+                                const struct Obstacle obstacle) {
+  if (particle_count <= 0) return SPHPC_OK;
+  if (!obstacle.obstacle_cuda)
+    return set_error(SPHPC_ENOTREADY, "CalculateParticleCollisions: obstacle not uploaded");
+  DeviceSim tmp;
+  tmp.n = particle_count;
+  Params prm{};
+  prm.smoothing_radius = 1.0;
+  prm.time_step = 1.0;
+  const DevParams P = tmp.params(prm, nullptr, &obstacle);
+  tmp.n = 0;
+  launch_collisions_double(P, x, y, z, particle_count, 0);
+  SPHPC_CK(cudaGetLastError());
+  return SPHPC_OK;
+}
+
+// ---- Thrust seam ----
+
+static int seam_scratch(int count, SortScratch* out) {
+  int dev = 0;
+  SPHPC_CK(cudaGetDevice(&dev));
+  SeamScratch& sc = g_seam[dev];
+  if (sc.cap < count) {
+    dfree(sc.s.keys_alt);
+    dfree(sc.s.vals_alt);
+    dfree(sc.aux);
+    sc.cap = 0;
+    SPHPC_RC(dalloc(&sc.s.keys_alt, (size_t)count));
+    SPHPC_RC(dalloc(&sc.s.vals_alt, (size_t)count));
+    const size_t aux = sort_aux_words(count) + 4;
+    SPHPC_RC(dalloc(&sc.aux, aux));
+    SPHPC_CK(cudaMemset(sc.aux, 0, aux * sizeof(uint32_t)));
+    sc.s.hist = sc.aux;
+    sc.s.counters = sc.aux + (size_t)kMaxPasses * kRadix;
+    sc.s.err = sc.aux + (size_t)kMaxPasses * kRadix + kMaxPasses;
+    sc.s.lookback = sc.aux + (size_t)kMaxPasses * kRadix + kMaxPasses + 4;
+    sc.cap = count;
+  }
+  *out = sc.s;
+  return SPHPC_OK;
+}
+
+int SortByKey(unsigned int* const keys, unsigned int* const values, const int count,
+              const void* const cuda_stream) {
+  if (count < 0 || (count > 0 && (!keys || !values)))
+    return set_error(SPHPC_EINVAL, "SortByKey: bad arguments");
+  if (count <= 1) return SPHPC_OK;
+  std::lock_guard<std::mutex> lk(g_seam_mu);
+  SortScratch sc;
+  SPHPC_RC(seam_scratch(count, &sc));
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  const cudaError_t e = radix_sort_pairs(keys, values, count, kMaxPasses, sc, st, false, false,
+                                         true, nullptr, nullptr);
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "SortByKey: %s", cudaGetErrorString(e));
+  // the scratch is shared by every caller: finish before releasing it
+  SPHPC_CK(cudaStreamSynchronize(st));
+  uint32_t herr = 0;
+  SPHPC_CK(cudaMemcpy(&herr, sc.err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (herr) {
+    cudaMemset(sc.err, 0, sizeof(uint32_t));
+    return set_error(SPHPC_EKERNEL, "SortByKey: look-back wait gave up (error bits 0x%x)", herr);
+  }
+  return SPHPC_OK;
+}
+
+int FindLowerBounds(const unsigned int* const hash_values, const int value_count,
+                    const int search_count, unsigned int* const start_indices,
+                    const void* const cuda_stream) {
+  if (value_count < 0 || search_count < 0)
+    return set_error(SPHPC_EINVAL, "FindLowerBounds: negative count");
+  const cudaError_t e = launch_bounds(hash_values, value_count, search_count, start_indices,
+                                      false, (cudaStream_t)cuda_stream);
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "FindLowerBounds: %s", cudaGetErrorString(e));
+  return SPHPC_OK;
+}
+
+int FindUpperBounds(const unsigned int* const hash_values, const int value_count,
+                    const int search_count, unsigned int* const end_indices,
+                    const void* const cuda_stream) {
+  if (value_count < 0 || search_count < 0)
+    return set_error(SPHPC_EINVAL, "FindUpperBounds: negative count");
+  const cudaError_t e = launch_bounds(hash_values, value_count, search_count, end_indices, true,
+                                      (cudaStream_t)cuda_stream);
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "FindUpperBounds: %s", cudaGetErrorString(e));
+  return SPHPC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,244 @@
+// sphpc_dev.cuh -- device-side layout, parameters and shared primitives of
+// the B200 PBF pipeline.
+//
+// State layout in HBM (slot order = particles sorted by uniform-grid cell
+// key, rebuilt every step):
+//   pos[n]   float4  x, the step-start position (.w unused)
+//   disp[n]  float4  d = x* - x, the predicted-position displacement.
+//                    .w carries lambda after the density/lambda pass and the
+//                    density after the position pass.
+//   vel[n]   float4  v
+//   ids[n]   u32     original particle index of each slot
+//   cellp[n] u32     packed grid cell (cx | cy<<bx | cz<<(bx+by)) of x* at
+//                    neighbour-build time; bit 31 = explicit neighbour list
+//   mask[kMaskWords][n] u32  neighbour bitmask over the candidate sequence
+//                    (see for_each_neighbor)
+//   cstart[C+1] u32  start slot of every cell (lower bound), cstart[C] = n
+//
+// The canonical predicted position is the double fl64(x + d): the hash, the
+// neighbour test, the box clamp and the SDF lookup are evaluated on it in
+// FP64 exactly as the reference evaluates its double x_star; pair
+// differences inside the neighbour sums are (x_p - x_q) + (d_p - d_q) in
+// FP32, which keeps relative precision at any box size.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sphpc {
+
+constexpr int kMaxNeighbors = 60;   // MAX_NEIGHBORS, neighbors.h:6
+constexpr int kMaskWords = 16;      // bitmask capacity: 512 candidates
+constexpr int kExplicitStride = kMaxNeighbors + 1;  // [count, slot...]
+constexpr uint32_t kExplicitFlag = 0x80000000u;
+
+// Error bits raised by kernels (host reads them back).
+enum : uint32_t {
+  kErrExplicitOverflow = 1u << 0,  // explicit neighbour-list table full
+  kErrSortSpin = 1u << 1,          // radix-sort look-back wait gave up
+  kErrCellRange = 1u << 2,         // a particle hashed outside the grid
+  kErrScanSpin = 1u << 3,
+};
+
+struct DevParams {
+  int n;
+  int nx, ny, nz;
+  uint32_t nxny;
+  uint32_t ncells;      // C = nx*ny*nz
+  int bx, by;           // packed-cell bit widths of x and y
+  uint32_t mx, my;      // masks for cx and cy
+  double hd;            // smoothing radius (double)
+  double h2d;
+  float h, h2;
+  float rmin;           // r floor 1e-4 h (particles.c:636)
+  // smoothing-kernel constants; *_m variants carry the particle mass
+  float W0m;            // m * W(0)
+  float Wn, Wn_m;       // poly6 norm
+  float DWn, DWn_m;     // spiky gradient norm
+  float DWPn;           // poly6 gradient norm
+  float m, rho0, inv_rho0, inv_rho0_sq;
+  float lambda_eps;
+  float scorr_k;        // s_corr = -k (W/W(dq))^n
+  int scorr_n;
+  float inv_Wdq;
+  float c_xsph;
+  int xsph_exact;       // 0: reference r expression (particles.c:439)
+  float gamma, C_norm;  // surface tension
+  float vort_eps;
+  float dt, inv_dt, v_max;
+  double dt_d, gdt_d;   // gravity increment (-g*dt) in double
+  int gaxis;
+  float gdt_f;
+  double bmin[3], bmax[3], bmax_eps[3];  // clamp (particles.c:842-867)
+  // obstacle SDF (x fastest), tex3D-style sampling
+  int has_sdf;
+  int sdim[3];
+  const float* sdf;
+  double ob_min[3], ob_max[3];
+  float ob_len[3];      // world extents as float (obstacle_cuda.cu:74-85)
+  float tex_sp[3];      // 1/dim in normalised coordinates
+  float model_to_world;
+};
+
+// View of the per-step neighbour structure.
+struct NbrView {
+  const uint32_t* __restrict__ cellp;
+  const uint32_t* __restrict__ mask;
+  const uint32_t* __restrict__ explist;
+  const uint32_t* __restrict__ cstart;
+  int n;
+  int nx, ny, nz;
+  uint32_t nxny;
+  int bx, by;
+  uint32_t mx, my;
+};
+
+__device__ __forceinline__ void unpack_cell(const NbrView& v, uint32_t cp, int& cx,
+                                            int& cy, int& cz) {
+  cp &= ~kExplicitFlag;
+  cx = (int)(cp & v.mx);
+  cy = (int)((cp >> v.bx) & v.my);
+  cz = (int)(cp >> (v.bx + v.by));
+}
+
+// Visits the neighbour slots of particle p in the reference's bucket order
+// (FillNeighbors, neighbors.c:247-295: dz, dy, dx, then ascending sorted
+// index).  For a regular particle the candidates of each (dz, dy) row are
+// the contiguous slot range of cells cx-1..cx+1, and the candidate sequence
+// is the concatenation of the valid rows; bit k of the mask marks candidate
+// k as a neighbour.  Particles whose neighbour cells are not cx-1..cx+1
+// (FP64 rounding at a cell face) or whose candidates exceed the mask carry an
+// explicit list instead.
+template <class F>
+__device__ __forceinline__ void for_each_neighbor(const NbrView& v, int p, F&& f) {
+  const uint32_t cp = __ldg(v.cellp + p);
+  if (cp & kExplicitFlag) {
+    const uint32_t idx = __ldg(v.mask + p);
+    const uint32_t* lst = v.explist + (size_t)idx * kExplicitStride;
+    const int cnt = (int)__ldg(lst);
+    for (int j = 0; j < cnt; ++j) f((int)__ldg(lst + 1 + j));
+    return;
+  }
+  int cx, cy, cz;
+  unpack_cell(v, cp, cx, cy, cz);
+  const int xlo = cx - (cx > 0);
+  const int xhi = cx + (cx < v.nx - 1);
+  int base = 0;  // candidate index of the first slot of the current row
+  int cur_w = -1;
+  uint32_t cur_word = 0;
+#pragma unroll 1
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = cz + dz;
+    if ((unsigned)z >= (unsigned)v.nz) continue;
+#pragma unroll 1
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = cy + dy;
+      if ((unsigned)y >= (unsigned)v.ny) continue;
+      const uint32_t rk = (uint32_t)z * v.nxny + (uint32_t)y * (uint32_t)v.nx;
+      const int b = (int)__ldg(v.cstart + rk + xlo);
+      const int e = (int)__ldg(v.cstart + rk + xhi + 1);
+      const int end = base + (e - b);
+      int pos = base;
+#pragma unroll 1
+      while (pos < end) {
+        const int w = pos >> 5;
+        if (w != cur_w) {
+          cur_w = w;
+          cur_word = __ldg(v.mask + (size_t)w * v.n + p);
+        }
+        const int sh = pos & 31;
+        const int take = min(32 - sh, end - pos);
+        uint32_t bits = cur_word >> sh;
+        if (take < 32) bits &= (1u << take) - 1u;
+        const int slot0 = b + (pos - base);
+        while (bits) {
+          const int k = __ffs(bits) - 1;
+          bits &= bits - 1u;
+          f(slot0 + k);
+        }
+        pos += take;
+      }
+      base = end;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Canonical double predicted position and the reference's box clamp.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double xstar_d(float x, float d) {
+  return __dadd_rn((double)x, (double)d);
+}
+
+// ApplyBoundaryConditions, particles.c:842-867, on one axis.
+__device__ __forceinline__ double clamp_axis(double x, double lo, double hi,
+                                             double hi_eps) {
+  if (x < lo) return lo;
+  if (x >= hi) return hi_eps;
+  return x;
+}
+
+// HashVal, neighbors.c:79-98, per axis: floor(x / spacing) in FP64.
+__device__ __forceinline__ int grid_coord(double x, double h) {
+  return (int)(unsigned)floor(__ddiv_rn(x, h));
+}
+
+// ---------------------------------------------------------------------------
+// SDF obstacle: tex3D<float> (linear filter, clamp addressing, normalised
+// coordinates; obstacle_cuda.cu:166-181) with exact FP32 weights.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sdf_texel(const DevParams& P, int i, int j, int k) {
+  i = min(max(i, 0), P.sdim[0] - 1);
+  j = min(max(j, 0), P.sdim[1] - 1);
+  k = min(max(k, 0), P.sdim[2] - 1);
+  return __ldg(P.sdf + ((size_t)k * P.sdim[1] + j) * P.sdim[0] + i);
+}
+
+__device__ __forceinline__ float lerp_rn(float a, float b, float t) {
+  return __fmaf_rn(t, __fsub_rn(b, a), a);
+}
+
+__device__ __forceinline__ float sdf_sample(const DevParams& P, float u, float v, float w) {
+  const float xb = __fsub_rn(__fmul_rn(u, (float)P.sdim[0]), 0.5f);
+  const float yb = __fsub_rn(__fmul_rn(v, (float)P.sdim[1]), 0.5f);
+  const float zb = __fsub_rn(__fmul_rn(w, (float)P.sdim[2]), 0.5f);
+  const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
+  const float ax = __fsub_rn(xb, fx), ay = __fsub_rn(yb, fy), az = __fsub_rn(zb, fz);
+  const int i = (int)fx, j = (int)fy, k = (int)fz;
+  const float c00 = lerp_rn(sdf_texel(P, i, j, k), sdf_texel(P, i + 1, j, k), ax);
+  const float c10 = lerp_rn(sdf_texel(P, i, j + 1, k), sdf_texel(P, i + 1, j + 1, k), ax);
+  const float c01 = lerp_rn(sdf_texel(P, i, j, k + 1), sdf_texel(P, i + 1, j, k + 1), ax);
+  const float c11 = lerp_rn(sdf_texel(P, i, j + 1, k + 1), sdf_texel(P, i + 1, j + 1, k + 1), ax);
+  const float c0 = lerp_rn(c00, c10, ay);
+  const float c1 = lerp_rn(c01, c11, ay);
+  return lerp_rn(c0, c1, az);
+}
+
+// CalculateParticleCollisions_kernel body (obstacle_cuda.cu:62-115) on one
+// double position.  Returns true and updates xyz when the particle is pushed.
+__device__ __forceinline__ bool sdf_collide(const DevParams& P, double& x, double& y,
+                                            double& z) {
+  if (!(x > P.ob_min[0] && x < P.ob_max[0] && y > P.ob_min[1] && y < P.ob_max[1] &&
+        z > P.ob_min[2] && z < P.ob_max[2]))
+    return false;
+  const float xt = (float)__ddiv_rn(__dsub_rn(x, P.ob_min[0]), (double)P.ob_len[0]);
+  const float yt = (float)__ddiv_rn(__dsub_rn(y, P.ob_min[1]), (double)P.ob_len[1]);
+  const float zt = (float)__ddiv_rn(__dsub_rn(z, P.ob_min[2]), (double)P.ob_len[2]);
+  const float dist = sdf_sample(P, xt, yt, zt);
+  if (!(dist < 0.0f)) return false;
+  const float gx = __fsub_rn(sdf_sample(P, __fadd_rn(xt, P.tex_sp[0]), yt, zt),
+                             sdf_sample(P, __fsub_rn(xt, P.tex_sp[0]), yt, zt));
+  const float gy = __fsub_rn(sdf_sample(P, xt, __fadd_rn(yt, P.tex_sp[1]), zt),
+                             sdf_sample(P, xt, __fsub_rn(yt, P.tex_sp[1]), zt));
+  const float gz = __fsub_rn(sdf_sample(P, xt, yt, __fadd_rn(zt, P.tex_sp[2])),
+                             sdf_sample(P, xt, yt, __fsub_rn(zt, P.tex_sp[2])));
+  const float dot = __fadd_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)),
+                              __fmul_rn(gz, gz));
+  const float inv = __fdiv_rn(1.0f, __fsqrt_rn(dot));
+  const float dw = __fmul_rn(fabsf(dist), P.model_to_world);
+  y = __dadd_rn(y, (double)__fmul_rn(dw, __fmul_rn(gy, inv)));
+  x = __dadd_rn(x, (double)__fmul_rn(dw, __fmul_rn(gx, inv)));
+  z = __dadd_rn(z, (double)__fmul_rn(dw, __fmul_rn(gz, inv)));
+  return true;
+}
+
+}  // namespace sphpc

@@ -1,0 +1,198 @@
+"""Python host driver over the C ABI, mirroring the reference's main()
+(Simulation/src/simulation.c:19-128): load the configuration, allocate and
+initialise particles, neighbours and obstacle, then step.
+
+Every call goes through libsphpc_cuda.so; host arrays are the reference's
+FP64 SoA in original particle order (numpy views of the C arrays).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import (AABB, Diag, KernelTime, Neighbors, Obstacle, Params, Particles, Solver,
+                   PARTICLE_FIELDS, call, load)
+from .scenes import config_path
+
+
+class Simulation:
+    """One particle set on the device.
+
+    ``solver_overrides`` replaces fields of the configuration's solver
+    settings (struct SphpcSolver) before the particles are created.
+    """
+
+    def __init__(self, config: str, solver_overrides: dict | None = None,
+                 obstacle: bool = True):
+        self.lib = load()
+        self.path = config_path(config)
+        self.params = Params()
+        self.particles = Particles()
+        self.boundary = AABB()
+        self.fluid = AABB()
+        self.obstacle = Obstacle()
+        self.neighbors = Neighbors()
+        self.solver = Solver()
+        call("sphpc_load_config", self.path.encode(), C.byref(self.params),
+             C.byref(self.particles), C.byref(self.boundary), C.byref(self.fluid),
+             C.byref(self.obstacle), C.byref(self.solver))
+        for k, v in (solver_overrides or {}).items():
+            setattr(self.solver, k, v)
+        self.lib.sphpc_set_default_solver(C.byref(self.solver))
+        call("SetParticleNumbers", C.byref(self.fluid), C.byref(self.particles),
+             C.byref(self.params), None)
+        call("AllocInitParticles", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.fluid))
+        self._alive = True
+        call("sphpc_set_solver", C.byref(self.particles), C.byref(self.solver))
+        call("AllocInitNeighbors", C.byref(self.neighbors), C.byref(self.particles),
+             C.byref(self.params), C.byref(self.boundary))
+        self.has_obstacle = bool(obstacle and self.obstacle.SDF_file_name)
+        if self.has_obstacle:
+            call("AllocInitObstacle", C.byref(self.obstacle))
+        self.n = self.particles.local_count
+
+    # ---------------- lifetime ----------------
+    def close(self):
+        if getattr(self, "_alive", False):
+            if self.has_obstacle:
+                self.lib.FinalizeObstacle(C.byref(self.obstacle))
+            self.lib.FinalizeNeighbors(C.byref(self.neighbors))
+            self.lib.FinalizeParticles(C.byref(self.particles))
+            self._alive = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---------------- host arrays ----------------
+    def host(self, field: str) -> np.ndarray:
+        """numpy view of a host array of struct Particles (FP64, original order)."""
+        ptr = getattr(self.particles, field)
+        return np.ctypeslib.as_array(ptr, shape=(self.particles.max_local,))[: self.n]
+
+    def fetch(self, fields=None) -> dict:
+        """Device -> host (sphpc_update_host), returns copies of the fields."""
+        call("sphpc_update_host", C.byref(self.particles))
+        fields = fields or PARTICLE_FIELDS
+        return {f: self.host(f).copy() for f in fields}
+
+    def push(self, arrays: dict | None = None):
+        """Writes `arrays` into the host arrays, then host -> device."""
+        for f, v in (arrays or {}).items():
+            self.host(f)[:] = v
+        call("sphpc_update_device", C.byref(self.particles))
+
+    def set_solver(self, **kw):
+        for k, v in kw.items():
+            setattr(self.solver, k, v)
+        call("sphpc_set_solver", C.byref(self.particles), C.byref(self.solver))
+
+    def set_stream(self, stream_ptr: int):
+        call("sphpc_set_stream", C.byref(self.particles), C.c_void_p(stream_ptr))
+
+    # ---------------- stepping ----------------
+    def _ob(self):
+        return C.byref(self.obstacle) if self.has_obstacle else None
+
+    def step(self, steps: int = 1):
+        call("sphpc_step", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.neighbors), C.byref(self.boundary), self._ob(), steps)
+
+    def diagnostics(self) -> dict:
+        d = Diag()
+        call("sphpc_diagnostics", C.byref(self.particles), C.byref(d))
+        return d.as_dict()
+
+    def device_errors(self) -> int:
+        bits = C.c_uint(0)
+        call("sphpc_device_errors", C.byref(self.particles), C.byref(bits))
+        return bits.value
+
+    def profile(self, enable: bool = True):
+        call("sphpc_profile", C.byref(self.particles), 1 if enable else 0)
+
+    def profile_read(self) -> dict:
+        buf = (KernelTime * 64)()
+        n = C.c_int(0)
+        call("sphpc_profile_read", C.byref(self.particles), buf, 64, C.byref(n))
+        return {buf[i].name.decode(): (buf[i].launches, buf[i].total_ms)
+                for i in range(min(n.value, 64))}
+
+    # reference-named stages (particles.h / neighbors.h), one device stage each
+    def apply_gravity(self):
+        call("ApplyGravity", C.byref(self.particles), C.byref(self.params))
+
+    def predict_positions(self):
+        call("PredictPositions", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.boundary))
+
+    def find_all_neighbors(self):
+        call("FindAllNeighbors", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.neighbors))
+
+    def compute_densities(self):
+        call("ComputeDensities", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.neighbors))
+
+    def compute_lambda(self):
+        call("ComputeLambda", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.neighbors))
+
+    def update_dps(self, substep: int):
+        call("UpdateDPs", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.neighbors), substep)
+
+    def update_position_stars(self):
+        call("UpdatePositionStars", C.byref(self.particles), C.byref(self.boundary),
+             self._ob(), C.byref(self.params))
+
+    def update_velocities(self):
+        call("UpdateVelocities", C.byref(self.particles), C.byref(self.params))
+
+    def surface_tension(self):
+        call("ComputeSurfaceTension", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.neighbors))
+
+    def apply_viscosity(self):
+        call("ApplyViscosity", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.neighbors))
+
+    def compute_vorticity(self):
+        call("ComputeVorticity", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.neighbors))
+
+    def vorticity_confinement(self):
+        call("ApplyVorticityConfinement", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.neighbors))
+
+    def update_positions(self):
+        call("UpdatePositions", C.byref(self.particles))
+
+    def neighbor_buckets(self):
+        idx = np.zeros(self.n * _lib.MAX_NEIGHBORS, np.uint32)
+        cnt = np.zeros(self.n, np.int32)
+        call("sphpc_get_neighbor_buckets", C.byref(self.particles),
+             idx.ctypes.data_as(C.POINTER(C.c_uint)), cnt.ctypes.data_as(C.POINTER(C.c_int)))
+        return cnt, idx.reshape(self.n, _lib.MAX_NEIGHBORS)
+
+    def cell_data(self):
+        nx, ny, nz = (self.neighbors.hash_size_x, self.neighbors.hash_size_y,
+                      self.neighbors.hash_size_z)
+        keys = np.zeros(self.n, np.uint32)
+        ids = np.zeros(self.n, np.uint32)
+        start = np.zeros(nx * ny * nz + 1, np.uint32)
+        P = C.POINTER(C.c_uint)
+        call("sphpc_get_cell_data", C.byref(self.particles), keys.ctypes.data_as(P),
+             ids.ctypes.data_as(P), start.ctypes.data_as(P))
+        return keys, ids, start
