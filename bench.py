@@ -1,0 +1,399 @@
+#!/usr/bin/env python3
+"""Benchmark of the PBF particle pipeline: particle-steps per second on
+B200, with the constraint solve iterated until the FP64 max density error is
+at most 1% (or the iteration cap).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME]
+    python bench.py --impl reference ...   # the reference's own CPU code
+
+One JSON line on stdout (rank 0).  Workload: the 16,777,216-particle full
+pipeline scene (configs/full_16m.ini) unless --config says otherwise.  With
+N > 1 every rank runs its own replica (the reference path is single rank:
+no halo exchange), and `value` is the aggregate over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/sec at max density err <=1%: MLP warm-start vs plain, 1 B200"
+UNIT = "particle-steps/s"
+
+# Algorithmic (compulsory) HBM bytes per particle of each stage for this
+# layout: each particle's own records read/written once, neighbour data
+# assumed cache-resident.  mask = ~7 words of candidate bitmask.
+MASK_B = 28
+STAGE_BYTES = {
+    "hash": 32 + 8,                         # x, v in; key, slot scattered out
+    "radix_sort": None,                     # 16 B per digit pass (+4 hist), set below
+    "cell_starts": 4,                       # + 4 per cell, added below
+    "reorder": 4 + 4 + 32 + 32 + 4,         # ids, loc, x+v in, x+d out, cell
+    "build_neighbors": 32 + 4 + MASK_B + 1,
+    "density_lambda": 32 + 4 + MASK_B + 16 + 4,
+    "position": 32 + 4 + MASK_B + 4 + 16,
+    "surface_tension": 2 * (32 + 4 + MASK_B) + 16 + 16 + 16,
+    "xsph": 32 + 16 + 4 + MASK_B + 16,
+    "vorticity": 2 * (32 + 4 + MASK_B) + 16 + 16 + 16 + 16,
+    "velocity": 16 + 16,
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+# --------------------------------------------------------------------------
+# CPU reference (the reference's own particles.c / neighbors.c)
+# --------------------------------------------------------------------------
+
+def reference_sample(config_name, iterations, target_s=12.0, max_steps=50, warmup=1,
+                     lattice=(32, 32, 32)):
+    """Times the reference's CPU path (oracle/_ref, -O3) on a bounded sample of
+    the workload: a 32^3 block of the configuration's lattice with its h,
+    dt, box and obstacle.  Returns particle-steps/s and a description."""
+    from oracle.pyoracle import RefSim, scene_from_ini
+    from sphpc_b200.scenes import config_path
+    sc = scene_from_ini(config_path(config_name))
+    nl = sc.meta["lattice"]
+    keep = []
+    # first lattice[0] x lattice[1] x lattice[2] sub-block of the lattice
+    for iz in range(min(lattice[2], nl[2])):
+        for iy in range(min(lattice[1], nl[1])):
+            base = (iz * nl[1] + iy) * nl[0]
+            keep.extend(range(base, base + min(lattice[0], nl[0])))
+    keep = np.array(keep)
+    sc.x0 = np.ascontiguousarray(sc.x0[:, keep])
+    ref = RefSim(sc, fast=True)
+    for _ in range(warmup):
+        ref.step(1, iterations)
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps:
+        ref.step(1, iterations)
+        steps += 1
+        if time.perf_counter() - t0 > target_s:
+            break
+    dt = time.perf_counter() - t0
+    return sc.n * steps / dt, {
+        "sample": f"{sc.n} particles ({'x'.join(map(str, lattice))} block of {config_name}), "
+                  f"{steps} steps x {iterations} iterations, {dt:.1f} s",
+        "cores": 1, "kind": "reference"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    steps_done, t_all = 0, 0.0
+    from oracle.pyoracle import RefSim  # noqa: F401  (fails loudly if not built)
+    iters = args.ref_iterations
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, info = reference_sample(args.config, iters, target_s=args.ref_seconds, max_steps=3,
+                                   warmup=0)
+        if k >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.config, "sample": info["sample"],
+                   "iterations_per_step": iters},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": info["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# Our arm
+# --------------------------------------------------------------------------
+
+def run_ours(args, world, rank, local, dist):
+    import torch
+    from sphpc_b200 import Simulation
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    overrides = {"adaptive": 1, "density_tolerance": args.tol,
+                 "max_iterations": args.max_iters}
+    if args.fixed:
+        overrides = {"adaptive": 0}
+    t_init = time.perf_counter()
+    sim = Simulation(args.config, solver_overrides=overrides)
+    stream = torch.cuda.current_stream(dev)
+    sim.set_stream(stream.cuda_stream)
+    n = sim.n
+    log(f"[rank {rank}] {args.config}: {n} particles, init {time.perf_counter()-t_init:.1f}s")
+    for _ in range(args.warmup):
+        sim.step(1)
+    torch.cuda.synchronize()
+    it_before = sim.diagnostics()
+    launches0 = sim.launches()
+    iters = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    conv = 0
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            sim.step(1)
+            if not args.fixed:
+                d = sim.last_step_info()
+                iters.append(d["iterations"])
+                conv += d["converged"]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = sim.launches() - launches0
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * n * args.steps / (ms_max / 1e3)
+    errs = sim.device_errors()
+    if errs:
+        raise RuntimeError(f"device error bits 0x{errs:x} during the timed region")
+    diag = sim.diagnostics()
+
+    # per-stage CUDA-event profile of two more steps (not part of the timed value)
+    sim.profile(True)
+    sim.step(2)
+    prof = sim.profile_read()
+    sim.profile(False)
+    prof.pop("kernel_launches", None)
+
+    roof = None
+    if prof:
+        name, (cnt, tot) = max(prof.items(), key=lambda kv: kv[1][1])
+        per = STAGE_BYTES.get(name)
+        if name == "radix_sort":
+            per = 16 * sim_passes(sim)
+        if name == "cell_starts":
+            per = 4
+        if per is not None and cnt:
+            avg_s = tot / cnt / 1e3
+            bytes_launch = per * n
+            peak, kind = peaks()
+            achieved = bytes_launch / avg_s / 1e9
+            roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak,
+                    "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": ncu_traffic(name, n), "bytes_per_particle": per,
+                    "avg_launch_ms": tot / cnt}
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(sim, args, dist, world, n)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, info = reference_sample(args.config, args.ref_iterations,
+                                       target_s=args.ref_seconds, max_steps=20)
+            cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                   "sample": info["sample"]}
+        except Exception as e:  # the checker is optional on a box without it
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+    sim.close()
+    if rank != 0:
+        return
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic",
+        "config": {"workload": args.config, "particles_per_gpu": n,
+                   "solver": "fixed iterations" if args.fixed else
+                   f"plain, iterate to max density err <= {args.tol} (cap {args.max_iters})",
+                   "mean_iterations": float(np.mean(iters)) if iters else None,
+                   "steps_converged": conv if iters else None,
+                   "l2": "state larger than L2 (no flush)",
+                   "final_max_density_error": diag["max_density_error"],
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "roofline": roof,
+        "stage_ms_per_step": {k: v[1] / 2 for k, v in prof.items()},
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def sim_passes(sim):
+    C_ = sim.neighbors.hash_size_x * sim.neighbors.hash_size_y * sim.neighbors.hash_size_z
+    bits = max(1, int(C_ - 1).bit_length())
+    return (bits + 7) // 8
+
+
+def ncu_traffic(stage, n):
+    """DRAM bytes per launch of `stage` from the committed ncu summary, scaled
+    to n particles (profiles/ncu_traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        e = d[stage]
+        return e["bytes_per_particle"] * n
+    except Exception:
+        return None
+
+
+def run_e2e(sim, args, dist, world, n):
+    """Host buffers in, host buffers out, through the public C API: upload the
+    state from the host arrays (x, v), K steps each followed by the FP64
+    diagnostics read-back, the reference's output frame (x, y, z, density
+    every 1/(30 dt) steps, simulation.c:113-114), and the final state."""
+    import torch
+    fields_in = ["x", "y", "z", "v_x", "v_y", "v_z"]
+    frame_fields = ["x", "y", "z", "density"]
+    out_fields = ["x", "y", "z", "v_x", "v_y", "v_z", "density"]
+    frame_every = max(1, int(1.0 / (sim.params.time_step * 30.0)))
+    sim.fetch_fields(fields_in)  # host arrays hold a valid state
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.push_fields(fields_in)
+    frames = 0
+    for k in range(args.steps):
+        sim.step(1)
+        sim.diagnostics()
+        if k % frame_every == 0:
+            sim.fetch_fields(frame_fields)
+            frames += 1
+    sim.fetch_fields(out_fields)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dt = float(t.item())
+    h2d = 8 * len(fields_in) * n
+    d2h = args.steps * 72 + frames * 8 * len(frame_fields) * n + 8 * len(out_fields) * n
+    return {"value": world * n * args.steps / dt, "unit": UNIT,
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+            "host_memory": "pageable (the reference's calloc'd arrays)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="full_16m")
+    ap.add_argument("--tol", type=float, default=0.01)
+    ap.add_argument("--max-iters", type=int, default=12)
+    ap.add_argument("--fixed", action="store_true", help="configured iteration count")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-iterations", type=int, default=6)
+    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    args = ap.parse_args()
+    world, rank, local, dist = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -85,6 +85,14 @@ int FinalizeParticles(struct Particles *particles);
 int sphpc_enter_data(struct Particles *particles, const struct Params *params);
 int sphpc_exit_data(struct Particles *particles);
 int sphpc_update_host(struct Particles *particles);    /* device -> host, all fields */
+/* Selected fields only: bit k of field_mask is the k-th double array of
+ * struct Particles (0 x_star ... 3 x, 4 y, 5 z ... 18 density, 19 lambda),
+ * e.g. (1<<3)|(1<<4)|(1<<5)|(1<<18) for the output frame of
+ * fileio_adios.c:73-76. */
+int sphpc_update_host_fields(struct Particles *particles, unsigned int field_mask);
+/* Host -> device of selected field groups (same bit numbering; a group
+ * such as x/y/z is uploaded when all its bits are set; x/y/z are required). */
+int sphpc_update_device_fields(struct Particles *particles, unsigned int field_mask);
 int sphpc_update_device(struct Particles *particles);  /* host -> device, all fields */
 /* Solver settings of this particle set (copied). */
 int sphpc_set_solver(struct Particles *particles, const struct SphpcSolver *solver);
@@ -157,10 +165,14 @@ int sphpc_step(struct Particles *particles, const struct Params *params,
 /* FP64 diagnostics of the device copy (density error from the last density
  * evaluation, energy, centre of mass, momentum). */
 int sphpc_diagnostics(const struct Particles *particles, struct SphpcDiag *diag);
+/* Iterations, convergence and residual of the last sphpc_step. */
+int sphpc_step_info(const struct Particles *particles, struct SphpcStepInfo *info);
 /* Kernel-reported error bits since the last call (0 = none); clears them. */
 int sphpc_device_errors(const struct Particles *particles, unsigned int *bits);
 
-/* Per-kernel CUDA-event timing of the particle set's launches. */
+/* Per-stage CUDA-event timing of the particle set's launches.  The last
+ * entry sphpc_profile_read returns is "kernel_launches": the number of
+ * kernels the particle set has launched in total (its launches field). */
 int sphpc_profile(struct Particles *particles, int enable);
 int sphpc_profile_read(const struct Particles *particles, struct SphpcKernelTime *out,
                        int max_entries, int *n_entries);

@@ -166,6 +166,16 @@ struct SphpcDiag {
   double warm_start_used;     /* 1 if the last step used the MLP start */
 };
 
+/* Host-side record of the last sphpc_step (no device work to read it). */
+struct SphpcStepInfo {
+  int iterations;             /* constraint iterations run (warm start counts 1) */
+  int converged;              /* adaptive: max density error reached tolerance */
+  int warm_start_used;
+  int pad;
+  double max_density_error;   /* FP64, at the last density evaluation */
+  double mean_density_error;
+};
+
 /* Per-kernel device time collected with CUDA events (sphpc_profile). */
 struct SphpcKernelTime {
   char name[32];

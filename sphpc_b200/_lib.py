@@ -92,6 +92,12 @@ class Diag(C.Structure):
                 "warm_start_used": self.warm_start_used}
 
 
+class StepInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int),
+                ("warm_start_used", C.c_int), ("pad", C.c_int),
+                ("max_density_error", C.c_double), ("mean_density_error", C.c_double)]
+
+
 class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("pad", C.c_int),
                 ("total_ms", C.c_double)]
@@ -124,6 +130,8 @@ SIGNATURES = {
     "sphpc_exit_data": ([PP], C.c_int),
     "sphpc_update_host": ([PP], C.c_int),
     "sphpc_update_device": ([PP], C.c_int),
+    "sphpc_update_host_fields": ([PP, C.c_uint], C.c_int),
+    "sphpc_update_device_fields": ([PP, C.c_uint], C.c_int),
     "sphpc_set_solver": ([PP, C.POINTER(Solver)], C.c_int),
     "sphpc_get_solver": ([PP, C.POINTER(Solver)], C.c_int),
     "sphpc_set_stream": ([PP, C.c_void_p], C.c_int),
@@ -150,6 +158,7 @@ SIGNATURES = {
     "sphpc_step": ([PP, P, PN, PA, PO, C.c_int], C.c_int),
     "sphpc_diagnostics": ([PP, C.POINTER(Diag)], C.c_int),
     "sphpc_device_errors": ([PP, U], C.c_int),
+    "sphpc_step_info": ([PP, C.POINTER(StepInfo)], C.c_int),
     "sphpc_profile": ([PP, C.c_int], C.c_int),
     "sphpc_profile_read": ([PP, C.POINTER(KernelTime), C.c_int, C.POINTER(C.c_int)], C.c_int),
     "SortByKey": ([U, U, C.c_int, C.c_void_p], C.c_int),

@@ -95,7 +95,8 @@ __global__ void __launch_bounds__(kBlock)
     if (MODE == 2) rho = a.rho[p];
     if (MODE != 2) a.rho[p] = rho;
     if (MODE != 1) {
-      const float C = fmaxf(__fdiv_rn(rho, P.rho0) - 1.0f, 0.0f);
+      // ComputeLambda's constraint (particles.c:616-617) in FP64
+      const float C = (float)fmax(__ddiv_rn((double)rho, P.rho0_d) - 1.0, 0.0);
       sC += sgx * sgx + sgy * sgy + sgz * sgz;
       sC *= P.inv_rho0_sq;
       const float lam = -C / (sC + P.lambda_eps);

@@ -182,8 +182,12 @@ __global__ void __launch_bounds__(kSortThreads)
     const uint32_t kk = s_keys[k];
     const uint32_t d = (kk >> shift) & (kRadix - 1);
     const uint32_t g = s_gbase[d] + (uint32_t)k - s_dstart[d];
-    keys_out[g] = kk;
-    vals_out[g] = s_vals[k];
+    if (g < (uint32_t)n) {
+      keys_out[g] = kk;
+      vals_out[g] = s_vals[k];
+    } else {
+      atomicOr(err, 4u);  // inconsistent digit counts: never write out of range
+    }
   }
 }
 

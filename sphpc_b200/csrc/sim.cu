@@ -102,9 +102,11 @@ class DeviceSim {
 
   MlpState mlp{};
 
+  unsigned long long launches = 0;  // kernels launched by this particle set
   double last_iterations = 0.0;
   double last_warm = 0.0;
   double last_max_err = 0.0, last_mean_err = 0.0;
+  int last_converged = 0;
 
   // profiling
   bool prof = false;
@@ -332,6 +334,7 @@ DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob
   P.DWPn = (float)prm.DelW_poly_norm;
   P.m = (float)m;
   P.rho0 = (float)rho0;
+  P.rho0_d = rho0;
   P.inv_rho0 = (float)(1.0 / rho0);
   P.inv_rho0_sq = (float)(1.0 / (rho0 * rho0));
   P.lambda_eps = (float)(solver.lambda_epsilon_mass_units
@@ -395,6 +398,7 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
     SPHPC_CK(cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * kMaxPasses * kRadix, stream));
     launch_hash(P, pos, vel, disp, ids, keys_by_id, loc_by_id, sort.hist, passes, predict, err(),
                 stream);
+    launches += 1;
   }
   uint32_t *K = nullptr, *R = nullptr;
   {
@@ -403,11 +407,13 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
                                            true, false, &K, &R);
     if (e != cudaSuccess)
       return set_error(SPHPC_ECUDA, "radix sort: %s", cudaGetErrorString(e));
+    launches += 1 + (unsigned)passes;
   }
   keys_sorted = K;
   {
     Scope sc(this, "cell_starts");
     launch_cell_starts(K, n, C, cstart, gaps, gap_count(), err(), stream);
+    launches += 2;
   }
   {
     Scope sc(this, "reorder");
@@ -423,6 +429,7 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
     const bool mv = move_vel || full;
     launch_reorder(P, R, loc_by_id, pos, vel, disp, pos_alt, vel_alt, disp_alt, cellp, predict,
                    mv, &ex, stream);
+    launches += 1;
     std::swap(pos, pos_alt);
     std::swap(disp, disp_alt);
     if (mv) std::swap(vel, vel_alt);
@@ -442,6 +449,7 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
     Scope sc(this, "build_neighbors");
     launch_build_neighbors(P, view(), pos, disp, cellp, mask, explist, exp_cap, exp_count(),
                            ncount, err(), stream);
+    launches += 1;
   }
   SPHPC_CK(cudaGetLastError());
   nbr_valid = true;
@@ -478,6 +486,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     a.stiffness = 1.0f;
     a.last = 0;
     launch_position(P, V, a, 0, stream);
+    launches += 1;
     last_warm = 1.0;
   }
   int iters = 0;
@@ -490,6 +499,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       a.disp_out = disp_alt;
       a.lam = nullptr;
       launch_density_lambda(P, V, a, 0, true, stream);
+      launches += 1;
     }
     if (adaptive) {
       double h_res[2];
@@ -510,17 +520,22 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       a.stiffness = stiffness_of(solver.stiffness_k, warm ? k + 1 : k);
       a.last = (!adaptive && k == max_iters - 1) ? 1 : 0;
       launch_position(P, V, a, 0, stream);
+      launches += 1;
     }
     ++iters;
   }
   if (adaptive || max_iters == 0) {
     // converged (or cap reached): velocities from x* and the freshest density
     Scope sc(this, "velocity");
-    if (converged) launch_pack_w(P, disp, rho, stream);
-    else if (max_iters == 0) launch_pack_w(P, disp, rho, stream);
+    if (converged || max_iters == 0) {
+      launch_pack_w(P, disp, rho, stream);
+      launches += 1;
+    }
     launch_update_velocities(P, disp, vel, stream);
+    launches += 1;
   }
   last_iterations = iters + (warm ? 1 : 0);
+  last_converged = converged ? 1 : 0;
   // post-solve passes (simulation.c:93-106)
   a.disp = disp;
   a.pos_out = pos_alt;
@@ -530,6 +545,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     launch_color(P, V, a, stream);
     a.vel = vel;
     launch_tension(P, V, a, stream);
+    launches += 2;
   }
   {
     Scope sc(this, "xsph");
@@ -537,6 +553,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     a.vel_out = vel_alt;
     a.write_pos = solver.vorticity ? 0 : 1;
     launch_xsph(P, V, a, stream);
+    launches += 1;
   }
   if (solver.vorticity) {
     Scope sc(this, "vorticity");
@@ -546,6 +563,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     launch_vorticity(P, V, a, stream);
     a.write_pos = 1;
     launch_confinement(P, V, a, stream);
+    launches += 2;
   }
   std::swap(vel, vel_alt);
   std::swap(pos, pos_alt);
@@ -749,7 +767,9 @@ int sphpc_set_stream(struct Particles* particles, void* cuda_stream) {
   return SPHPC_OK;
 }
 
-int sphpc_update_host(struct Particles* p) {
+int sphpc_update_host(struct Particles* p) { return sphpc_update_host_fields(p, 0xFFFFFFFFu); }
+
+int sphpc_update_host_fields(struct Particles* p, unsigned int field_mask) {
   SPHPC_SIM(s, p);
   SPHPC_RC(s->ensure_stage());
   const int n = s->n;
@@ -761,7 +781,7 @@ int sphpc_update_host(struct Particles* p) {
                         p->v_z, p->dp_x, p->dp_y, p->dp_z, p->w_x, p->w_y, p->w_z,
                         p->color_x, p->color_y, p->color_z, p->density, p->lambda};
   for (int k = 0; k < 20; ++k)
-    if (fields[k])
+    if (fields[k] && (field_mask & (1u << k)))
       SPHPC_CK(cudaMemcpyAsync(fields[k], s->stage + (size_t)k * n, sizeof(double) * n,
                                cudaMemcpyDeviceToHost, s->stream));
   SPHPC_CK(cudaStreamSynchronize(s->stream));
@@ -770,7 +790,9 @@ int sphpc_update_host(struct Particles* p) {
   return SPHPC_OK;
 }
 
-int sphpc_update_device(struct Particles* p) {
+int sphpc_update_device(struct Particles* p) { return sphpc_update_device_fields(p, 0xFFFFFFFFu); }
+
+int sphpc_update_device_fields(struct Particles* p, unsigned int field_mask) {
   SPHPC_SIM(s, p);
   SPHPC_RC(s->ensure_stage());
   const int n = s->n;
@@ -782,7 +804,8 @@ int sphpc_update_device(struct Particles* p) {
   const int groups[8][2] = {{0, 3}, {3, 3}, {6, 3}, {9, 3}, {12, 3}, {15, 3}, {18, 1}, {19, 1}};
   for (auto& g : groups) {
     bool all = true;
-    for (int k = g[0]; k < g[0] + g[1]; ++k) all = all && fields[k] != nullptr;
+    for (int k = g[0]; k < g[0] + g[1]; ++k)
+      all = all && fields[k] != nullptr && (field_mask & (1u << k));
     if (!all) continue;
     mask |= 1u << g[0];
     for (int k = g[0]; k < g[0] + g[1]; ++k)
@@ -1150,6 +1173,18 @@ int sphpc_diagnostics(const struct Particles* particles, struct SphpcDiag* diag)
   return SPHPC_OK;
 }
 
+int sphpc_step_info(const struct Particles* particles, struct SphpcStepInfo* info) {
+  SPHPC_SIM(s, particles);
+  if (!info) return set_error(SPHPC_EINVAL, "sphpc_step_info: null");
+  memset(info, 0, sizeof(*info));
+  info->iterations = (int)s->last_iterations;
+  info->converged = s->last_converged;
+  info->warm_start_used = s->last_warm != 0.0;
+  info->max_density_error = s->last_max_err;
+  info->mean_density_error = s->last_mean_err;
+  return SPHPC_OK;
+}
+
 int sphpc_device_errors(const struct Particles* particles, unsigned int* bits) {
   SPHPC_SIM(s, particles);
   uint32_t h[2] = {0, 0};
@@ -1183,7 +1218,12 @@ int sphpc_profile_read(const struct Particles* particles, struct SphpcKernelTime
     out[i].launches = s->prof_count[i];
     out[i].total_ms = s->prof_ms[i];
   }
-  if (n_entries) *n_entries = m;
+  if (m < max_entries) {
+    memset(&out[m], 0, sizeof(out[m]));
+    strncpy(out[m].name, "kernel_launches", sizeof(out[m].name) - 1);
+    out[m].launches = (int)(s->launches & 0x7fffffff);
+  }
+  if (n_entries) *n_entries = m + 1;
   return SPHPC_OK;
 }
 

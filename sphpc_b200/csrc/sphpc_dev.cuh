@@ -56,6 +56,7 @@ struct DevParams {
   float DWn, DWn_m;     // spiky gradient norm
   float DWPn;           // poly6 gradient norm
   float m, rho0, inv_rho0, inv_rho0_sq;
+  double rho0_d;
   float lambda_eps;
   float scorr_k;        // s_corr = -k (W/W(dq))^n
   int scorr_n;
@@ -141,6 +142,7 @@ __device__ __forceinline__ void for_each_neighbor(const NbrView& v, int p, F&& f
 #pragma unroll 1
       while (pos < end) {
         const int w = pos >> 5;
+        if (w >= kMaskWords) return;  // only a particle flagged by an overflow
         if (w != cur_w) {
           cur_w = w;
           cur_word = __ldg(v.mask + (size_t)w * v.n + p);

@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (AABB, Diag, KernelTime, Neighbors, Obstacle, Params, Particles, Solver,
-                   PARTICLE_FIELDS, call, load)
+                   StepInfo, PARTICLE_FIELDS, call, load)
 from .scenes import config_path
 
 
@@ -87,6 +87,23 @@ class Simulation:
         fields = fields or PARTICLE_FIELDS
         return {f: self.host(f).copy() for f in fields}
 
+    def fetch_fields(self, fields):
+        """Device -> host of the named fields only (no copies returned)."""
+        mask = 0
+        for f in fields:
+            mask |= 1 << PARTICLE_FIELDS.index(f)
+        call("sphpc_update_host_fields", C.byref(self.particles), mask)
+
+    def push_fields(self, fields):
+        """Host -> device of the named fields (groups must be complete)."""
+        mask = 0
+        for f in fields:
+            mask |= 1 << PARTICLE_FIELDS.index(f)
+        call("sphpc_update_device_fields", C.byref(self.particles), mask)
+
+    def launches(self) -> int:
+        return self.profile_read().get("kernel_launches", (0, 0.0))[0]
+
     def push(self, arrays: dict | None = None):
         """Writes `arrays` into the host arrays, then host -> device."""
         for f, v in (arrays or {}).items():
@@ -113,6 +130,14 @@ class Simulation:
         d = Diag()
         call("sphpc_diagnostics", C.byref(self.particles), C.byref(d))
         return d.as_dict()
+
+    def last_step_info(self) -> dict:
+        i = StepInfo()
+        call("sphpc_step_info", C.byref(self.particles), C.byref(i))
+        return {"iterations": i.iterations, "converged": i.converged,
+                "warm_start_used": i.warm_start_used,
+                "max_density_error": i.max_density_error,
+                "mean_density_error": i.mean_density_error}
 
     def device_errors(self) -> int:
         bits = C.c_uint(0)
