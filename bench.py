@@ -132,60 +132,63 @@ def dist_init(args):
 # CPU reference (the reference's own particles.c / neighbors.c)
 # --------------------------------------------------------------------------
 
-def reference_sample(config_name, iterations, target_s=12.0, max_steps=50, warmup=1,
-                     lattice=(32, 32, 32)):
-    """Times the reference's CPU path (oracle/_ref, -O3) on a bounded sample of
-    the workload: a 32^3 block of the configuration's lattice with its h,
-    dt, box and obstacle.  Returns particle-steps/s and a description."""
-    from oracle.pyoracle import RefSim, scene_from_ini
-    from sphpc_b200.scenes import config_path
-    sc = scene_from_ini(config_path(config_name))
-    nl = sc.meta["lattice"]
-    keep = []
-    # first lattice[0] x lattice[1] x lattice[2] sub-block of the lattice
-    for iz in range(min(lattice[2], nl[2])):
-        for iy in range(min(lattice[1], nl[1])):
-            base = (iz * nl[1] + iy) * nl[0]
-            keep.extend(range(base, base + min(lattice[0], nl[0])))
-    keep = np.array(keep)
-    sc.x0 = np.ascontiguousarray(sc.x0[:, keep])
-    ref = RefSim(sc, fast=True)
-    for _ in range(warmup):
-        ref.step(1, iterations)
+class ReferenceSample:
+    """The reference's CPU path (oracle/_ref/libsphpc_ref_fast.so: its own
+    particles.c and neighbors.c at -O3) on a bounded sample of the workload:
+    a 32x32x32 block of the configuration's lattice with its h, dt, box and
+    obstacle, stepped with `iterations` constraint iterations."""
+
+    def __init__(self, config_name, iterations, lattice=(32, 32, 32)):
+        from oracle.pyoracle import RefSim, scene_from_ini
+        from sphpc_b200.scenes import config_path
+        sc = scene_from_ini(config_path(config_name))
+        nl = sc.meta["lattice"]
+        keep = []
+        for iz in range(min(lattice[2], nl[2])):
+            for iy in range(min(lattice[1], nl[1])):
+                base = (iz * nl[1] + iy) * nl[0]
+                keep.extend(range(base, base + min(lattice[0], nl[0])))
+        sc.x0 = np.ascontiguousarray(sc.x0[:, np.array(keep)])
+        self.ref = RefSim(sc, fast=True)
+        self.n = sc.n
+        self.iterations = iterations
+        self.desc = (f"{self.n} particles ({'x'.join(map(str, lattice))} block of "
+                     f"{config_name}), {iterations} iterations per step, 1 thread")
+
+    def step_rate(self, steps=1):
+        t0 = time.perf_counter()
+        self.ref.step(steps, self.iterations)
+        return self.n * steps / (time.perf_counter() - t0)
+
+
+def reference_sample(config_name, iterations, target_s=8.0, max_steps=50):
+    rs = ReferenceSample(config_name, iterations)
+    rs.step_rate(1)  # warm-up
     steps, t0 = 0, time.perf_counter()
-    while steps < max_steps:
-        ref.step(1, iterations)
+    while steps < max_steps and time.perf_counter() - t0 < target_s:
+        rs.ref.step(1, iterations)
         steps += 1
-        if time.perf_counter() - t0 > target_s:
-            break
     dt = time.perf_counter() - t0
-    return sc.n * steps / dt, {
-        "sample": f"{sc.n} particles ({'x'.join(map(str, lattice))} block of {config_name}), "
-                  f"{steps} steps x {iterations} iterations, {dt:.1f} s",
-        "cores": 1, "kind": "reference"}
+    return rs.n * steps / dt, {"sample": rs.desc + f", {steps} timed steps", "cores": 1,
+                               "kind": "reference"}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    steps_done, t_all = 0, 0.0
-    from oracle.pyoracle import RefSim  # noqa: F401  (fails loudly if not built)
-    iters = args.ref_iterations
-    vals = []
-    for k in range(args.warmup + args.steps):
-        v, info = reference_sample(args.config, iters, target_s=args.ref_seconds, max_steps=3,
-                                   warmup=0)
-        if k >= args.warmup:
-            vals.append(v)
-    value = float(np.mean(vals))
+    rs = ReferenceSample(args.config, args.ref_iterations)
+    for _ in range(args.warmup):
+        rs.step_rate(1)
+    t0 = time.perf_counter()
+    rs.ref.step(args.steps, rs.iterations)
+    value = rs.n * args.steps / (time.perf_counter() - t0)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.config, "sample": info["sample"],
-                   "iterations_per_step": iters},
+        "config": {"workload": args.config, "sample": rs.desc},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": info["sample"]},
+                         "sample": rs.desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -280,7 +283,7 @@ def run_ours(args, world, rank, local, dist):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             v, info = reference_sample(args.config, args.ref_iterations,
-                                       target_s=args.ref_seconds, max_steps=20)
+                                       target_s=args.ref_seconds, max_steps=40)
             cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
                    "sample": info["sample"]}
         except Exception as e:  # the checker is optional on a box without it
