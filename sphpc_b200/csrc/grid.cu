@@ -103,8 +103,8 @@ __global__ void __launch_bounds__(kBlock)
               const uint32_t* __restrict__ loc_by_id, const float4* __restrict__ pos_in,
               const float4* __restrict__ vel_in, const float4* __restrict__ disp_in,
               float4* __restrict__ pos_out, float4* __restrict__ vel_out,
-              float4* __restrict__ disp_out, uint32_t* __restrict__ cellp, int predict,
-              int move_vel, ReorderExtra ex) {
+              float4* __restrict__ disp_out, float4* __restrict__ xsa,
+              uint32_t* __restrict__ cellp, int predict, int move_vel, ReorderExtra ex) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= P.n) return;
   const uint32_t id = __ldg(sorted_ids + j);
@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(kBlock)
   pos_out[j] = x;
   d.w = dg.w;
   disp_out[j] = d;
+  xsa[j] = make_float4((float)xs, (float)ys, (float)zs, 0.0f);
   cellp[j] = pack_cell(P, cx, cy, cz);
   if (move_vel) {
     if (predict) {
@@ -142,6 +143,18 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 constexpr int kSmallGap = 32;
+constexpr int64_t kGapChunk = 4096;  // worklist entries cover at most this many cells
+
+__device__ __forceinline__ void push_gap(int64_t lo, int64_t hi, uint32_t val, uint4* gaps,
+                                         uint32_t* gap_count) {
+  const int64_t pieces = (hi - lo + kGapChunk) / kGapChunk;
+  const uint32_t g = atomicAdd(gap_count, (uint32_t)pieces);
+  for (int64_t k = 0; k < pieces; ++k) {
+    const int64_t a = lo + k * kGapChunk;
+    const int64_t b = min(hi, a + kGapChunk - 1);
+    gaps[g + k] = make_uint4((uint32_t)a, (uint32_t)b, val, 0u);
+  }
+}
 
 // start[c] = lower_bound(keys, c): the first slot j of every non-empty key
 // writes j into the cells (key[j-1], key[j]]; long runs of empty cells go to
@@ -163,8 +176,7 @@ __global__ void __launch_bounds__(kBlock)
     if (hi - lo + 1 <= kSmallGap) {
       for (int64_t c = lo; c <= hi; ++c) cstart[c] = (uint32_t)j;
     } else {
-      const uint32_t g = atomicAdd(gap_count, 1u);
-      gaps[g] = make_uint4((uint32_t)lo, (uint32_t)hi, (uint32_t)j, 0u);
+      push_gap(lo, hi, (uint32_t)j, gaps, gap_count);
     }
   }
   if (j == n - 1) {
@@ -172,8 +184,7 @@ __global__ void __launch_bounds__(kBlock)
     if (hi - lo + 1 <= kSmallGap) {
       for (int64_t c = lo; c <= hi; ++c) cstart[c] = (uint32_t)n;
     } else {
-      const uint32_t g = atomicAdd(gap_count, 1u);
-      gaps[g] = make_uint4((uint32_t)lo, (uint32_t)hi, (uint32_t)n, 0u);
+      push_gap(lo, hi, (uint32_t)n, gaps, gap_count);
     }
   }
 }
@@ -208,24 +219,26 @@ __device__ __forceinline__ bool axis_regular(double x, double h, int c, int nmax
 }
 
 struct BuildCtx {
-  float4 xp, dp;
-  double xs, ys, zs;
+  float4 xf;              // x* as FP32 (candidate pre-test)
+  float4 xp, dp;          // exact representation x + d
+  double xs, ys, zs;      // canonical double x*
   float h2lo, h2hi;
   double h2d;
 };
 
 // r^2 < h^2 exactly as neighbors.c:278-285 evaluates it on the canonical
-// double positions; an FP32 estimate decides all pairs outside a narrow band
-// around h^2.
+// double positions.  The FP32 absolute positions decide every pair whose r^2
+// lies outside a band of +-2^-10 h^2 (FP32 rounding of coordinates up to
+// 2^15 h moves r^2 by far less); the FP64 test decides the rest.
 __device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const float4* __restrict__ pos,
-                                            const float4* __restrict__ disp, int j) {
-  const float4 xq = __ldg(pos + j), dq = __ldg(disp + j);
-  const float fx = (c.xp.x - xq.x) + (c.dp.x - dq.x);
-  const float fy = (c.xp.y - xq.y) + (c.dp.y - dq.y);
-  const float fz = (c.xp.z - xq.z) + (c.dp.z - dq.z);
+                                            const float4* __restrict__ disp,
+                                            const float4* __restrict__ xsa, int j) {
+  const float4 q = __ldg(xsa + j);
+  const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
   const float r2f = fx * fx + fy * fy + fz * fz;
   if (r2f < c.h2lo) return true;
   if (r2f > c.h2hi) return false;
+  const float4 xq = __ldg(pos + j), dq = __ldg(disp + j);
   const double ddx = __dsub_rn(c.xs, xstar_d(xq.x, dq.x));
   const double ddy = __dsub_rn(c.ys, xstar_d(xq.y, dq.y));
   const double ddz = __dsub_rn(c.zs, xstar_d(xq.z, dq.z));
@@ -234,81 +247,60 @@ __device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const float4* __r
   return r2 < c.h2d;
 }
 
-__global__ void __launch_bounds__(kBlock)
+constexpr int kBuildBlock = 128;
+
+// FillNeighbors, neighbors.c:217-298: one thread per particle; the bucket is
+// staged in shared memory and written out as columns nbr[j][*] so that each
+// store instruction of a warp fills one contiguous line.
+__global__ void __launch_bounds__(kBuildBlock)
     k_build_neighbors(const DevParams P, const NbrView V, const float4* __restrict__ pos,
-                      const float4* __restrict__ disp, uint32_t* __restrict__ cellp,
-                      uint32_t* __restrict__ mask, uint32_t* __restrict__ explist,
-                      uint32_t exp_cap, uint32_t* __restrict__ exp_count,
-                      uint8_t* __restrict__ ncount, uint32_t* __restrict__ err) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P.n) return;
-  BuildCtx c;
-  c.xp = __ldg(pos + p);
-  c.dp = __ldg(disp + p);
-  c.xs = xstar_d(c.xp.x, c.dp.x);
-  c.ys = xstar_d(c.xp.y, c.dp.y);
-  c.zs = xstar_d(c.xp.z, c.dp.z);
-  c.h2lo = P.h2 * (1.0f - 1.0f / 16384.0f);
-  c.h2hi = P.h2 * (1.0f + 1.0f / 16384.0f);
-  c.h2d = P.h2d;
-  const uint32_t cp = cellp[p] & ~kExplicitFlag;
-  int cx, cy, cz;
-  unpack_cell(V, cp, cx, cy, cz);
-  bool regular = axis_regular(c.xs, P.hd, cx, P.nx) && axis_regular(c.ys, P.hd, cy, P.ny) &&
-                 axis_regular(c.zs, P.hd, cz, P.nz);
-  const int xlo = cx - (cx > 0);
-  const int xhi = cx + (cx < P.nx - 1);
-  if (regular) {
-    int L = 0;
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int z = cz + dz;
-      if ((unsigned)z >= (unsigned)P.nz) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int y = cy + dy;
-        if ((unsigned)y >= (unsigned)P.ny) continue;
-        const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
-        L += (int)(__ldg(V.cstart + rk + xhi + 1) - __ldg(V.cstart + rk + xlo));
-      }
-    }
-    if (L > 32 * kMaskWords) regular = false;
-  }
+                      const float4* __restrict__ disp, const float4* __restrict__ xsa,
+                      const uint32_t* __restrict__ cellp, uint32_t* __restrict__ nbr,
+                      uint8_t* __restrict__ ncount) {
+  __shared__ uint32_t s_list[kMaxNeighbors][kBuildBlock];
+  const int t = threadIdx.x;
+  const int p = blockIdx.x * kBuildBlock + t;
   int count = 0;
-  if (regular) {
-    uint32_t word = 0;
-    int wbit = 0, widx = 0;
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int z = cz + dz;
-      if ((unsigned)z >= (unsigned)P.nz) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int y = cy + dy;
-        if ((unsigned)y >= (unsigned)P.ny) continue;
-        const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
-        const int b = (int)__ldg(V.cstart + rk + xlo);
-        const int e = (int)__ldg(V.cstart + rk + xhi + 1);
-        for (int j = b; j < e; ++j) {
-          if (count < kMaxNeighbors && j != p && is_neighbor(c, pos, disp, j)) {
-            word |= 1u << wbit;
-            ++count;
-          }
-          if (++wbit == 32) {
-            mask[(size_t)widx * P.n + p] = word;
-            ++widx;
-            word = 0;
-            wbit = 0;
+  if (p < P.n) {
+    BuildCtx c;
+    c.xp = __ldg(pos + p);
+    c.dp = __ldg(disp + p);
+    c.xf = __ldg(xsa + p);
+    c.xs = xstar_d(c.xp.x, c.dp.x);
+    c.ys = xstar_d(c.xp.y, c.dp.y);
+    c.zs = xstar_d(c.xp.z, c.dp.z);
+    c.h2lo = P.h2 * (1.0f - 1.0f / 1024.0f);
+    c.h2hi = P.h2 * (1.0f + 1.0f / 1024.0f);
+    c.h2d = P.h2d;
+    int cx, cy, cz;
+    unpack_cell(V, __ldg(cellp + p), cx, cy, cz);
+    const bool regular = axis_regular(c.xs, P.hd, cx, P.nx) &&
+                         axis_regular(c.ys, P.hd, cy, P.ny) &&
+                         axis_regular(c.zs, P.hd, cz, P.nz);
+    if (regular) {
+      // rows (dz, dy) of cells cx-1..cx+1 are contiguous slot ranges
+      const int xlo = cx - (cx > 0);
+      const int xhi = cx + (cx < P.nx - 1);
+      for (int dz = -1; dz <= 1 && count < kMaxNeighbors; ++dz) {
+        const int z = cz + dz;
+        if ((unsigned)z >= (unsigned)P.nz) continue;
+        for (int dy = -1; dy <= 1 && count < kMaxNeighbors; ++dy) {
+          const int y = cy + dy;
+          if ((unsigned)y >= (unsigned)P.ny) continue;
+          const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
+          const int b = (int)__ldg(V.cstart + rk + xlo);
+          const int e = (int)__ldg(V.cstart + rk + xhi + 1);
+          for (int j = b; j < e; ++j) {
+            if (j != p && is_neighbor(c, pos, disp, xsa, j)) {
+              s_list[count][t] = (uint32_t)j;
+              if (++count == kMaxNeighbors) break;
+            }
           }
         }
       }
-    }
-    if (wbit > 0) mask[(size_t)widx * P.n + p] = word;
-    cellp[p] = cp;
-  } else {
-    const uint32_t idx = atomicAdd(exp_count, 1u);
-    if (idx >= exp_cap) {
-      atomicOr(err, kErrExplicitOverflow);
-      for (int w = 0; w < kMaskWords; ++w) mask[(size_t)w * P.n + p] = 0u;
-      cellp[p] = cp;
     } else {
-      uint32_t* lst = explist + (size_t)idx * kExplicitStride;
+      // neighbour cells are not cx-1..cx+1 (FP64 rounding at a cell face):
+      // the reference's 27-cell walk, verbatim
       for (int dz = -1; dz <= 1; ++dz)
         for (int dy = -1; dy <= 1; ++dy)
           for (int dx = -1; dx <= 1; ++dx) {
@@ -321,20 +313,14 @@ __global__ void __launch_bounds__(kBlock)
             if (key >= P.ncells) continue;
             const int b = (int)__ldg(V.cstart + key);
             const int e = (int)__ldg(V.cstart + key + 1);
-            for (int j = b; j < e; ++j) {
-              if (j == p) continue;
-              if (count < kMaxNeighbors && is_neighbor(c, pos, disp, j)) {
-                lst[1 + count] = (uint32_t)j;
-                ++count;
-              }
+            for (int j = b; j < e && count < kMaxNeighbors; ++j) {
+              if (j != p && is_neighbor(c, pos, disp, xsa, j)) s_list[count++][t] = (uint32_t)j;
             }
           }
-      lst[0] = (uint32_t)count;
-      mask[p] = idx;
-      cellp[p] = cp | kExplicitFlag;
     }
+    ncount[p] = (uint8_t)count;
+    for (int j = 0; j < count; ++j) nbr[(size_t)j * P.n + p] = s_list[j][t];
   }
-  ncount[p] = (uint8_t)count;
 }
 
 __global__ void __launch_bounds__(kBlock)
@@ -369,12 +355,13 @@ void launch_hash_plain(const DevParams& P, const float4* pos, const float4* disp
 
 void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
                     const float4* pos_in, const float4* vel_in, const float4* disp_in,
-                    float4* pos_out, float4* vel_out, float4* disp_out, uint32_t* cellp,
-                    bool predict, bool move_vel, const ReorderExtra* extra, cudaStream_t st) {
+                    float4* pos_out, float4* vel_out, float4* disp_out, float4* xsa,
+                    uint32_t* cellp, bool predict, bool move_vel, const ReorderExtra* extra,
+                    cudaStream_t st) {
   ReorderExtra ex = {};
   if (extra) ex = *extra;
   k_reorder<<<grid_for(P.n), kBlock, 0, st>>>(P, sorted_ids, loc_by_id, pos_in, vel_in,
-                                              disp_in, pos_out, vel_out, disp_out, cellp,
+                                              disp_in, pos_out, vel_out, disp_out, xsa, cellp,
                                               predict ? 1 : 0, move_vel ? 1 : 0, ex);
 }
 
@@ -387,16 +374,14 @@ void launch_cell_starts(const uint32_t* keys_sorted, int n, uint32_t ncells, uin
   cudaMemsetAsync(gap_count, 0, sizeof(uint32_t), st);
   k_cell_starts<<<grid_for(n), kBlock, 0, st>>>(keys_sorted, n, ncells, cstart, gaps,
                                                  gap_count, err);
-  k_fill_gaps<<<148 * 4, kBlock, 0, st>>>(gaps, gap_count, cstart);
+  k_fill_gaps<<<148 * 16, kBlock, 0, st>>>(gaps, gap_count, cstart);
 }
 
 void launch_build_neighbors(const DevParams& P, const NbrView& V, const float4* pos,
-                            const float4* disp, uint32_t* cellp, uint32_t* mask,
-                            uint32_t* explist, uint32_t exp_cap, uint32_t* exp_count,
-                            uint8_t* ncount, uint32_t* err, cudaStream_t st) {
-  cudaMemsetAsync(exp_count, 0, sizeof(uint32_t), st);
-  k_build_neighbors<<<grid_for(P.n), kBlock, 0, st>>>(P, V, pos, disp, cellp, mask, explist,
-                                                      exp_cap, exp_count, ncount, err);
+                            const float4* disp, const float4* xsa, const uint32_t* cellp,
+                            uint32_t* nbr, uint8_t* ncount, cudaStream_t st) {
+  k_build_neighbors<<<grid_for(P.n, kBuildBlock), kBuildBlock, 0, st>>>(P, V, pos, disp, xsa,
+                                                                         cellp, nbr, ncount);
 }
 
 void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr, int32_t* count,

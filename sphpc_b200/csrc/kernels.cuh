@@ -41,20 +41,21 @@ struct ReorderExtra {
 };
 void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
                     const float4* pos_in, const float4* vel_in, const float4* disp_in,
-                    float4* pos_out, float4* vel_out, float4* disp_out, uint32_t* cellp,
-                    bool predict, bool move_vel, const ReorderExtra* extra, cudaStream_t st);
+                    float4* pos_out, float4* vel_out, float4* disp_out, float4* xsa,
+                    uint32_t* cellp, bool predict, bool move_vel, const ReorderExtra* extra,
+                    cudaStream_t st);
 
 // Cell start table cstart[0..C] from sorted keys (lower bounds; cstart[C]=n).
-// gaps: worklist scratch of >= n+2 uint4 entries; gap_count: one u32.
+// gaps: worklist scratch of >= n + 2 + C/4096 + 2 uint4 entries; gap_count:
+// one u32.
 void launch_cell_starts(const uint32_t* keys_sorted, int n, uint32_t ncells, uint32_t* cstart,
                         uint4* gaps, uint32_t* gap_count, uint32_t* err, cudaStream_t st);
 
-// Neighbour build (FillNeighbors, neighbors.c:217-298): per particle, the
-// candidate bitmask (or an explicit list), and the neighbour count.
+// Neighbour build (FillNeighbors, neighbors.c:217-298): per particle, its
+// bucket of neighbour slots nbr[j][p] and its size ncount[p].
 void launch_build_neighbors(const DevParams& P, const NbrView& V, const float4* pos,
-                            const float4* disp, uint32_t* cellp, uint32_t* mask,
-                            uint32_t* explist, uint32_t exp_cap, uint32_t* exp_count,
-                            uint8_t* ncount, uint32_t* err, cudaStream_t st);
+                            const float4* disp, const float4* xsa, const uint32_t* cellp,
+                            uint32_t* nbr, uint8_t* ncount, cudaStream_t st);
 
 // Export the buckets in original-index space: nbr[id*60 + j], count[id].
 void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr, int32_t* count,

@@ -88,12 +88,12 @@ class DeviceSim {
   float *rho_alt = nullptr, *lam_alt = nullptr;
   uint32_t *ids = nullptr, *ids_spare = nullptr, *keys_by_id = nullptr, *loc_by_id = nullptr;
   uint32_t* keys_sorted = nullptr;  // view into keys_by_id or sort.keys_alt
-  uint32_t *cellp = nullptr, *mask = nullptr, *explist = nullptr, *cstart = nullptr;
+  uint32_t *cellp = nullptr, *nbr = nullptr, *cstart = nullptr;
+  float4* xsa = nullptr;
   uint8_t* ncount = nullptr;
   uint4* gaps = nullptr;
   uint32_t* small = nullptr;  // [0] gap count, [1] explicit count, [2] error bits
   double* resid = nullptr;    // [0] max (bits), [1] sum, [2..] diagnostics
-  uint32_t exp_cap = 0;
   SortScratch sort{};
   uint32_t* sort_aux = nullptr;
   double* stage = nullptr;  // 20 * n doubles for host transfers
@@ -124,7 +124,6 @@ class DeviceSim {
   ~DeviceSim() { release(); }
 
   uint32_t* gap_count() { return small; }
-  uint32_t* exp_count() { return small + 1; }
   uint32_t* err() { return small + 2; }
 
   void release() {
@@ -132,7 +131,7 @@ class DeviceSim {
     dfree(color); dfree(omega); dfree(dp); dfree(rho); dfree(lam);
     dfree(color_alt); dfree(omega_alt); dfree(dp_alt); dfree(rho_alt); dfree(lam_alt);
     dfree(ids); dfree(ids_spare); dfree(keys_by_id); dfree(loc_by_id); dfree(cellp);
-    dfree(mask); dfree(explist); dfree(cstart); dfree(ncount); dfree(gaps); dfree(small);
+    dfree(nbr); dfree(xsa); dfree(cstart); dfree(ncount); dfree(gaps); dfree(small);
     dfree(resid); dfree(sort.keys_alt); dfree(sort.vals_alt); dfree(sort_aux); dfree(stage);
     mlp_release(mlp);
     for (auto& p : pending) {
@@ -154,10 +153,9 @@ class DeviceSim {
     SPHPC_RC(dalloc(&ids, n)); SPHPC_RC(dalloc(&ids_spare, n));
     SPHPC_RC(dalloc(&keys_by_id, n)); SPHPC_RC(dalloc(&loc_by_id, n));
     SPHPC_RC(dalloc(&cellp, n)); SPHPC_RC(dalloc(&ncount, n));
-    SPHPC_RC(dalloc(&mask, (size_t)kMaskWords * n));
-    exp_cap = (uint32_t)(n / 16 + 1024);
-    SPHPC_RC(dalloc(&explist, (size_t)exp_cap * kExplicitStride));
-    SPHPC_RC(dalloc(&gaps, (size_t)n + 2));
+    SPHPC_RC(dalloc(&nbr, (size_t)kMaxNeighbors * n));
+    SPHPC_RC(dalloc(&xsa, n));
+    SPHPC_CK(cudaMemsetAsync(ncount, 0, n, stream));
     SPHPC_RC(dalloc(&small, 8));
     SPHPC_RC(dalloc(&resid, 16));
     SPHPC_RC(dalloc(&sort.keys_alt, n));
@@ -215,6 +213,8 @@ class DeviceSim {
     passes = (bits_for(C - 1) + kRadixBits - 1) / kRadixBits;
     if (passes > kMaxPasses) passes = kMaxPasses;
     SPHPC_RC(dalloc(&cstart, (size_t)C + 1));
+    dfree(gaps);
+    SPHPC_RC(dalloc(&gaps, (size_t)n + 4 + C / 4096));
     SPHPC_CK(cudaMemsetAsync(cstart, 0, sizeof(uint32_t) * ((size_t)C + 1), stream));
     grid_ready = true;
     nbr_valid = false;
@@ -223,9 +223,8 @@ class DeviceSim {
 
   NbrView view() const {
     NbrView v;
-    v.cellp = cellp;
-    v.mask = mask;
-    v.explist = explist;
+    v.nbr = nbr;
+    v.ncount = ncount;
     v.cstart = cstart;
     v.n = n;
     v.nx = nx; v.ny = ny; v.nz = nz;
@@ -427,8 +426,8 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
       ex.in1[1] = lam; ex.out1[1] = lam_alt;
     }
     const bool mv = move_vel || full;
-    launch_reorder(P, R, loc_by_id, pos, vel, disp, pos_alt, vel_alt, disp_alt, cellp, predict,
-                   mv, &ex, stream);
+    launch_reorder(P, R, loc_by_id, pos, vel, disp, pos_alt, vel_alt, disp_alt, xsa, cellp,
+                   predict, mv, &ex, stream);
     launches += 1;
     std::swap(pos, pos_alt);
     std::swap(disp, disp_alt);
@@ -447,8 +446,7 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
   }
   {
     Scope sc(this, "build_neighbors");
-    launch_build_neighbors(P, view(), pos, disp, cellp, mask, explist, exp_cap, exp_count(),
-                           ncount, err(), stream);
+    launch_build_neighbors(P, view(), pos, disp, xsa, cellp, nbr, ncount, stream);
     launches += 1;
   }
   SPHPC_CK(cudaGetLastError());

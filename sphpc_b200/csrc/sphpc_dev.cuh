@@ -7,12 +7,15 @@
 //   disp[n]  float4  d = x* - x, the predicted-position displacement.
 //                    .w carries lambda after the density/lambda pass and the
 //                    density after the position pass.
+//   xsa[n]   float4  x* as absolute FP32 (neighbour-build candidate test)
 //   vel[n]   float4  v
 //   ids[n]   u32     original particle index of each slot
 //   cellp[n] u32     packed grid cell (cx | cy<<bx | cz<<(bx+by)) of x* at
-//                    neighbour-build time; bit 31 = explicit neighbour list
-//   mask[kMaskWords][n] u32  neighbour bitmask over the candidate sequence
-//                    (see for_each_neighbor)
+//                    neighbour-build time
+//   nbr[60][n] u32   neighbour slots of every particle in the reference's
+//                    bucket order (column j of all particles contiguous, so a
+//                    warp reads one 128-byte line per neighbour index)
+//   ncount[n] u8     bucket sizes
 //   cstart[C+1] u32  start slot of every cell (lower bound), cstart[C] = n
 //
 // The canonical predicted position is the double fl64(x + d): the hash, the
@@ -27,13 +30,9 @@
 namespace sphpc {
 
 constexpr int kMaxNeighbors = 60;   // MAX_NEIGHBORS, neighbors.h:6
-constexpr int kMaskWords = 16;      // bitmask capacity: 512 candidates
-constexpr int kExplicitStride = kMaxNeighbors + 1;  // [count, slot...]
-constexpr uint32_t kExplicitFlag = 0x80000000u;
 
 // Error bits raised by kernels (host reads them back).
 enum : uint32_t {
-  kErrExplicitOverflow = 1u << 0,  // explicit neighbour-list table full
   kErrSortSpin = 1u << 1,          // radix-sort look-back wait gave up
   kErrCellRange = 1u << 2,         // a particle hashed outside the grid
   kErrScanSpin = 1u << 3,
@@ -82,10 +81,9 @@ struct DevParams {
 
 // View of the per-step neighbour structure.
 struct NbrView {
-  const uint32_t* __restrict__ cellp;
-  const uint32_t* __restrict__ mask;
-  const uint32_t* __restrict__ explist;
-  const uint32_t* __restrict__ cstart;
+  const uint32_t* __restrict__ nbr;     // [kMaxNeighbors][n]
+  const uint8_t* __restrict__ ncount;   // [n]
+  const uint32_t* __restrict__ cstart;  // [C+1]
   int n;
   int nx, ny, nz;
   uint32_t nxny;
@@ -95,7 +93,6 @@ struct NbrView {
 
 __device__ __forceinline__ void unpack_cell(const NbrView& v, uint32_t cp, int& cx,
                                             int& cy, int& cz) {
-  cp &= ~kExplicitFlag;
   cx = (int)(cp & v.mx);
   cy = (int)((cp >> v.bx) & v.my);
   cz = (int)(cp >> (v.bx + v.by));
@@ -103,65 +100,13 @@ __device__ __forceinline__ void unpack_cell(const NbrView& v, uint32_t cp, int& 
 
 // Visits the neighbour slots of particle p in the reference's bucket order
 // (FillNeighbors, neighbors.c:247-295: dz, dy, dx, then ascending sorted
-// index).  For a regular particle the candidates of each (dz, dy) row are
-// the contiguous slot range of cells cx-1..cx+1, and the candidate sequence
-// is the concatenation of the valid rows; bit k of the mask marks candidate
-// k as a neighbour.  Particles whose neighbour cells are not cx-1..cx+1
-// (FP64 rounding at a cell face) or whose candidates exceed the mask carry an
-// explicit list instead.
+// index), as stored by the neighbour build.
 template <class F>
 __device__ __forceinline__ void for_each_neighbor(const NbrView& v, int p, F&& f) {
-  const uint32_t cp = __ldg(v.cellp + p);
-  if (cp & kExplicitFlag) {
-    const uint32_t idx = __ldg(v.mask + p);
-    const uint32_t* lst = v.explist + (size_t)idx * kExplicitStride;
-    const int cnt = (int)__ldg(lst);
-    for (int j = 0; j < cnt; ++j) f((int)__ldg(lst + 1 + j));
-    return;
-  }
-  int cx, cy, cz;
-  unpack_cell(v, cp, cx, cy, cz);
-  const int xlo = cx - (cx > 0);
-  const int xhi = cx + (cx < v.nx - 1);
-  int base = 0;  // candidate index of the first slot of the current row
-  int cur_w = -1;
-  uint32_t cur_word = 0;
-#pragma unroll 1
-  for (int dz = -1; dz <= 1; ++dz) {
-    const int z = cz + dz;
-    if ((unsigned)z >= (unsigned)v.nz) continue;
-#pragma unroll 1
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int y = cy + dy;
-      if ((unsigned)y >= (unsigned)v.ny) continue;
-      const uint32_t rk = (uint32_t)z * v.nxny + (uint32_t)y * (uint32_t)v.nx;
-      const int b = (int)__ldg(v.cstart + rk + xlo);
-      const int e = (int)__ldg(v.cstart + rk + xhi + 1);
-      const int end = base + (e - b);
-      int pos = base;
-#pragma unroll 1
-      while (pos < end) {
-        const int w = pos >> 5;
-        if (w >= kMaskWords) return;  // only a particle flagged by an overflow
-        if (w != cur_w) {
-          cur_w = w;
-          cur_word = __ldg(v.mask + (size_t)w * v.n + p);
-        }
-        const int sh = pos & 31;
-        const int take = min(32 - sh, end - pos);
-        uint32_t bits = cur_word >> sh;
-        if (take < 32) bits &= (1u << take) - 1u;
-        const int slot0 = b + (pos - base);
-        while (bits) {
-          const int k = __ffs(bits) - 1;
-          bits &= bits - 1u;
-          f(slot0 + k);
-        }
-        pos += take;
-      }
-      base = end;
-    }
-  }
+  const int cnt = (int)__ldg(v.ncount + p);
+  const uint32_t* lst = v.nbr + p;
+#pragma unroll 2
+  for (int j = 0; j < cnt; ++j) f((int)__ldg(lst + (size_t)j * v.n));
 }
 
 // ---------------------------------------------------------------------------
