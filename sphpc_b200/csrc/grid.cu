@@ -54,8 +54,8 @@ __device__ __forceinline__ uint32_t pack_cell(const DevParams& P, int cx, int cy
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_hash(const DevParams P, const float4* __restrict__ pos, const float4* __restrict__ vel,
-           const float4* __restrict__ disp, const uint32_t* __restrict__ ids,
+    k_hash(const DevParams P, const PD* __restrict__ pd, const float4* __restrict__ vel,
+           const uint32_t* __restrict__ ids,
            uint32_t* __restrict__ keys_by_id, uint32_t* __restrict__ loc_by_id,
            uint32_t* __restrict__ hist, int passes, int predict, uint32_t* __restrict__ err) {
   __shared__ uint32_t s_hist[kMaxPasses * kRadix];
@@ -63,9 +63,9 @@ __global__ void __launch_bounds__(kBlock)
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < P.n) {
-    const float4 x = __ldg(pos + i);
+    float4 x, dg;
+    ld_pd(pd, i, x, dg);
     const float4 v = predict ? __ldg(vel + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 dg = predict ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(disp + i);
     float4 d;
     double xs, ys, zs;
     canonical_xstar(P, x, v, dg, predict != 0, d, xs, ys, zs);
@@ -87,31 +87,18 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_hash_plain(const DevParams P, const float4* __restrict__ pos,
-                 const float4* __restrict__ disp, uint32_t* __restrict__ keys) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.n) return;
-  const float4 x = __ldg(pos + i), d = __ldg(disp + i);
-  const double xs = xstar_d(x.x, d.x), ys = xstar_d(x.y, d.y), zs = xstar_d(x.z, d.z);
-  int cx, cy, cz;
-  grid_cell(P, xs, ys, zs, cx, cy, cz);
-  keys[i] = cell_key(P, cx, cy, cz);
-}
-
-__global__ void __launch_bounds__(kBlock)
     k_reorder(const DevParams P, const uint32_t* __restrict__ sorted_ids,
-              const uint32_t* __restrict__ loc_by_id, const float4* __restrict__ pos_in,
-              const float4* __restrict__ vel_in, const float4* __restrict__ disp_in,
-              float4* __restrict__ pos_out, float4* __restrict__ vel_out,
-              float4* __restrict__ disp_out, float4* __restrict__ xsa,
+              const uint32_t* __restrict__ loc_by_id, const PD* __restrict__ pd_in,
+              const float4* __restrict__ vel_in, PD* __restrict__ pd_out,
+              float4* __restrict__ vel_out, float4* __restrict__ xsa,
               uint32_t* __restrict__ cellp, int predict, int move_vel, ReorderExtra ex) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= P.n) return;
   const uint32_t id = __ldg(sorted_ids + j);
   const uint32_t src = __ldg(loc_by_id + id);
-  const float4 x = __ldg(pos_in + src);
+  float4 x, dg;
+  ld_pd(pd_in, (int)src, x, dg);
   float4 v = (predict || move_vel) ? __ldg(vel_in + src) : make_float4(0.f, 0.f, 0.f, 0.f);
-  const float4 dg = predict ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(disp_in + src);
   float4 d;
   double xs, ys, zs;
   canonical_xstar(P, x, v, dg, predict != 0, d, xs, ys, zs);
@@ -120,9 +107,8 @@ __global__ void __launch_bounds__(kBlock)
   cx = min(cx, P.nx - 1);
   cy = min(cy, P.ny - 1);
   cz = min(cz, P.nz - 1);
-  pos_out[j] = x;
-  d.w = dg.w;
-  disp_out[j] = d;
+  d.w = predict ? 0.0f : dg.w;
+  st_pd(pd_out, j, x, d);
   xsa[j] = make_float4((float)xs, (float)ys, (float)zs, 0.0f);
   cellp[j] = pack_cell(P, cx, cy, cz);
   if (move_vel) {
@@ -230,15 +216,15 @@ struct BuildCtx {
 // double positions.  The FP32 absolute positions decide every pair whose r^2
 // lies outside a band of +-2^-10 h^2 (FP32 rounding of coordinates up to
 // 2^15 h moves r^2 by far less); the FP64 test decides the rest.
-__device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const float4* __restrict__ pos,
-                                            const float4* __restrict__ disp,
+__device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const PD* __restrict__ pd,
                                             const float4* __restrict__ xsa, int j) {
   const float4 q = __ldg(xsa + j);
   const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
   const float r2f = fx * fx + fy * fy + fz * fz;
   if (r2f < c.h2lo) return true;
   if (r2f > c.h2hi) return false;
-  const float4 xq = __ldg(pos + j), dq = __ldg(disp + j);
+  float4 xq, dq;
+  ld_pd(pd, j, xq, dq);
   const double ddx = __dsub_rn(c.xs, xstar_d(xq.x, dq.x));
   const double ddy = __dsub_rn(c.ys, xstar_d(xq.y, dq.y));
   const double ddz = __dsub_rn(c.zs, xstar_d(xq.z, dq.z));
@@ -253,8 +239,8 @@ constexpr int kBuildBlock = 128;
 // staged in shared memory and written out as columns nbr[j][*] so that each
 // store instruction of a warp fills one contiguous line.
 __global__ void __launch_bounds__(kBuildBlock)
-    k_build_neighbors(const DevParams P, const NbrView V, const float4* __restrict__ pos,
-                      const float4* __restrict__ disp, const float4* __restrict__ xsa,
+    k_build_neighbors(const DevParams P, const NbrView V, const PD* __restrict__ pd,
+                      const float4* __restrict__ xsa,
                       const uint32_t* __restrict__ cellp, uint32_t* __restrict__ nbr,
                       uint8_t* __restrict__ ncount) {
   __shared__ uint32_t s_list[kMaxNeighbors][kBuildBlock];
@@ -263,8 +249,7 @@ __global__ void __launch_bounds__(kBuildBlock)
   int count = 0;
   if (p < P.n) {
     BuildCtx c;
-    c.xp = __ldg(pos + p);
-    c.dp = __ldg(disp + p);
+    ld_pd(pd, p, c.xp, c.dp);
     c.xf = __ldg(xsa + p);
     c.xs = xstar_d(c.xp.x, c.dp.x);
     c.ys = xstar_d(c.xp.y, c.dp.y);
@@ -291,7 +276,7 @@ __global__ void __launch_bounds__(kBuildBlock)
           const int b = (int)__ldg(V.cstart + rk + xlo);
           const int e = (int)__ldg(V.cstart + rk + xhi + 1);
           for (int j = b; j < e; ++j) {
-            if (j != p && is_neighbor(c, pos, disp, xsa, j)) {
+            if (j != p && is_neighbor(c, pd, xsa, j)) {
               s_list[count][t] = (uint32_t)j;
               if (++count == kMaxNeighbors) break;
             }
@@ -314,7 +299,7 @@ __global__ void __launch_bounds__(kBuildBlock)
             const int b = (int)__ldg(V.cstart + key);
             const int e = (int)__ldg(V.cstart + key + 1);
             for (int j = b; j < e && count < kMaxNeighbors; ++j) {
-              if (j != p && is_neighbor(c, pos, disp, xsa, j)) s_list[count++][t] = (uint32_t)j;
+              if (j != p && is_neighbor(c, pd, xsa, j)) s_list[count++][t] = (uint32_t)j;
             }
           }
     }
@@ -341,28 +326,22 @@ __global__ void __launch_bounds__(kBlock)
 
 }  // namespace
 
-void launch_hash(const DevParams& P, const float4* pos, const float4* vel, const float4* disp,
-                 const uint32_t* ids, uint32_t* keys_by_id, uint32_t* loc_by_id, uint32_t* hist,
-                 int passes, bool predict, uint32_t* err, cudaStream_t st) {
-  k_hash<<<grid_for(P.n), kBlock, 0, st>>>(P, pos, vel, disp, ids, keys_by_id, loc_by_id, hist,
+void launch_hash(const DevParams& P, const PD* pd, const float4* vel, const uint32_t* ids,
+                 uint32_t* keys_by_id, uint32_t* loc_by_id, uint32_t* hist, int passes,
+                 bool predict, uint32_t* err, cudaStream_t st) {
+  k_hash<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, vel, ids, keys_by_id, loc_by_id, hist,
                                            passes, predict ? 1 : 0, err);
 }
 
-void launch_hash_plain(const DevParams& P, const float4* pos, const float4* disp,
-                       uint32_t* keys, cudaStream_t st) {
-  k_hash_plain<<<grid_for(P.n), kBlock, 0, st>>>(P, pos, disp, keys);
-}
-
 void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
-                    const float4* pos_in, const float4* vel_in, const float4* disp_in,
-                    float4* pos_out, float4* vel_out, float4* disp_out, float4* xsa,
-                    uint32_t* cellp, bool predict, bool move_vel, const ReorderExtra* extra,
-                    cudaStream_t st) {
+                    const PD* pd_in, const float4* vel_in, PD* pd_out, float4* vel_out,
+                    float4* xsa, uint32_t* cellp, bool predict, bool move_vel,
+                    const ReorderExtra* extra, cudaStream_t st) {
   ReorderExtra ex = {};
   if (extra) ex = *extra;
-  k_reorder<<<grid_for(P.n), kBlock, 0, st>>>(P, sorted_ids, loc_by_id, pos_in, vel_in,
-                                              disp_in, pos_out, vel_out, disp_out, xsa, cellp,
-                                              predict ? 1 : 0, move_vel ? 1 : 0, ex);
+  k_reorder<<<grid_for(P.n), kBlock, 0, st>>>(P, sorted_ids, loc_by_id, pd_in, vel_in, pd_out,
+                                              vel_out, xsa, cellp, predict ? 1 : 0,
+                                              move_vel ? 1 : 0, ex);
 }
 
 void launch_cell_starts(const uint32_t* keys_sorted, int n, uint32_t ncells, uint32_t* cstart,
@@ -377,11 +356,11 @@ void launch_cell_starts(const uint32_t* keys_sorted, int n, uint32_t ncells, uin
   k_fill_gaps<<<148 * 16, kBlock, 0, st>>>(gaps, gap_count, cstart);
 }
 
-void launch_build_neighbors(const DevParams& P, const NbrView& V, const float4* pos,
-                            const float4* disp, const float4* xsa, const uint32_t* cellp,
-                            uint32_t* nbr, uint8_t* ncount, cudaStream_t st) {
-  k_build_neighbors<<<grid_for(P.n, kBuildBlock), kBuildBlock, 0, st>>>(P, V, pos, disp, xsa,
-                                                                         cellp, nbr, ncount);
+void launch_build_neighbors(const DevParams& P, const NbrView& V, const PD* pd,
+                            const float4* xsa, const uint32_t* cellp, uint32_t* nbr,
+                            uint8_t* ncount, cudaStream_t st) {
+  k_build_neighbors<<<grid_for(P.n, kBuildBlock), kBuildBlock, 0, st>>>(P, V, pd, xsa, cellp,
+                                                                         nbr, ncount);
 }
 
 void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr, int32_t* count,

@@ -20,19 +20,15 @@ inline int grid_for(int n, int block = kBlock) { return n > 0 ? (n + block - 1) 
 // and the slot into original-index order.  When `predict` is false the
 // current x* (pos + disp) is hashed instead.  Accumulates the radix digit
 // histograms of all `passes` into hist.
-void launch_hash(const DevParams& P, const float4* pos, const float4* vel, const float4* disp,
-                 const uint32_t* ids, uint32_t* keys_by_id, uint32_t* loc_by_id, uint32_t* hist,
-                 int passes, bool predict, uint32_t* err, cudaStream_t st);
-
-// Hash of explicit canonical positions (x, d), original order, iota ids:
-// HashParticles on its own, for the seam/unit path.
-void launch_hash_plain(const DevParams& P, const float4* pos, const float4* disp,
-                       uint32_t* keys, cudaStream_t st);
+void launch_hash(const DevParams& P, const PD* pd, const float4* vel, const uint32_t* ids,
+                 uint32_t* keys_by_id, uint32_t* loc_by_id, uint32_t* hist, int passes,
+                 bool predict, uint32_t* err, cudaStream_t st);
 
 // Reorder gather: new slot j takes particle sorted_ids[j] from its old slot.
 // predict: recompute x* from x and v (+gravity) as launch_hash did, else
-// gather disp.  Writes cellp (packed cell of x*).  Optional extra float4 /
-// float fields are gathered too (nullptr to skip).
+// gather d.  Writes the records, x* as FP32 (xsa) and cellp (packed cell of
+// x*).  Optional extra float4 / float fields are gathered too (nullptr to
+// skip).
 struct ReorderExtra {
   const float4* in4[6];
   float4* out4[6];
@@ -40,10 +36,9 @@ struct ReorderExtra {
   float* out1[4];
 };
 void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
-                    const float4* pos_in, const float4* vel_in, const float4* disp_in,
-                    float4* pos_out, float4* vel_out, float4* disp_out, float4* xsa,
-                    uint32_t* cellp, bool predict, bool move_vel, const ReorderExtra* extra,
-                    cudaStream_t st);
+                    const PD* pd_in, const float4* vel_in, PD* pd_out, float4* vel_out,
+                    float4* xsa, uint32_t* cellp, bool predict, bool move_vel,
+                    const ReorderExtra* extra, cudaStream_t st);
 
 // Cell start table cstart[0..C] from sorted keys (lower bounds; cstart[C]=n).
 // gaps: worklist scratch of >= n + 2 + C/4096 + 2 uint4 entries; gap_count:
@@ -53,9 +48,9 @@ void launch_cell_starts(const uint32_t* keys_sorted, int n, uint32_t ncells, uin
 
 // Neighbour build (FillNeighbors, neighbors.c:217-298): per particle, its
 // bucket of neighbour slots nbr[j][p] and its size ncount[p].
-void launch_build_neighbors(const DevParams& P, const NbrView& V, const float4* pos,
-                            const float4* disp, const float4* xsa, const uint32_t* cellp,
-                            uint32_t* nbr, uint8_t* ncount, cudaStream_t st);
+void launch_build_neighbors(const DevParams& P, const NbrView& V, const PD* pd,
+                            const float4* xsa, const uint32_t* cellp, uint32_t* nbr,
+                            uint8_t* ncount, cudaStream_t st);
 
 // Export the buckets in original-index space: nbr[id*60 + j], count[id].
 void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr, int32_t* count,
@@ -64,9 +59,8 @@ void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr,
 // ---- PBF passes (pbf.cu) ----
 
 struct PassArgs {
-  const float4* pos;   // x
-  const float4* disp;  // x* - x (+ .w payload)
-  float4* disp_out;
+  const PD* pd;        // records {x, d} read by the pass (neighbours included)
+  PD* pd_out;          // records written by the pass (never the same buffer)
   float4* vel;
   float4* vel_out;
   float* rho;
@@ -74,7 +68,6 @@ struct PassArgs {
   float4* dp;          // UpdateDPs output (per-function path)
   float4* color;
   float4* omega;
-  float4* pos_out;     // UpdatePositions target
   double* resid;       // [0] max density error bits (as u64), [1] sum
   float stiffness;     // UpdateDPs stiffness for this substep
   int last;            // fused position pass: also UpdateVelocities
@@ -82,22 +75,24 @@ struct PassArgs {
 };
 
 // Density (+lambda) pass: ComputeDensities (particles.c:461-514) and
-// ComputeLambda (:588-666).  mode 0: both (lambda to disp.w and lam[]),
-// mode 1: density only, mode 2: lambda only (reads rho[]).
+// ComputeLambda (:588-666).  mode 0: both (records with lambda in d.w to
+// pd_out, lam[] if set), mode 1: density only, mode 2: lambda only (reads
+// rho[]).
 void launch_density_lambda(const DevParams& P, const NbrView& V, const PassArgs& a, int mode,
                            bool residual, cudaStream_t st);
-// Position pass: UpdateDPs (:668-746) with lambda from disp.w; mode 0 fuses
+// Position pass: UpdateDPs (:668-746) with lambda from d.w; mode 0 fuses
 // UpdatePositionStars (:529-564, clamp + SDF collision) and, if a.last,
 // UpdateVelocities (:787-838); mode 1 writes dp[] only.
 void launch_position(const DevParams& P, const NbrView& V, const PassArgs& a, int mode,
                      cudaStream_t st);
-// UpdatePositionStars alone: disp += dp, clamp, SDF collision.
+// UpdatePositionStars alone, in place on pd_out: d += dp, clamp, SDF.
 void launch_apply_dp(const DevParams& P, const PassArgs& a, cudaStream_t st);
 // ComputeSurfaceTension colour pass (:94-140) and force pass (:142-204).
-// Density of neighbours is read from disp.w.
+// Density of neighbours is read from d.w.
 void launch_color(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st);
 void launch_tension(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st);
-// ApplyViscosity (:383-459) as a Jacobi update vel -> vel_out.
+// ApplyViscosity (:383-459) as a Jacobi update vel -> vel_out; with
+// write_pos also UpdatePositions into pd_out.
 void launch_xsph(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st);
 // ComputeVorticity (:207-283) from vel; ApplyVorticityConfinement (:285-381)
 // updates vel in place.
@@ -106,14 +101,11 @@ void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a,
                         cudaStream_t st);
 // Pointwise steps.
 void launch_gravity(const DevParams& P, float4* vel, cudaStream_t st);
-void launch_predict(const DevParams& P, const float4* pos, const float4* vel, float4* disp,
-                    cudaStream_t st);
-void launch_update_velocities(const DevParams& P, const float4* disp, float4* vel,
-                              cudaStream_t st);
-void launch_update_positions(const DevParams& P, const float4* pos, float4* disp,
-                             float4* pos_out, cudaStream_t st);
-// disp.w <- src[p] (repack a per-particle scalar for the neighbour passes).
-void launch_pack_w(const DevParams& P, float4* disp, const float* src, cudaStream_t st);
+void launch_predict(const DevParams& P, PD* pd, const float4* vel, cudaStream_t st);
+void launch_update_velocities(const DevParams& P, const PD* pd, float4* vel, cudaStream_t st);
+void launch_update_positions(const DevParams& P, PD* pd, cudaStream_t st);
+// d.w <- src[p] (repack a per-particle scalar for the neighbour passes).
+void launch_pack_w(const DevParams& P, PD* pd, const float* src, cudaStream_t st);
 // CalculateParticleCollisions seam on device double arrays.
 void launch_collisions_double(const DevParams& P, double* x, double* y, double* z, int n,
                               cudaStream_t st);

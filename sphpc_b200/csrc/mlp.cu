@@ -4,8 +4,8 @@
 
 namespace sphpc {
 
-int mlp_warm_start(MlpState& m, const DevParams&, const NbrView&, const float4*, const float4*,
-                   float4*, const float4*, const uint8_t*, cudaStream_t) {
+int mlp_warm_start(MlpState& m, const DevParams&, const NbrView&, const PD*, PD*,
+                   const float4*, const uint8_t*, cudaStream_t) {
   (void)m;
   return set_error(SPHPC_ENOTREADY, "warm start: no network loaded");
 }

@@ -13,10 +13,9 @@ struct MlpState {
 
 inline void mlp_release(MlpState& m) { m.ready = false; }
 
-// Writes disp_out = (d, lambda0) for every particle from the network's
+// Writes pd_out = {x, (d, lambda0)} for every particle from the network's
 // prediction; returns a negative code when the network is not loaded.
-int mlp_warm_start(MlpState& m, const DevParams& P, const NbrView& V, const float4* pos,
-                   const float4* disp_in, float4* disp_out, const float4* vel,
-                   const uint8_t* ncount, cudaStream_t st);
+int mlp_warm_start(MlpState& m, const DevParams& P, const NbrView& V, const PD* pd,
+                   PD* pd_out, const float4* vel, const uint8_t* ncount, cudaStream_t st);
 
 }  // namespace sphpc

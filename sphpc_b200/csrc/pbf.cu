@@ -4,7 +4,8 @@
 // neighbour loop visits the bucket of the particle in the reference's order
 // (for_each_neighbor).  Sums are FP32 (density with Kahan compensation);
 // the box clamp, the SDF lookup and the position update are FP64 on the
-// canonical double x* = x + d.
+// canonical double x* = x + d.  Particle records {x, d} are read with one
+// 256-bit load per neighbour.
 #include "kernels.cuh"
 
 namespace sphpc {
@@ -17,6 +18,11 @@ struct Pair {
 
 // x*_p - x*_q as (x_p - x_q) + (d_p - d_q): exact in the first term for any
 // box size, so the FP32 pair geometry keeps its relative precision.
+__device__ __forceinline__ void ld_rw(const PD* base, int i, float4& x, float4& d) {
+  x = base[i].x;
+  d = base[i].d;
+}
+
 __device__ __forceinline__ Pair pair_geom(const float4 xp, const float4 dp, const float4 xq,
                                           const float4 dq) {
   Pair g;
@@ -67,11 +73,14 @@ __global__ void __launch_bounds__(kBlock)
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   double err = 0.0;
   if (p < P.n) {
-    const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+    float4 xp, dp;
+    ld_pd(a.pd, p, xp, dp);
     float rho = P.W0m, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
     for_each_neighbor(V, p, [&](int q) {
-      const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), __ldg(a.disp + q));
+      float4 xq, dq;
+      ld_pd(a.pd, q, xq, dq);
+      const Pair g = pair_geom(xp, dp, xq, dq);
       if (MODE != 2) {
         const float t = P.h2 - g.r2;
         const float w = t > 0.0f ? P.Wn_m * t * t * t : 0.0f;
@@ -100,7 +109,7 @@ __global__ void __launch_bounds__(kBlock)
       sC += sgx * sgx + sgy * sgy + sgz * sgz;
       sC *= P.inv_rho0_sq;
       const float lam = -C / (sC + P.lambda_eps);
-      a.disp_out[p] = make_float4(dp.x, dp.y, dp.z, lam);
+      st_pd(a.pd_out, p, xp, make_float4(dp.x, dp.y, dp.z, lam));
       if (a.lam) a.lam[p] = lam;
     }
     if (RESID) err = fmax((double)rho / (double)P.rho0 - 1.0, 0.0);
@@ -113,12 +122,14 @@ __global__ void __launch_bounds__(kBlock)
     k_position(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  float4 xp, dp;
+  ld_pd(a.pd, p, xp, dp);
   const float lp = dp.w;
   float ax = 0.f, ay = 0.f, az = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    const float4 dq = __ldg(a.disp + q);
-    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
+    const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float hm = P.h - r;
@@ -156,8 +167,9 @@ __global__ void __launch_bounds__(kBlock)
   if (SDF) sdf_collide(P, xs, ys, zs);
   const double ex = __dsub_rn(xs, (double)xp.x), ey = __dsub_rn(ys, (double)xp.y),
                ez = __dsub_rn(zs, (double)xp.z);
-  a.disp_out[p] = make_float4(__double2float_rn(ex), __double2float_rn(ey),
-                              __double2float_rn(ez), a.rho[p]);
+  st_pd(a.pd_out, p, xp,
+        make_float4(__double2float_rn(ex), __double2float_rn(ey), __double2float_rn(ez),
+                    a.rho[p]));
   if (a.last) {
     // UpdateVelocities, particles.c:814-837
     float vx = __double2float_rn(__ddiv_rn(ex, P.dt_d));
@@ -174,7 +186,9 @@ template <bool SDF>
 __global__ void __launch_bounds__(kBlock) k_apply_dp(const DevParams P, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 xp = __ldg(a.pos + p), dp = a.disp_out[p], dd = __ldg(a.dp + p);
+  float4 xp, dp;
+  ld_rw(a.pd_out, p, xp, dp);
+  const float4 dd = __ldg(a.dp + p);
   double xs = __dadd_rn(xstar_d(xp.x, dp.x), (double)dd.x);
   double ys = __dadd_rn(xstar_d(xp.y, dp.y), (double)dd.y);
   double zs = __dadd_rn(xstar_d(xp.z, dp.z), (double)dd.z);
@@ -182,7 +196,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_dp(const DevParams P, const Pa
   ys = clamp_axis(ys, P.bmin[1], P.bmax[1], P.bmax_eps[1]);
   zs = clamp_axis(zs, P.bmin[2], P.bmax[2], P.bmax_eps[2]);
   if (SDF) sdf_collide(P, xs, ys, zs);
-  a.disp_out[p] = make_float4(__double2float_rn(__dsub_rn(xs, (double)xp.x)),
+  a.pd_out[p].d = make_float4(__double2float_rn(__dsub_rn(xs, (double)xp.x)),
                               __double2float_rn(__dsub_rn(ys, (double)xp.y)),
                               __double2float_rn(__dsub_rn(zs, (double)xp.z)), dp.w);
 }
@@ -191,11 +205,13 @@ __global__ void __launch_bounds__(kBlock)
     k_color(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  float4 xp, dp;
+  ld_pd(a.pd, p, xp, dp);
   float cx = 0.f, cy = 0.f, cz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    const float4 dq = __ldg(a.disp + q);
-    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
+    const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float t = P.h2 - r * r;
@@ -226,15 +242,17 @@ __global__ void __launch_bounds__(kBlock)
     k_tension(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  float4 xp, dp;
+  ld_pd(a.pd, p, xp, dp);
   const float4 cp = __ldg(a.color + p);
   const float rp = dp.w;
   const float kcoh = -20.0f * P.gamma * P.m * P.m;
   const float kcur = -P.gamma * P.m;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    const float4 dq = __ldg(a.disp + q);
-    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
+    const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float4 cq = __ldg(a.color + q);
@@ -256,12 +274,14 @@ __global__ void __launch_bounds__(kBlock)
     k_xsph(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  float4 xp, dp;
+  ld_pd(a.pd, p, xp, dp);
   const float4 vp = __ldg(a.vel + p);
   float sx = 0.f, sy = 0.f, sz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    const float4 dq = __ldg(a.disp + q);
-    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
+    const Pair g = pair_geom(xp, dp, xq, dq);
     // particles.c:439 evaluates x^2 + y^2 * z^2 (kept unless xsph_exact)
     const float rr = P.xsph_exact ? g.r2 : g.dx * g.dx + g.dy * g.dy * g.dz * g.dz;
     const float t = P.h2 - rr;
@@ -274,20 +294,25 @@ __global__ void __launch_bounds__(kBlock)
   a.vel_out[p] = make_float4(vp.x + P.c_xsph * sx, vp.y + P.c_xsph * sy,
                              vp.z + P.c_xsph * sz, 0.0f);
   if (a.write_pos)
-    a.pos_out[p] = make_float4(__double2float_rn(xstar_d(xp.x, dp.x)),
-                               __double2float_rn(xstar_d(xp.y, dp.y)),
-                               __double2float_rn(xstar_d(xp.z, dp.z)), 0.0f);
+    st_pd(a.pd_out, p,
+          make_float4(__double2float_rn(xstar_d(xp.x, dp.x)),
+                      __double2float_rn(xstar_d(xp.y, dp.y)),
+                      __double2float_rn(xstar_d(xp.z, dp.z)), 0.0f),
+          make_float4(0.f, 0.f, 0.f, dp.w));
 }
 
 __global__ void __launch_bounds__(kBlock)
     k_vorticity(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  float4 xp, dp;
+  ld_pd(a.pd, p, xp, dp);
   const float4 vp = __ldg(a.vel + p);
   float wx = 0.f, wy = 0.f, wz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), __ldg(a.disp + q));
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
+    const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float hm = P.h - r;
@@ -306,10 +331,13 @@ __global__ void __launch_bounds__(kBlock)
     k_confinement(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 xp = __ldg(a.pos + p), dp = __ldg(a.disp + p);
+  float4 xp, dp;
+  ld_pd(a.pd, p, xp, dp);
   float ex = 0.f, ey = 0.f, ez = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    const Pair g = pair_geom(xp, dp, __ldg(a.pos + q), __ldg(a.disp + q));
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
+    const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float hm = P.h - r;
@@ -329,9 +357,11 @@ __global__ void __launch_bounds__(kBlock)
   v.z += s * (nx * w.y - ny * w.x);
   a.vel[p] = v;
   if (a.write_pos)
-    a.pos_out[p] = make_float4(__double2float_rn(xstar_d(xp.x, dp.x)),
-                               __double2float_rn(xstar_d(xp.y, dp.y)),
-                               __double2float_rn(xstar_d(xp.z, dp.z)), 0.0f);
+    st_pd(a.pd_out, p,
+          make_float4(__double2float_rn(xstar_d(xp.x, dp.x)),
+                      __double2float_rn(xstar_d(xp.y, dp.y)),
+                      __double2float_rn(xstar_d(xp.z, dp.z)), 0.0f),
+          make_float4(0.f, 0.f, 0.f, dp.w));
 }
 
 __global__ void __launch_bounds__(kBlock) k_gravity(const DevParams P, float4* vel) {
@@ -345,29 +375,28 @@ __global__ void __launch_bounds__(kBlock) k_gravity(const DevParams P, float4* v
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_predict(const DevParams P, const float4* __restrict__ pos, const float4* __restrict__ vel,
-              float4* __restrict__ disp) {
+    k_predict(const DevParams P, PD* pd, const float4* __restrict__ vel) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 x = pos[p], v = vel[p];
+  const float4 x = pd[p].x, v = vel[p];
   double xs = __dadd_rn((double)x.x, __dmul_rn((double)v.x, P.dt_d));
   double ys = __dadd_rn((double)x.y, __dmul_rn((double)v.y, P.dt_d));
   double zs = __dadd_rn((double)x.z, __dmul_rn((double)v.z, P.dt_d));
   xs = clamp_axis(xs, P.bmin[0], P.bmax[0], P.bmax_eps[0]);
   ys = clamp_axis(ys, P.bmin[1], P.bmax[1], P.bmax_eps[1]);
   zs = clamp_axis(zs, P.bmin[2], P.bmax[2], P.bmax_eps[2]);
-  const float w = disp[p].w;
-  disp[p] = make_float4(__double2float_rn(__dsub_rn(xs, (double)x.x)),
+  const float w = pd[p].d.w;
+  pd[p].d = make_float4(__double2float_rn(__dsub_rn(xs, (double)x.x)),
                         __double2float_rn(__dsub_rn(ys, (double)x.y)),
                         __double2float_rn(__dsub_rn(zs, (double)x.z)), w);
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_update_velocities(const DevParams P, const float4* __restrict__ disp,
+    k_update_velocities(const DevParams P, const PD* __restrict__ pd,
                         float4* __restrict__ vel) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 d = disp[p];
+  const float4 d = pd[p].d;
   float vx = __double2float_rn(__ddiv_rn((double)d.x, P.dt_d));
   float vy = __double2float_rn(__ddiv_rn((double)d.y, P.dt_d));
   float vz = __double2float_rn(__ddiv_rn((double)d.z, P.dt_d));
@@ -378,27 +407,26 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_update_positions(const DevParams P, const float4* __restrict__ pos, float4* disp,
-                       float4* pos_out) {
+    k_update_positions(const DevParams P, PD* pd) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const float4 x = pos[p];
-  const float4 d = disp[p];
+  const float4 x = pd[p].x;
+  const float4 d = pd[p].d;
   const float nx = __double2float_rn(xstar_d(x.x, d.x));
   const float ny = __double2float_rn(xstar_d(x.y, d.y));
   const float nz = __double2float_rn(xstar_d(x.z, d.z));
-  pos_out[p] = make_float4(nx, ny, nz, 0.0f);
+  pd[p].x = make_float4(nx, ny, nz, 0.0f);
   // keep x* unchanged: d' = x* - x_new (exactly representable residue)
-  disp[p] = make_float4(__double2float_rn(__dsub_rn(xstar_d(x.x, d.x), (double)nx)),
+  pd[p].d = make_float4(__double2float_rn(__dsub_rn(xstar_d(x.x, d.x), (double)nx)),
                         __double2float_rn(__dsub_rn(xstar_d(x.y, d.y), (double)ny)),
                         __double2float_rn(__dsub_rn(xstar_d(x.z, d.z), (double)nz)), d.w);
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_pack_w(const DevParams P, float4* disp, const float* __restrict__ src) {
+    k_pack_w(const DevParams P, PD* pd, const float* __restrict__ src) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  reinterpret_cast<float*>(disp)[4 * (size_t)p + 3] = src[p];
+  pd[p].d.w = src[p];
 }
 
 __global__ void __launch_bounds__(kBlock)
@@ -471,20 +499,17 @@ void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a,
 void launch_gravity(const DevParams& P, float4* vel, cudaStream_t st) {
   k_gravity<<<grid_for(P.n), kBlock, 0, st>>>(P, vel);
 }
-void launch_predict(const DevParams& P, const float4* pos, const float4* vel, float4* disp,
-                    cudaStream_t st) {
-  k_predict<<<grid_for(P.n), kBlock, 0, st>>>(P, pos, vel, disp);
+void launch_predict(const DevParams& P, PD* pd, const float4* vel, cudaStream_t st) {
+  k_predict<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, vel);
 }
-void launch_update_velocities(const DevParams& P, const float4* disp, float4* vel,
-                              cudaStream_t st) {
-  k_update_velocities<<<grid_for(P.n), kBlock, 0, st>>>(P, disp, vel);
+void launch_update_velocities(const DevParams& P, const PD* pd, float4* vel, cudaStream_t st) {
+  k_update_velocities<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, vel);
 }
-void launch_update_positions(const DevParams& P, const float4* pos, float4* disp,
-                             float4* pos_out, cudaStream_t st) {
-  k_update_positions<<<grid_for(P.n), kBlock, 0, st>>>(P, pos, disp, pos_out);
+void launch_update_positions(const DevParams& P, PD* pd, cudaStream_t st) {
+  k_update_positions<<<grid_for(P.n), kBlock, 0, st>>>(P, pd);
 }
-void launch_pack_w(const DevParams& P, float4* disp, const float* src, cudaStream_t st) {
-  k_pack_w<<<grid_for(P.n), kBlock, 0, st>>>(P, disp, src);
+void launch_pack_w(const DevParams& P, PD* pd, const float* src, cudaStream_t st) {
+  k_pack_w<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, src);
 }
 void launch_collisions_double(const DevParams& P, double* x, double* y, double* z, int n,
                               cudaStream_t st) {

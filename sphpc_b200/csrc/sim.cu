@@ -80,7 +80,7 @@ class DeviceSim {
   int bx = 0, by = 0, passes = 1;
 
   // per-particle arrays, slot order
-  float4 *pos = nullptr, *pos_alt = nullptr, *disp = nullptr, *disp_alt = nullptr;
+  PD *pd = nullptr, *pd_alt = nullptr;
   float4 *vel = nullptr, *vel_alt = nullptr, *color = nullptr, *omega = nullptr, *dp = nullptr;
   float *rho = nullptr, *lam = nullptr;
   // alternates for the full reorder of the per-function path
@@ -98,7 +98,6 @@ class DeviceSim {
   uint32_t* sort_aux = nullptr;
   double* stage = nullptr;  // 20 * n doubles for host transfers
   bool nbr_valid = false;
-  bool disp_zero_pending = false;
 
   MlpState mlp{};
 
@@ -127,7 +126,7 @@ class DeviceSim {
   uint32_t* err() { return small + 2; }
 
   void release() {
-    dfree(pos); dfree(pos_alt); dfree(disp); dfree(disp_alt); dfree(vel); dfree(vel_alt);
+    dfree(pd); dfree(pd_alt); dfree(vel); dfree(vel_alt);
     dfree(color); dfree(omega); dfree(dp); dfree(rho); dfree(lam);
     dfree(color_alt); dfree(omega_alt); dfree(dp_alt); dfree(rho_alt); dfree(lam_alt);
     dfree(ids); dfree(ids_spare); dfree(keys_by_id); dfree(loc_by_id); dfree(cellp);
@@ -145,8 +144,7 @@ class DeviceSim {
 
   int alloc(int n_) {
     n = n_;
-    SPHPC_RC(dalloc(&pos, n)); SPHPC_RC(dalloc(&pos_alt, n));
-    SPHPC_RC(dalloc(&disp, n)); SPHPC_RC(dalloc(&disp_alt, n));
+    SPHPC_RC(dalloc(&pd, n)); SPHPC_RC(dalloc(&pd_alt, n));
     SPHPC_RC(dalloc(&vel, n)); SPHPC_RC(dalloc(&vel_alt, n));
     SPHPC_RC(dalloc(&color, n)); SPHPC_RC(dalloc(&omega, n)); SPHPC_RC(dalloc(&dp, n));
     SPHPC_RC(dalloc(&rho, n)); SPHPC_RC(dalloc(&lam, n));
@@ -168,7 +166,7 @@ class DeviceSim {
     sort.lookback = sort_aux + (size_t)kMaxPasses * kRadix + kMaxPasses + 4;
     SPHPC_CK(cudaMemsetAsync(small, 0, 8 * sizeof(uint32_t), stream));
     SPHPC_CK(cudaMemsetAsync(sort_aux, 0, aux * sizeof(uint32_t), stream));
-    SPHPC_CK(cudaMemsetAsync(disp, 0, sizeof(float4) * n, stream));
+    SPHPC_CK(cudaMemsetAsync(pd, 0, sizeof(PD) * n, stream));
     SPHPC_CK(cudaMemsetAsync(vel, 0, sizeof(float4) * n, stream));
     SPHPC_CK(cudaMemsetAsync(color, 0, sizeof(float4) * n, stream));
     SPHPC_CK(cudaMemsetAsync(omega, 0, sizeof(float4) * n, stream));
@@ -295,14 +293,6 @@ class DeviceSim {
 
   DevParams params(const Params& prm, const AABB* b, const Obstacle* ob) const;
 
-  int zero_disp_if_pending() {
-    if (disp_zero_pending) {
-      SPHPC_CK(cudaMemsetAsync(disp, 0, sizeof(float4) * n, stream));
-      disp_zero_pending = false;
-    }
-    return SPHPC_OK;
-  }
-
   int find_neighbors(const DevParams& P, bool predict, bool full, bool move_vel);
   int run_step(const DevParams& P, const Params& prm);
 };
@@ -395,7 +385,7 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
   {
     Scope sc(this, "hash");
     SPHPC_CK(cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * kMaxPasses * kRadix, stream));
-    launch_hash(P, pos, vel, disp, ids, keys_by_id, loc_by_id, sort.hist, passes, predict, err(),
+    launch_hash(P, pd, vel, ids, keys_by_id, loc_by_id, sort.hist, passes, predict, err(),
                 stream);
     launches += 1;
   }
@@ -426,11 +416,10 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
       ex.in1[1] = lam; ex.out1[1] = lam_alt;
     }
     const bool mv = move_vel || full;
-    launch_reorder(P, R, loc_by_id, pos, vel, disp, pos_alt, vel_alt, disp_alt, xsa, cellp,
-                   predict, mv, &ex, stream);
+    launch_reorder(P, R, loc_by_id, pd, vel, pd_alt, vel_alt, xsa, cellp, predict, mv, &ex,
+                   stream);
     launches += 1;
-    std::swap(pos, pos_alt);
-    std::swap(disp, disp_alt);
+    std::swap(pd, pd_alt);
     if (mv) std::swap(vel, vel_alt);
     if (full) {
       std::swap(color, color_alt);
@@ -446,12 +435,11 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
   }
   {
     Scope sc(this, "build_neighbors");
-    launch_build_neighbors(P, view(), pos, disp, xsa, cellp, nbr, ncount, stream);
+    launch_build_neighbors(P, view(), pd, xsa, cellp, nbr, ncount, stream);
     launches += 1;
   }
   SPHPC_CK(cudaGetLastError());
   nbr_valid = true;
-  disp_zero_pending = false;
   return SPHPC_OK;
 }
 
@@ -465,7 +453,6 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   SPHPC_RC(find_neighbors(P, true, false, warm));
   const NbrView V = view();
   PassArgs a{};
-  a.pos = pos;
   a.rho = rho;
   a.vel = vel;
   a.vel_out = vel;
@@ -473,14 +460,15 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   const int fixed_iters = solver.solve_iterations;
   const bool adaptive = solver.adaptive != 0;
   const int max_iters = adaptive ? solver.max_iterations : fixed_iters;
-  int k0 = 0;
   last_warm = 0.0;
+  // The current records are always in `pd`; the density/lambda pass writes
+  // pd_alt and the position pass writes back into pd.
   if (warm) {
     // warm start: features -> MLP lambda0 -> one position pass (stiffness 1)
     Scope sc(this, "mlp_warm_start");
-    SPHPC_RC(mlp_warm_start(mlp, P, V, pos, disp, disp_alt, vel, ncount, stream));
-    a.disp = disp_alt;
-    a.disp_out = disp;
+    SPHPC_RC(mlp_warm_start(mlp, P, V, pd, pd_alt, vel, ncount, stream));
+    a.pd = pd_alt;
+    a.pd_out = pd;
     a.stiffness = 1.0f;
     a.last = 0;
     launch_position(P, V, a, 0, stream);
@@ -489,12 +477,12 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   }
   int iters = 0;
   bool converged = false;
-  for (int k = k0; k < max_iters; ++k) {
+  for (int k = 0; k < max_iters; ++k) {
     {
       Scope sc(this, "density_lambda");
       SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
-      a.disp = disp;
-      a.disp_out = disp_alt;
+      a.pd = pd;
+      a.pd_out = pd_alt;
       a.lam = nullptr;
       launch_density_lambda(P, V, a, 0, true, stream);
       launches += 1;
@@ -512,8 +500,8 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     }
     {
       Scope sc(this, "position");
-      a.disp = disp_alt;
-      a.disp_out = disp;
+      a.pd = pd_alt;
+      a.pd_out = pd;
       // the warm-started pass counts as substep 0; plain iterations continue
       a.stiffness = stiffness_of(solver.stiffness_k, warm ? k + 1 : k);
       a.last = (!adaptive && k == max_iters - 1) ? 1 : 0;
@@ -526,17 +514,18 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     // converged (or cap reached): velocities from x* and the freshest density
     Scope sc(this, "velocity");
     if (converged || max_iters == 0) {
-      launch_pack_w(P, disp, rho, stream);
+      launch_pack_w(P, pd, rho, stream);
       launches += 1;
     }
-    launch_update_velocities(P, disp, vel, stream);
+    launch_update_velocities(P, pd, vel, stream);
     launches += 1;
   }
   last_iterations = iters + (warm ? 1 : 0);
   last_converged = converged ? 1 : 0;
-  // post-solve passes (simulation.c:93-106)
-  a.disp = disp;
-  a.pos_out = pos_alt;
+  // post-solve passes (simulation.c:93-106); the last one writes x = x*,
+  // d = 0 (UpdatePositions) into pd_alt
+  a.pd = pd;
+  a.pd_out = pd_alt;
   if (solver.surface_tension) {
     Scope sc(this, "surface_tension");
     a.color = color;
@@ -564,8 +553,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     launches += 2;
   }
   std::swap(vel, vel_alt);
-  std::swap(pos, pos_alt);
-  disp_zero_pending = true;  // UpdatePositions: x = x*, so x* - x = 0
+  std::swap(pd, pd_alt);
   SPHPC_CK(cudaGetLastError());
   (void)prm;
   return SPHPC_OK;
@@ -590,17 +578,17 @@ static DeviceSim* find_sim(const Particles* p) {
 
 // ---- host <-> device transfers ----
 
-__global__ void k_download(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ pos,
-                           const float4* __restrict__ disp, const float4* __restrict__ vel,
+__global__ void k_download(int n, const uint32_t* __restrict__ ids, const PD* __restrict__ pd,
+                           const float4* __restrict__ vel,
                            const float4* __restrict__ dp, const float4* __restrict__ omega,
                            const float4* __restrict__ color, const float* __restrict__ rho,
-                           const float* __restrict__ lam, int disp_zero, double* __restrict__ out) {
+                           const float* __restrict__ lam, double* __restrict__ out) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const size_t N = (size_t)n;
   const uint32_t id = ids[p];
-  const float4 x = pos[p];
-  const float4 d = disp_zero ? make_float4(0.f, 0.f, 0.f, 0.f) : disp[p];
+  const float4 x = pd[p].x;
+  const float4 d = pd[p].d;
   const float4 v = vel[p], q = dp[p], w = omega[p], c = color[p];
   out[0 * N + id] = xstar_d(x.x, d.x);
   out[1 * N + id] = xstar_d(x.y, d.y);
@@ -615,7 +603,7 @@ __global__ void k_download(int n, const uint32_t* __restrict__ ids, const float4
 }
 
 __global__ void k_upload(int n, const uint32_t* __restrict__ ids, const double* __restrict__ in,
-                         unsigned mask, float4* pos, float4* disp, float4* vel, float4* dp,
+                         unsigned mask, PD* pd, float4* vel, float4* dp,
                          float4* omega, float4* color, float* rho, float* lam) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
@@ -624,14 +612,14 @@ __global__ void k_upload(int n, const uint32_t* __restrict__ ids, const double* 
   auto f = [&](int k) { return in[(size_t)k * N + id]; };
   if (mask & (1u << 3)) {
     const float x = (float)f(3), y = (float)f(4), z = (float)f(5);
-    pos[p] = make_float4(x, y, z, 0.f);
-    float4 d = make_float4(0.f, 0.f, 0.f, disp[p].w);
+    pd[p].x = make_float4(x, y, z, 0.f);
+    float4 d = make_float4(0.f, 0.f, 0.f, pd[p].d.w);
     if (mask & (1u << 0)) {
       d.x = (float)(f(0) - (double)x);
       d.y = (float)(f(1) - (double)y);
       d.z = (float)(f(2) - (double)z);
     }
-    disp[p] = d;
+    pd[p].d = d;
   }
   if (mask & (1u << 6)) vel[p] = make_float4((float)f(6), (float)f(7), (float)f(8), 0.f);
   if (mask & (1u << 9)) dp[p] = make_float4((float)f(9), (float)f(10), (float)f(11), 0.f);
@@ -649,14 +637,14 @@ __global__ void k_iota(uint32_t* a, int n) {
 // FP64 diagnostics: [0] max err (u64 bits), [1] sum err, [2] sum |v|^2,
 // [3..5] sum x, [6..8] sum v
 __global__ void __launch_bounds__(kBlock)
-    k_diag(int n, float rho0, const float4* __restrict__ pos, const float4* __restrict__ vel,
+    k_diag(int n, float rho0, const PD* __restrict__ pd, const float4* __restrict__ vel,
            const float* __restrict__ rho, double* __restrict__ out) {
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const double e = fmax((double)rho[p] / (double)rho0 - 1.0, 0.0);
     v[0] = fmax(v[0], e);
     v[1] += e;
-    const float4 u = vel[p], x = pos[p];
+    const float4 u = vel[p], x = pd[p].x;
     v[2] += (double)u.x * u.x + (double)u.y * u.y + (double)u.z * u.z;
     v[3] += x.x; v[4] += x.y; v[5] += x.z;
     v[6] += u.x; v[7] += u.y; v[8] += u.z;
@@ -771,9 +759,9 @@ int sphpc_update_host_fields(struct Particles* p, unsigned int field_mask) {
   SPHPC_SIM(s, p);
   SPHPC_RC(s->ensure_stage());
   const int n = s->n;
-  k_download<<<grid_for(n), kBlock, 0, s->stream>>>(n, s->ids, s->pos, s->disp, s->vel, s->dp,
+  k_download<<<grid_for(n), kBlock, 0, s->stream>>>(n, s->ids, s->pd, s->vel, s->dp,
                                                     s->omega, s->color, s->rho, s->lam,
-                                                    s->disp_zero_pending ? 1 : 0, s->stage);
+                                                    s->stage);
   SPHPC_CK(cudaGetLastError());
   double* fields[20] = {p->x_star, p->y_star, p->z_star, p->x, p->y, p->z, p->v_x, p->v_y,
                         p->v_z, p->dp_x, p->dp_y, p->dp_z, p->w_x, p->w_y, p->w_z,
@@ -812,10 +800,8 @@ int sphpc_update_device_fields(struct Particles* p, unsigned int field_mask) {
   }
   if (!(mask & (1u << 3)))
     return set_error(SPHPC_EINVAL, "sphpc_update_device: x, y, z are required");
-  SPHPC_RC(s->zero_disp_if_pending());
-  k_upload<<<grid_for(n), kBlock, 0, s->stream>>>(n, s->ids, s->stage, mask, s->pos, s->disp,
-                                                  s->vel, s->dp, s->omega, s->color, s->rho,
-                                                  s->lam);
+  k_upload<<<grid_for(n), kBlock, 0, s->stream>>>(n, s->ids, s->stage, mask, s->pd, s->vel,
+                                                  s->dp, s->omega, s->color, s->rho, s->lam);
   SPHPC_CK(cudaGetLastError());
   SPHPC_CK(cudaStreamSynchronize(s->stream));
   return SPHPC_OK;
@@ -914,7 +900,6 @@ int FindAllNeighbors(const struct Particles* particles, const struct Params* par
   (void)neighbors;
   SPHPC_SIM(s, particles);
   if (!params) return set_error(SPHPC_EINVAL, "FindAllNeighbors: null params");
-  SPHPC_RC(s->zero_disp_if_pending());
   const DevParams P = s->params(*params, nullptr, nullptr);
   return s->find_neighbors(P, false, true, true);
 }
@@ -963,10 +948,9 @@ int sphpc_get_cell_data(const struct Particles* particles, unsigned int* hash_va
 
 // ---- step functions (one stage each) ----
 
-#define SPHPC_STAGE_BEGIN(particles, params)                               \
-  SPHPC_SIM(s, particles);                                                 \
-  if (!(params)) return set_error(SPHPC_EINVAL, "%s: null params", __func__); \
-  SPHPC_RC(s->zero_disp_if_pending());
+#define SPHPC_STAGE_BEGIN(particles, params) \
+  SPHPC_SIM(s, particles);                   \
+  if (!(params)) return set_error(SPHPC_EINVAL, "%s: null params", __func__);
 
 #define SPHPC_NEED_NBR()                                                                  \
   if (!s->nbr_valid)                                                                      \
@@ -986,7 +970,7 @@ int PredictPositions(struct Particles* particles, const struct Params* params,
   SPHPC_STAGE_BEGIN(particles, params);
   if (!boundary_global) return set_error(SPHPC_EINVAL, "PredictPositions: null boundary");
   const DevParams P = s->params(*params, boundary_global, nullptr);
-  launch_predict(P, s->pos, s->vel, s->disp, s->stream);
+  launch_predict(P, s->pd, s->vel, s->stream);
   SPHPC_LAUNCH_DONE();
 }
 
@@ -997,8 +981,7 @@ int ComputeDensities(struct Particles* particles, const struct Params* params,
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
   PassArgs a{};
-  a.pos = s->pos;
-  a.disp = s->disp;
+  a.pd = s->pd;
   a.rho = s->rho;
   a.resid = s->resid;
   SPHPC_CK(cudaMemsetAsync(s->resid, 0, 2 * sizeof(double), s->stream));
@@ -1013,13 +996,12 @@ int ComputeLambda(struct Particles* particles, const struct Params* params,
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
   PassArgs a{};
-  a.pos = s->pos;
-  a.disp = s->disp;
-  a.disp_out = s->disp_alt;
+  a.pd = s->pd;
+  a.pd_out = s->pd_alt;
   a.rho = s->rho;
   a.lam = s->lam;
   launch_density_lambda(P, s->view(), a, 2, false, s->stream);
-  std::swap(s->disp, s->disp_alt);
+  std::swap(s->pd, s->pd_alt);
   SPHPC_LAUNCH_DONE();
 }
 
@@ -1029,10 +1011,9 @@ int UpdateDPs(struct Particles* particles, const struct Params* params,
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
-  launch_pack_w(P, s->disp, s->lam, s->stream);
+  launch_pack_w(P, s->pd, s->lam, s->stream);
   PassArgs a{};
-  a.pos = s->pos;
-  a.disp = s->disp;
+  a.pd = s->pd;
   a.dp = s->dp;
   a.rho = s->rho;
   a.stiffness = stiffness_of(s->solver.stiffness_k, substep);
@@ -1046,8 +1027,7 @@ int UpdatePositionStars(struct Particles* particles, const struct AABB* boundary
   if (!boundary_global) return set_error(SPHPC_EINVAL, "UpdatePositionStars: null boundary");
   const DevParams P = s->params(*params, boundary_global, obstacle);
   PassArgs a{};
-  a.pos = s->pos;
-  a.disp_out = s->disp;
+  a.pd_out = s->pd;
   a.dp = s->dp;
   launch_apply_dp(P, a, s->stream);
   SPHPC_LAUNCH_DONE();
@@ -1056,7 +1036,7 @@ int UpdatePositionStars(struct Particles* particles, const struct AABB* boundary
 int UpdateVelocities(struct Particles* particles, const struct Params* params) {
   SPHPC_STAGE_BEGIN(particles, params);
   const DevParams P = s->params(*params, nullptr, nullptr);
-  launch_update_velocities(P, s->disp, s->vel, s->stream);
+  launch_update_velocities(P, s->pd, s->vel, s->stream);
   SPHPC_LAUNCH_DONE();
 }
 
@@ -1066,10 +1046,9 @@ int ComputeSurfaceTension(struct Particles* particles, const struct Params* para
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
-  launch_pack_w(P, s->disp, s->rho, s->stream);
+  launch_pack_w(P, s->pd, s->rho, s->stream);
   PassArgs a{};
-  a.pos = s->pos;
-  a.disp = s->disp;
+  a.pd = s->pd;
   a.color = s->color;
   a.vel = s->vel;
   launch_color(P, s->view(), a, s->stream);
@@ -1083,10 +1062,9 @@ int ApplyViscosity(struct Particles* particles, const struct Params* params,
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
-  launch_pack_w(P, s->disp, s->rho, s->stream);
+  launch_pack_w(P, s->pd, s->rho, s->stream);
   PassArgs a{};
-  a.pos = s->pos;
-  a.disp = s->disp;
+  a.pd = s->pd;
   a.vel = s->vel;
   a.vel_out = s->vel_alt;
   launch_xsph(P, s->view(), a, s->stream);
@@ -1101,8 +1079,7 @@ int ComputeVorticity(struct Particles* particles, const struct Params* params,
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
   PassArgs a{};
-  a.pos = s->pos;
-  a.disp = s->disp;
+  a.pd = s->pd;
   a.vel = s->vel;
   a.omega = s->omega;
   launch_vorticity(P, s->view(), a, s->stream);
@@ -1116,8 +1093,7 @@ int ApplyVorticityConfinement(struct Particles* particles, const struct Params* 
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
   PassArgs a{};
-  a.pos = s->pos;
-  a.disp = s->disp;
+  a.pd = s->pd;
   a.vel = s->vel;
   a.omega = s->omega;
   launch_confinement(P, s->view(), a, s->stream);
@@ -1126,10 +1102,9 @@ int ApplyVorticityConfinement(struct Particles* particles, const struct Params* 
 
 int UpdatePositions(struct Particles* particles) {
   SPHPC_SIM(s, particles);
-  SPHPC_RC(s->zero_disp_if_pending());
   DevParams P{};
   P.n = s->n;
-  launch_update_positions(P, s->pos, s->disp, s->pos, s->stream);
+  launch_update_positions(P, s->pd, s->stream);
   SPHPC_LAUNCH_DONE();
 }
 
@@ -1153,7 +1128,7 @@ int sphpc_diagnostics(const struct Particles* particles, struct SphpcDiag* diag)
   if (!diag) return set_error(SPHPC_EINVAL, "sphpc_diagnostics: null");
   double* out = s->resid + 4;
   SPHPC_CK(cudaMemsetAsync(out, 0, 9 * sizeof(double), s->stream));
-  k_diag<<<148 * 2, kBlock, 0, s->stream>>>(s->n, (float)s->rho0, s->pos, s->vel, s->rho, out);
+  k_diag<<<148 * 2, kBlock, 0, s->stream>>>(s->n, (float)s->rho0, s->pd, s->vel, s->rho, out);
   double h[9];
   SPHPC_CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
   SPHPC_CK(cudaStreamSynchronize(s->stream));

@@ -3,10 +3,11 @@
 //
 // State layout in HBM (slot order = particles sorted by uniform-grid cell
 // key, rebuilt every step):
-//   pos[n]   float4  x, the step-start position (.w unused)
-//   disp[n]  float4  d = x* - x, the predicted-position displacement.
-//                    .w carries lambda after the density/lambda pass and the
-//                    density after the position pass.
+//   pd[n]    PD      32-byte record {x, d}: x the step-start position (.w
+//                    unused), d = x* - x the predicted-position displacement
+//                    (.w carries lambda after the density/lambda pass and the
+//                    density after the position pass).  A neighbour's record
+//                    is one 256-bit load.
 //   xsa[n]   float4  x* as absolute FP32 (neighbour-build candidate test)
 //   vel[n]   float4  v
 //   ids[n]   u32     original particle index of each slot
@@ -30,6 +31,25 @@
 namespace sphpc {
 
 constexpr int kMaxNeighbors = 60;   // MAX_NEIGHBORS, neighbors.h:6
+
+// Position record of one particle: step-start x and displacement d = x* - x.
+struct __align__(32) PD {
+  float4 x;
+  float4 d;
+};
+
+// One 256-bit read-only load of a record (ld.global.nc.v8.f32, sm_100).
+__device__ __forceinline__ void ld_pd(const PD* __restrict__ base, int i, float4& x, float4& d) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(d.x), "=f"(d.y), "=f"(d.z), "=f"(d.w)
+      : "l"(base + i));
+}
+
+__device__ __forceinline__ void st_pd(PD* base, int i, const float4 x, const float4 d) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(base + i),
+               "f"(x.x), "f"(x.y), "f"(x.z), "f"(x.w), "f"(d.x), "f"(d.y), "f"(d.z), "f"(d.w)
+               : "memory");
+}
 
 // Error bits raised by kernels (host reads them back).
 enum : uint32_t {
