@@ -19,6 +19,21 @@ extern "C" {
 int SortByKey(unsigned int *const keys, unsigned int *const values, const int count,
               const void *const cuda_stream);
 
+/* No counterpart in the reference.  The same stable sort as SortByKey for
+ * callers that must not allocate device memory (a host that owns all device
+ * memory through its own pool, or a time-critical loop where a cudaMalloc,
+ * which can synchronise the device or fail under memory pressure, is not
+ * acceptable).  Its scratch is a fixed array of about 2.4 MB inside the
+ * library, held by every GPU that loads the library until the process exits,
+ * so count is limited to 262,144 pairs (larger counts return SPHPC_EINVAL).
+ * It calls no cudaMalloc or cudaFree.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls on a device share the one array:
+ * calls that overlap on the GPU (from several host threads or streams) race
+ * and must be serialised by the caller.  Returns after the sort completes. */
+int SortByKeyNoAlloc(unsigned int *const keys, unsigned int *const values, const int count,
+                     const void *const cuda_stream);
+
 /* thrust_c.h:46-50 (thrust_c.cu:93-105): start_indices[c] =
  * lower_bound(hash_values[0..value_count), c) for c in [0, search_count). */
 int FindLowerBounds(const unsigned int *const hash_values, const int value_count,

@@ -162,6 +162,7 @@ SIGNATURES = {
     "sphpc_profile": ([PP, C.c_int], C.c_int),
     "sphpc_profile_read": ([PP, C.POINTER(KernelTime), C.c_int, C.POINTER(C.c_int)], C.c_int),
     "SortByKey": ([U, U, C.c_int, C.c_void_p], C.c_int),
+    "SortByKeyNoAlloc": ([U, U, C.c_int, C.c_void_p], C.c_int),
     "FindLowerBounds": ([U, C.c_int, C.c_int, U, C.c_void_p], C.c_int),
     "FindUpperBounds": ([U, C.c_int, C.c_int, U, C.c_void_p], C.c_int),
     "CalculateParticleCollisions": ([_DP, _DP, _DP, C.c_int, Obstacle], C.c_int),
