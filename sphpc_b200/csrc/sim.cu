@@ -221,6 +221,7 @@ class DeviceSim {
 
   NbrView view() const {
     NbrView v;
+    v.cellp = cellp;
     v.nbr = nbr;
     v.ncount = ncount;
     v.cstart = cstart;
