@@ -6,11 +6,7 @@
 // the box clamp, the SDF lookup and the position update are FP64 on the
 // canonical double x* = x + d.  Particle records {x, d} are read with one
 // 256-bit load per neighbour.
-#include <map>
-#include <mutex>
-
 #include "kernels.cuh"
-#include "stage.cuh"
 
 namespace sphpc {
 
@@ -52,7 +48,7 @@ __device__ __forceinline__ void block_resid(double e, double* resid) {
     m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
     s += __shfl_xor_sync(0xffffffffu, s, o);
   }
-  __shared__ double sm[kStageThreads / 32], ss[kStageThreads / 32];
+  __shared__ double sm[kBlock / 32], ss[kBlock / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) {
     sm[warp] = m;
@@ -61,7 +57,7 @@ __device__ __forceinline__ void block_resid(double e, double* resid) {
   __syncthreads();
   if (threadIdx.x == 0) {
     double bm = 0.0, bs = 0.0;
-    for (int w = 0; w < kStageThreads / 32; ++w) {
+    for (int w = 0; w < kBlock / 32; ++w) {
       bm = fmax(bm, sm[w]);
       bs += ss[w];
     }
@@ -71,26 +67,10 @@ __device__ __forceinline__ void block_resid(double e, double* resid) {
   }
 }
 
-#define SPHPC_COMMA ,
-
-// Shared-memory preamble of a neighbour pass: stage the CTA's neighbourhood
-// records (every thread takes part), then the particle index.
-#define SPHPC_STAGE()                                                  \
-  extern __shared__ __align__(32) unsigned char s_dyn[];               \
-  PD* s_recs = reinterpret_cast<PD*>(s_dyn);                           \
-  __shared__ StageShared s_stage;                                      \
-  stage_load(V, V.cellp, a.pd, s_stage, s_recs);                       \
-  StageCursor cursor;                                                  \
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-
-#define SPHPC_NEIGHBOR_RECORD(q, xq, dq) \
-  float4 xq, dq;                         \
-  cursor.get(s_stage, s_recs, a.pd, q, xq, dq);
-
 template <int MODE, bool RESID>
 __global__ void __launch_bounds__(kBlock)
     k_density_lambda(const DevParams P, const NbrView V, const PassArgs a) {
-  SPHPC_STAGE();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   double err = 0.0;
   if (p < P.n) {
     float4 xp, dp;
@@ -98,7 +78,8 @@ __global__ void __launch_bounds__(kBlock)
     float rho = P.W0m, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
     for_each_neighbor(V, p, [&](int q) {
-      SPHPC_NEIGHBOR_RECORD(q, xq, dq);
+      float4 xq, dq;
+      ld_pd(a.pd, q, xq, dq);
       const Pair g = pair_geom(xp, dp, xq, dq);
       if (MODE != 2) {
         const float t = P.h2 - g.r2;
@@ -139,14 +120,15 @@ __global__ void __launch_bounds__(kBlock)
 template <int MODE, int SCORR_N, bool SDF>
 __global__ void __launch_bounds__(kBlock)
     k_position(const DevParams P, const NbrView V, const PassArgs a) {
-  SPHPC_STAGE();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   float4 xp, dp;
   ld_pd(a.pd, p, xp, dp);
   const float lp = dp.w;
   float ax = 0.f, ay = 0.f, az = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    SPHPC_NEIGHBOR_RECORD(q, xq, dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
     const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
@@ -221,13 +203,14 @@ __global__ void __launch_bounds__(kBlock) k_apply_dp(const DevParams P, const Pa
 
 __global__ void __launch_bounds__(kBlock)
     k_color(const DevParams P, const NbrView V, const PassArgs a) {
-  SPHPC_STAGE();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   float4 xp, dp;
   ld_pd(a.pd, p, xp, dp);
   float cx = 0.f, cy = 0.f, cz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    SPHPC_NEIGHBOR_RECORD(q, xq, dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
     const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
@@ -257,7 +240,7 @@ __device__ __forceinline__ float cohesion(const DevParams& P, float r) {
 
 __global__ void __launch_bounds__(kBlock)
     k_tension(const DevParams P, const NbrView V, const PassArgs a) {
-  SPHPC_STAGE();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   float4 xp, dp;
   ld_pd(a.pd, p, xp, dp);
@@ -267,7 +250,8 @@ __global__ void __launch_bounds__(kBlock)
   const float kcur = -P.gamma * P.m;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    SPHPC_NEIGHBOR_RECORD(q, xq, dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
     const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
@@ -288,14 +272,15 @@ __global__ void __launch_bounds__(kBlock)
 
 __global__ void __launch_bounds__(kBlock)
     k_xsph(const DevParams P, const NbrView V, const PassArgs a) {
-  SPHPC_STAGE();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   float4 xp, dp;
   ld_pd(a.pd, p, xp, dp);
   const float4 vp = __ldg(a.vel + p);
   float sx = 0.f, sy = 0.f, sz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    SPHPC_NEIGHBOR_RECORD(q, xq, dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
     const Pair g = pair_geom(xp, dp, xq, dq);
     // particles.c:439 evaluates x^2 + y^2 * z^2 (kept unless xsph_exact)
     const float rr = P.xsph_exact ? g.r2 : g.dx * g.dx + g.dy * g.dy * g.dz * g.dz;
@@ -318,14 +303,15 @@ __global__ void __launch_bounds__(kBlock)
 
 __global__ void __launch_bounds__(kBlock)
     k_vorticity(const DevParams P, const NbrView V, const PassArgs a) {
-  SPHPC_STAGE();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   float4 xp, dp;
   ld_pd(a.pd, p, xp, dp);
   const float4 vp = __ldg(a.vel + p);
   float wx = 0.f, wy = 0.f, wz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    SPHPC_NEIGHBOR_RECORD(q, xq, dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
     const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
@@ -343,13 +329,14 @@ __global__ void __launch_bounds__(kBlock)
 
 __global__ void __launch_bounds__(kBlock)
     k_confinement(const DevParams P, const NbrView V, const PassArgs a) {
-  SPHPC_STAGE();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   float4 xp, dp;
   ld_pd(a.pd, p, xp, dp);
   float ex = 0.f, ey = 0.f, ez = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    SPHPC_NEIGHBOR_RECORD(q, xq, dq);
+    float4 xq, dq;
+    ld_pd(a.pd, q, xq, dq);
     const Pair g = pair_geom(xp, dp, xq, dq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
@@ -454,51 +441,28 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// Opt every staged kernel in to the dynamic shared memory it needs (once per
-// kernel and device).
-template <class K>
-void stage_attr(K* kernel) {
-  static std::mutex mu;
-  static std::map<std::pair<int, const void*>, bool> done;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  std::lock_guard<std::mutex> lk(mu);
-  auto key = std::make_pair(dev, (const void*)kernel);
-  if (done.count(key)) return;
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(kStageRecords * sizeof(PD)));
-  done[key] = true;
-}
-
-constexpr size_t kStageBytes = kStageRecords * sizeof(PD);
-
-#define SPHPC_LAUNCH_STAGED(kernel, ...)                                            \
-  do {                                                                              \
-    stage_attr(kernel);                                                             \
-    kernel<<<grid_for(P.n, kStageThreads), kStageThreads, kStageBytes, st>>>(__VA_ARGS__); \
-  } while (0)
-
 }  // namespace
 
 void launch_density_lambda(const DevParams& P, const NbrView& V, const PassArgs& a, int mode,
                            bool residual, cudaStream_t st) {
+  const int g = grid_for(P.n);
   if (mode == 0) {
-    if (residual) SPHPC_LAUNCH_STAGED(k_density_lambda<0 SPHPC_COMMA true>, P, V, a);
-    else SPHPC_LAUNCH_STAGED(k_density_lambda<0 SPHPC_COMMA false>, P, V, a);
+    if (residual) k_density_lambda<0, true><<<g, kBlock, 0, st>>>(P, V, a);
+    else k_density_lambda<0, false><<<g, kBlock, 0, st>>>(P, V, a);
   } else if (mode == 1) {
-    if (residual) SPHPC_LAUNCH_STAGED(k_density_lambda<1 SPHPC_COMMA true>, P, V, a);
-    else SPHPC_LAUNCH_STAGED(k_density_lambda<1 SPHPC_COMMA false>, P, V, a);
+    if (residual) k_density_lambda<1, true><<<g, kBlock, 0, st>>>(P, V, a);
+    else k_density_lambda<1, false><<<g, kBlock, 0, st>>>(P, V, a);
   } else {
-    SPHPC_LAUNCH_STAGED(k_density_lambda<2 SPHPC_COMMA false>, P, V, a);
+    k_density_lambda<2, false><<<g, kBlock, 0, st>>>(P, V, a);
   }
 }
 
 void launch_position(const DevParams& P, const NbrView& V, const PassArgs& a, int mode,
                      cudaStream_t st) {
+  const int g = grid_for(P.n);
   const int sn = P.scorr_k != 0.0f ? (P.scorr_n == 4 ? 4 : -1) : 0;
   const bool sdf = P.has_sdf != 0;
-#define SPHPC_POS(M, N, S) \
-  SPHPC_LAUNCH_STAGED(k_position<M SPHPC_COMMA N SPHPC_COMMA S>, P, V, a)
+#define SPHPC_POS(M, N, S) k_position<M, N, S><<<g, kBlock, 0, st>>>(P, V, a)
   if (mode == 0) {
     if (sn == 0) { if (sdf) SPHPC_POS(0, 0, true); else SPHPC_POS(0, 0, false); }
     else if (sn == 4) { if (sdf) SPHPC_POS(0, 4, true); else SPHPC_POS(0, 4, false); }
@@ -517,20 +481,20 @@ void launch_apply_dp(const DevParams& P, const PassArgs& a, cudaStream_t st) {
 }
 
 void launch_color(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
-  SPHPC_LAUNCH_STAGED(k_color, P, V, a);
+  k_color<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
 }
 void launch_tension(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
-  SPHPC_LAUNCH_STAGED(k_tension, P, V, a);
+  k_tension<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
 }
 void launch_xsph(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
-  SPHPC_LAUNCH_STAGED(k_xsph, P, V, a);
+  k_xsph<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
 }
 void launch_vorticity(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
-  SPHPC_LAUNCH_STAGED(k_vorticity, P, V, a);
+  k_vorticity<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
 }
 void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a,
                         cudaStream_t st) {
-  SPHPC_LAUNCH_STAGED(k_confinement, P, V, a);
+  k_confinement<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
 }
 void launch_gravity(const DevParams& P, float4* vel, cudaStream_t st) {
   k_gravity<<<grid_for(P.n), kBlock, 0, st>>>(P, vel);

@@ -221,7 +221,6 @@ class DeviceSim {
 
   NbrView view() const {
     NbrView v;
-    v.cellp = cellp;
     v.nbr = nbr;
     v.ncount = ncount;
     v.cstart = cstart;

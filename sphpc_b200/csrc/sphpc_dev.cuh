@@ -101,7 +101,6 @@ struct DevParams {
 
 // View of the per-step neighbour structure.
 struct NbrView {
-  const uint32_t* __restrict__ cellp;   // [n] packed cell of each slot
   const uint32_t* __restrict__ nbr;     // [kMaxNeighbors][n]
   const uint8_t* __restrict__ ncount;   // [n]
   const uint32_t* __restrict__ cstart;  // [C+1]
