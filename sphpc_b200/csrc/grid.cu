@@ -216,13 +216,8 @@ struct BuildCtx {
 // double positions.  The FP32 absolute positions decide every pair whose r^2
 // lies outside a band of +-2^-10 h^2 (FP32 rounding of coordinates up to
 // 2^15 h moves r^2 by far less); the FP64 test decides the rest.
-__device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const PD* __restrict__ pd,
-                                            const float4* __restrict__ xsa, int j) {
-  const float4 q = __ldg(xsa + j);
-  const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
-  const float r2f = fx * fx + fy * fy + fz * fz;
-  if (r2f < c.h2lo) return true;
-  if (r2f > c.h2hi) return false;
+__device__ __noinline__ bool exact_neighbor(const BuildCtx& c, const PD* __restrict__ pd,
+                                            int j) {
   float4 xq, dq;
   ld_pd(pd, j, xq, dq);
   const double ddx = __dsub_rn(c.xs, xstar_d(xq.x, dq.x));
@@ -233,79 +228,98 @@ __device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const PD* __restr
   return r2 < c.h2d;
 }
 
+__device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const PD* __restrict__ pd,
+                                            const float4* __restrict__ xsa, int j) {
+  const float4 q = __ldg(xsa + j);
+  const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
+  const float r2f = fx * fx + fy * fy + fz * fz;
+  if (r2f < c.h2lo) return true;
+  if (r2f > c.h2hi) return false;
+  return exact_neighbor(c, pd, j);
+}
+
 constexpr int kBuildBlock = 128;
 
-// FillNeighbors, neighbors.c:217-298: one thread per particle; the bucket is
-// staged in shared memory and written out as columns nbr[j][*] so that each
-// store instruction of a warp fills one contiguous line.
-__global__ void __launch_bounds__(kBuildBlock)
+// FillNeighbors, neighbors.c:217-298: one thread per particle, bucket entries
+// written as they are found into column nbr[count][p] (L2 merges the partial
+// lines of a warp's columns).
+__global__ void __launch_bounds__(kBuildBlock, 10)
     k_build_neighbors(const DevParams P, const NbrView V, const PD* __restrict__ pd,
-                      const float4* __restrict__ xsa,
-                      const uint32_t* __restrict__ cellp, uint32_t* __restrict__ nbr,
-                      uint8_t* __restrict__ ncount) {
-  __shared__ uint32_t s_list[kMaxNeighbors][kBuildBlock];
-  const int t = threadIdx.x;
-  const int p = blockIdx.x * kBuildBlock + t;
+                      const float4* __restrict__ xsa, const uint32_t* __restrict__ cellp,
+                      uint32_t* __restrict__ nbr, uint8_t* __restrict__ ncount) {
+  const int p = blockIdx.x * kBuildBlock + threadIdx.x;
+  if (p >= P.n) return;
+  BuildCtx c;
+  ld_pd(pd, p, c.xp, c.dp);
+  c.xf = __ldg(xsa + p);
+  c.xs = xstar_d(c.xp.x, c.dp.x);
+  c.ys = xstar_d(c.xp.y, c.dp.y);
+  c.zs = xstar_d(c.xp.z, c.dp.z);
+  c.h2lo = P.h2 * (1.0f - 1.0f / 1024.0f);
+  c.h2hi = P.h2 * (1.0f + 1.0f / 1024.0f);
+  c.h2d = P.h2d;
+  int cx, cy, cz;
+  unpack_cell(V, __ldg(cellp + p), cx, cy, cz);
+  const bool regular = axis_regular(c.xs, P.hd, cx, P.nx) &&
+                       axis_regular(c.ys, P.hd, cy, P.ny) &&
+                       axis_regular(c.zs, P.hd, cz, P.nz);
+  uint32_t* out = nbr + p;
+  const size_t stride = (size_t)P.n;
   int count = 0;
-  if (p < P.n) {
-    BuildCtx c;
-    ld_pd(pd, p, c.xp, c.dp);
-    c.xf = __ldg(xsa + p);
-    c.xs = xstar_d(c.xp.x, c.dp.x);
-    c.ys = xstar_d(c.xp.y, c.dp.y);
-    c.zs = xstar_d(c.xp.z, c.dp.z);
-    c.h2lo = P.h2 * (1.0f - 1.0f / 1024.0f);
-    c.h2hi = P.h2 * (1.0f + 1.0f / 1024.0f);
-    c.h2d = P.h2d;
-    int cx, cy, cz;
-    unpack_cell(V, __ldg(cellp + p), cx, cy, cz);
-    const bool regular = axis_regular(c.xs, P.hd, cx, P.nx) &&
-                         axis_regular(c.ys, P.hd, cy, P.ny) &&
-                         axis_regular(c.zs, P.hd, cz, P.nz);
-    if (regular) {
-      // rows (dz, dy) of cells cx-1..cx+1 are contiguous slot ranges
-      const int xlo = cx - (cx > 0);
-      const int xhi = cx + (cx < P.nx - 1);
-      for (int dz = -1; dz <= 1 && count < kMaxNeighbors; ++dz) {
-        const int z = cz + dz;
-        if ((unsigned)z >= (unsigned)P.nz) continue;
-        for (int dy = -1; dy <= 1 && count < kMaxNeighbors; ++dy) {
-          const int y = cy + dy;
-          if ((unsigned)y >= (unsigned)P.ny) continue;
-          const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
-          const int b = (int)__ldg(V.cstart + rk + xlo);
-          const int e = (int)__ldg(V.cstart + rk + xhi + 1);
-          for (int j = b; j < e; ++j) {
-            if (j != p && is_neighbor(c, pd, xsa, j)) {
-              s_list[count][t] = (uint32_t)j;
-              if (++count == kMaxNeighbors) break;
-            }
+  if (regular) {
+    // rows (dz, dy) of cells cx-1..cx+1 are contiguous slot ranges
+    const int xlo = cx - (cx > 0);
+    const int xhi = cx + (cx < P.nx - 1);
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int z = cz + dz;
+      if ((unsigned)z >= (unsigned)P.nz) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = cy + dy;
+        if ((unsigned)y >= (unsigned)P.ny) continue;
+        const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
+        const int b = (int)__ldg(V.cstart + rk + xlo);
+        const int e = (int)__ldg(V.cstart + rk + xhi + 1);
+        for (int j = b; j < e; j += 4) {
+          float r2f[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float4 q = j + u < e ? __ldg(xsa + j + u) : make_float4(3e30f, 0.f, 0.f, 0.f);
+            const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
+            r2f[u] = fx * fx + fy * fy + fz * fz;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int jj = j + u;
+            if (jj >= e || jj == p || r2f[u] > c.h2hi) continue;
+            if (r2f[u] >= c.h2lo && !exact_neighbor(c, pd, jj)) continue;
+            out[(size_t)count * stride] = (uint32_t)jj;
+            if (++count == kMaxNeighbors) goto done;
           }
         }
       }
-    } else {
-      // neighbour cells are not cx-1..cx+1 (FP64 rounding at a cell face):
-      // the reference's 27-cell walk, verbatim
-      for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-          for (int dx = -1; dx <= 1; ++dx) {
-            int gx, gy, gz;
-            if (!shifted_coord(__dadd_rn(c.xs, (double)dx * P.hd), P.hd, P.nx, gx)) continue;
-            if (!shifted_coord(__dadd_rn(c.ys, (double)dy * P.hd), P.hd, P.ny, gy)) continue;
-            if (!shifted_coord(__dadd_rn(c.zs, (double)dz * P.hd), P.hd, P.nz, gz)) continue;
-            const uint32_t key = (uint32_t)P.nx * (uint32_t)P.ny * (uint32_t)gz +
-                                 ((uint32_t)gy * (uint32_t)P.nx + (uint32_t)gx);
-            if (key >= P.ncells) continue;
-            const int b = (int)__ldg(V.cstart + key);
-            const int e = (int)__ldg(V.cstart + key + 1);
-            for (int j = b; j < e && count < kMaxNeighbors; ++j) {
-              if (j != p && is_neighbor(c, pd, xsa, j)) s_list[count++][t] = (uint32_t)j;
-            }
-          }
     }
-    ncount[p] = (uint8_t)count;
-    for (int j = 0; j < count; ++j) nbr[(size_t)j * P.n + p] = s_list[j][t];
+  } else {
+    // neighbour cells are not cx-1..cx+1 (FP64 rounding at a cell face):
+    // the reference's 27-cell walk, verbatim
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          int gx, gy, gz;
+          if (!shifted_coord(__dadd_rn(c.xs, (double)dx * P.hd), P.hd, P.nx, gx)) continue;
+          if (!shifted_coord(__dadd_rn(c.ys, (double)dy * P.hd), P.hd, P.ny, gy)) continue;
+          if (!shifted_coord(__dadd_rn(c.zs, (double)dz * P.hd), P.hd, P.nz, gz)) continue;
+          const uint32_t key = (uint32_t)P.nx * (uint32_t)P.ny * (uint32_t)gz +
+                               ((uint32_t)gy * (uint32_t)P.nx + (uint32_t)gx);
+          if (key >= P.ncells) continue;
+          const int b = (int)__ldg(V.cstart + key);
+          const int e = (int)__ldg(V.cstart + key + 1);
+          for (int j = b; j < e && count < kMaxNeighbors; ++j) {
+            if (j != p && is_neighbor(c, pd, xsa, j)) out[(size_t)(count++) * stride] = (uint32_t)j;
+          }
+        }
   }
+done:
+  ncount[p] = (uint8_t)count;
 }
 
 __global__ void __launch_bounds__(kBlock)
