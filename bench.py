@@ -29,22 +29,23 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/sec at max density err <=1%: MLP warm-start vs plain, 1 B200"
 UNIT = "particle-steps/s"
 
-# Algorithmic (compulsory) HBM bytes per particle of each stage for this
-# layout: each particle's own records read/written once, neighbour data
-# assumed cache-resident.  mask = ~7 words of candidate bitmask.
-MASK_B = 28
+# Algorithmic (compulsory) HBM bytes per particle of each stage: every
+# particle's own state read and written once in FP32 float4 SoA, neighbour data
+# counted once (ideal cache reuse).  The neighbour-list build is not a
+# reference-layout stage: x* and cell in, one count byte and ~30 four-byte
+# list entries out.
 STAGE_BYTES = {
-    "hash": 32 + 8,                         # x, v in; key, slot scattered out
-    "radix_sort": None,                     # 16 B per digit pass (+4 hist), set below
-    "cell_starts": 4,                       # + 4 per cell, added below
-    "reorder": 4 + 4 + 32 + 32 + 4,         # ids, loc, x+v in, x+d out, cell
-    "build_neighbors": 32 + 4 + MASK_B + 1,
-    "density_lambda": 32 + 4 + MASK_B + 16 + 4,
-    "position": 32 + 4 + MASK_B + 4 + 16,
-    "surface_tension": 2 * (32 + 4 + MASK_B) + 16 + 16 + 16,
-    "xsph": 32 + 16 + 4 + MASK_B + 16,
-    "vorticity": 2 * (32 + 4 + MASK_B) + 16 + 16 + 16 + 16,
-    "velocity": 16 + 16,
+    "hash": 24,                             # r x*; w key, index
+    "radix_sort": None,                     # 16 B per digit pass + 4, set below
+    "cell_starts": 4,                       # + 8 per cell, added below
+    "reorder": 104,                         # gather x, x*, v, id: read and write
+    "build_neighbors": 16 + 4 + 1 + 4 * 30,
+    "density_lambda": 24,
+    "position": 36,
+    "surface_tension": 36 + 68,             # colour + tension
+    "xsph": 52,
+    "vorticity": 48 + 64,                   # vorticity + confinement
+    "velocity": 48,
 }
 
 
@@ -261,9 +262,9 @@ def run_ours(args, world, rank, local, dist):
         name, (cnt, tot) = max(prof.items(), key=lambda kv: kv[1][1])
         per = STAGE_BYTES.get(name)
         if name == "radix_sort":
-            per = 16 * sim_passes(sim)
+            per = 16 * sim_passes(sim) + 4
         if name == "cell_starts":
-            per = 4
+            per = 4 + 8 * sim_cells(sim) / n
         if per is not None and cnt:
             avg_s = tot / cnt / 1e3
             bytes_launch = per * n
@@ -316,8 +317,12 @@ def run_ours(args, world, rank, local, dist):
     print(json.dumps(line), flush=True)
 
 
+def sim_cells(sim):
+    return sim.neighbors.hash_size_x * sim.neighbors.hash_size_y * sim.neighbors.hash_size_z
+
+
 def sim_passes(sim):
-    C_ = sim.neighbors.hash_size_x * sim.neighbors.hash_size_y * sim.neighbors.hash_size_z
+    C_ = sim_cells(sim)
     bits = max(1, int(C_ - 1).bit_length())
     return (bits + 7) // 8
 

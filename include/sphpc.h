@@ -170,6 +170,16 @@ int sphpc_step_info(const struct Particles *particles, struct SphpcStepInfo *inf
 /* Kernel-reported error bits since the last call (0 = none); clears them. */
 int sphpc_device_errors(const struct Particles *particles, unsigned int *bits);
 
+/* ---------------- learned warm start ---------------- */
+
+/* Forward pass of the warm-start network on n feature rows d_feat[n][16]
+ * (device memory) into d_out[n] (device), with the FP32 parameter vector
+ * params[9473] (W1[64][16] b1 W2[64][64] b2 W3[64][64] b3 w4[64] b4) and
+ * normalisation norm[33] (mean[16] inv_std[16] out_scale) on the host.
+ * No counterpart in the reference. */
+int sphpc_mlp_forward(const float *d_feat, int n, const float *params, const float *norm,
+                      float *d_out, void *cuda_stream);
+
 /* Per-stage CUDA-event timing of the particle set's launches.  The last
  * entry sphpc_profile_read returns is "kernel_launches": the number of
  * kernels the particle set has launched in total (its launches field). */

@@ -161,6 +161,8 @@ SIGNATURES = {
     "sphpc_step_info": ([PP, C.POINTER(StepInfo)], C.c_int),
     "sphpc_profile": ([PP, C.c_int], C.c_int),
     "sphpc_profile_read": ([PP, C.POINTER(KernelTime), C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "sphpc_mlp_forward": ([C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                           C.c_void_p, C.c_void_p], C.c_int),
     "SortByKey": ([U, U, C.c_int, C.c_void_p], C.c_int),
     "SortByKeyNoAlloc": ([U, U, C.c_int, C.c_void_p], C.c_int),
     "FindLowerBounds": ([U, C.c_int, C.c_int, U, C.c_void_p], C.c_int),
