@@ -200,29 +200,16 @@ def run_reference(args, world, rank):
 # Our arm
 # --------------------------------------------------------------------------
 
-def run_ours(args, world, rank, local, dist):
+def timed_arm(sim, args, stream, dist, local, dev):
+    """W untimed steps, then K steps timed with CUDA events on the launching
+    stream between barriers (max over ranks), with the clocks sampled."""
     import torch
-    from sphpc_b200 import Simulation
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    overrides = {"adaptive": 1, "density_tolerance": args.tol,
-                 "max_iterations": args.max_iters}
-    if args.fixed:
-        overrides = {"adaptive": 0}
-    t_init = time.perf_counter()
-    sim = Simulation(args.config, solver_overrides=overrides)
-    stream = torch.cuda.current_stream(dev)
-    sim.set_stream(stream.cuda_stream)
-    n = sim.n
-    log(f"[rank {rank}] {args.config}: {n} particles, init {time.perf_counter()-t_init:.1f}s")
     for _ in range(args.warmup):
         sim.step(1)
     torch.cuda.synchronize()
-    it_before = sim.diagnostics()
     launches0 = sim.launches()
-    iters = []
+    iters, conv, rejected, used = [], 0, 0, 0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    conv = 0
     with ClockSampler(local) as clk:
         if dist:
             dist.barrier()
@@ -234,21 +221,66 @@ def run_ours(args, world, rank, local, dist):
                 d = sim.last_step_info()
                 iters.append(d["iterations"])
                 conv += d["converged"]
+                used += d["warm_start_used"]
+                rejected += d["warm_start_rejected"]
         ev1.record(stream)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
     ms = ev0.elapsed_time(ev1)
-    launches = sim.launches() - launches0
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * n * args.steps / (ms_max / 1e3)
     errs = sim.device_errors()
     if errs:
         raise RuntimeError(f"device error bits 0x{errs:x} during the timed region")
-    diag = sim.diagnostics()
+    return {"ms": float(t.item()), "iters": iters, "converged": conv, "rejected": rejected,
+            "warm_used": used, "launches": sim.launches() - launches0,
+            "clocks": clk.summary(), "diag": sim.diagnostics()}
+
+
+def run_ours(args, world, rank, local, dist):
+    import torch
+    from sphpc_b200 import Simulation
+    from sphpc_b200 import warm_start as ws
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    overrides = {"adaptive": 1, "density_tolerance": args.tol,
+                 "max_iterations": args.max_iters}
+    if args.fixed:
+        overrides = {"adaptive": 0}
+    net = None
+    if not args.no_warm and os.path.exists(args.weights):
+        net = ws.load_network(args.weights)
+    stream = torch.cuda.current_stream(dev)
+
+    def make_sim(warm):
+        t_init = time.perf_counter()
+        sim = Simulation(args.config, solver_overrides=overrides)
+        sim.set_stream(stream.cuda_stream)
+        if warm:
+            sim.mlp_load(net[0], net[1])
+            sim.set_solver(warm_start=1)
+        log(f"[rank {rank}] {args.config}: {sim.n} particles, warm start {warm}, "
+            f"init {time.perf_counter()-t_init:.1f}s")
+        return sim
+
+    # plain solver first, then (with a trained network) the warm-started one
+    sim = make_sim(False)
+    n = sim.n
+    plain = timed_arm(sim, args, stream, dist, local, dev)
+    warm = None
+    if net is not None:
+        sim.close()
+        sim = make_sim(True)
+        warm = timed_arm(sim, args, stream, dist, local, dev)
+    head = warm if warm is not None else plain
+    ms_max = head["ms"]
+    value = world * n * args.steps / (ms_max / 1e3)
+    iters = head["iters"]
+    conv = head["converged"]
+    launches = head["launches"]
+    diag = head["diag"]
 
     # per-stage CUDA-event profile of two more steps (not part of the timed value)
     sim.profile(True)
@@ -293,15 +325,32 @@ def run_ours(args, world, rank, local, dist):
     sim.close()
     if rank != 0:
         return
-    clocks = clk.summary()
+    clocks = head["clocks"]
+
+    def arm_summary(a):
+        if a is None:
+            return None
+        return {"value": world * n * args.steps / (a["ms"] / 1e3),
+                "ms_per_step": a["ms"] / args.steps,
+                "mean_iterations": float(np.mean(a["iters"])) if a["iters"] else None,
+                "steps_converged": a["converged"] if a["iters"] else None,
+                "warm_start_steps": a["warm_used"], "gate_rejections": a["rejected"],
+                "final_max_density_error": a["diag"]["max_density_error"],
+                "gpu_launches": a["launches"]}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
         "data": "synthetic",
         "config": {"workload": args.config, "particles_per_gpu": n,
-                   "solver": "fixed iterations" if args.fixed else
-                   f"plain, iterate to max density err <= {args.tol} (cap {args.max_iters})",
+                   "solver": ("fixed iterations" if args.fixed else
+                              f"iterate to max density err <= {args.tol} (cap {args.max_iters})")
+                   + (", MLP warm start" if warm is not None else ", plain (no network file)"),
+                   "plain": arm_summary(plain),
+                   "warm_start": arm_summary(warm),
+                   "warm_start_weights": (os.path.relpath(args.weights, ROOT)
+                                          if warm is not None else None),
+                   "speedup_vs_plain": (plain["ms"] / warm["ms"]) if warm is not None else None,
                    "mean_iterations": float(np.mean(iters)) if iters else None,
                    "steps_converged": conv if iters else None,
                    "l2": "state larger than L2 (no flush)",
@@ -389,6 +438,9 @@ def main():
     ap.add_argument("--fixed", action="store_true", help="configured iteration count")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-warm", action="store_true", help="plain solver only")
+    ap.add_argument("--weights", default=os.path.join(ROOT, "sphpc_b200", "weights",
+                                                      "warm_start.npz"))
     ap.add_argument("--ref-iterations", type=int, default=6)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     args = ap.parse_args()

@@ -180,6 +180,56 @@ int sphpc_device_errors(const struct Particles *particles, unsigned int *bits);
 int sphpc_mlp_forward(const float *d_feat, int n, const float *params, const float *norm,
                       float *d_out, void *cuda_stream);
 
+/* Gradient of the batch loss L = 1/(2n) sum_p (u_p - t_p / out_scale)^2 (u the
+ * network output before out_scale) over n rows d_feat[n][16], d_target[n]
+ * (device memory), through the tensor-core training kernels: grad_out[9473]
+ * and *loss_out on the host.  No counterpart in the reference. */
+int sphpc_mlp_grad(const float *d_feat, const float *d_target, int n, const float *params,
+                   const float *norm, float *grad_out, float *loss_out, void *cuda_stream);
+
+/* The process's training set of (features, target) rows, resident on the
+ * device that reserved it.  reserve grows it (keeping the rows), clear empties
+ * it, free releases it; append copies rows from the host; read copies rows
+ * [offset, offset + count) to the host; stats writes the normalisation
+ * norm[33] (feature means, 1/standard deviations, target standard deviation).
+ * No counterpart in the reference. */
+int sphpc_mlp_dataset_reserve(long long capacity);
+int sphpc_mlp_dataset_size(long long *n);
+int sphpc_mlp_dataset_clear(void);
+int sphpc_mlp_dataset_free(void);
+int sphpc_mlp_dataset_append(const float *feat, const float *target, long long count);
+int sphpc_mlp_dataset_read(long long offset, long long count, float *feat, float *target);
+int sphpc_mlp_dataset_stats(float *norm);
+
+/* AdamW (beta 0.9/0.999, eps 1e-8, decoupled weight decay on weights only)
+ * on the training set: `steps` steps of `batch` rows, each pass over the set
+ * in a fresh seeded permutation; params_out[9473] and loss_out[steps] (batch
+ * loss before each update, may be NULL) on the host.  No counterpart in the
+ * reference. */
+int sphpc_mlp_train(const float *params_in, const float *norm, int steps, int batch, float lr,
+                    float weight_decay, unsigned long long seed, float *params_out,
+                    float *loss_out);
+
+/* One time step like sphpc_step with the plain solver at a fixed
+ * `iterations`, appending one training row per particle (as many as fit):
+ * the 16 features of the predicted state and target sum_k s_k lambda_k, the
+ * stiffness-weighted multiplier sum of the solve.  Returns the rows appended
+ * (>= 0) or an error code.  No counterpart in the reference. */
+int sphpc_mlp_collect(struct Particles *particles, const struct Params *params,
+                      struct Neighbors *neighbors, const struct AABB *boundary_global,
+                      const struct Obstacle *obstacle, int iterations);
+
+/* Installs (or removes) the network the warm start of sphpc_step uses when
+ * the solver's warm_start is set: params[9473], norm[33] as above. */
+int sphpc_mlp_load(struct Particles *particles, const float *params, const float *norm);
+int sphpc_mlp_unload(struct Particles *particles);
+
+/* Features [N][16] (by particle id, host memory) of the current device state;
+ * call after FindAllNeighbors.  Overwrites no particle state. */
+int sphpc_mlp_features(struct Particles *particles, const struct Params *params,
+                       const struct AABB *boundary_global, const struct Obstacle *obstacle,
+                       float *features);
+
 /* Per-stage CUDA-event timing of the particle set's launches.  The last
  * entry sphpc_profile_read returns is "kernel_launches": the number of
  * kernels the particle set has launched in total (its launches field). */

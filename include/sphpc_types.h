@@ -171,7 +171,7 @@ struct SphpcStepInfo {
   int iterations;             /* constraint iterations run (warm start counts 1) */
   int converged;              /* adaptive: max density error reached tolerance */
   int warm_start_used;
-  int pad;
+  int warm_start_rejected;    /* the residual gate discarded the warm pass */
   double max_density_error;   /* FP64, at the last density evaluation */
   double mean_density_error;
 };

@@ -774,6 +774,103 @@ void oracle_step(const OracleParams *p, OracleState *s, OracleNeighbors *nb) {
   oracle_update_positions(s);
 }
 
+/* Warm-start features of every particle (no reference counterpart: they
+ * are the inputs of the learned warm start of the constraint solve whose
+ * plain iteration is particles.c:588-746).  Computed from the predicted
+ * state (x*, v) and the neighbour buckets, in double:
+ *   0 rho/rho0 - 1, 1 C = max(rho/rho0 - 1, 0), 2 lambda (particles.c:616-663),
+ *   3 sum_q |grad_q C|^2 / rho0^2, 4 |sum_q grad_q C|^2 / rho0^2,
+ *   5 neighbour count, 6-8 mean (x*_q - x*_p) / h,
+ *   9-11 mean (v_q - v_p) dt / h, 12 SDF distance at x* / h clamped to
+ *   [-4, 4] (4 without an obstacle or outside its box), 13 nearest-neighbour
+ *   distance / h (1 without neighbours), 14 distance to the nearest box wall
+ *   / h clamped to [0, 4], 15 v along the gravity axis * dt / h. */
+void oracle_features(const OracleParams *p, const OracleState *s,
+                     const OracleNeighbors *nb, double *feat) {
+  const double h = p->h, m = p->rest_mass, rho0 = p->rest_density;
+  const double W0 = m * p->W_norm * h * h * h * h * h * h;
+  for (int i = 0; i < s->n; ++i) {
+    const uint32_t *nbr = nb->nbr + (size_t)i * ORACLE_MAX_NEIGHBORS;
+    const double xp = s->xs[i], yp = s->ys[i], zp = s->zs[i];
+    double rho = W0, sgx = 0, sgy = 0, sgz = 0, sC = 0;
+    double o[3] = {0, 0, 0}, u[3] = {0, 0, 0}, rmin2 = h * h;
+    const int cnt = nb->count[i];
+    for (int j = 0; j < cnt; ++j) {
+      const int q = (int)nbr[j];
+      const double dx = xp - s->xs[q], dy = yp - s->ys[q], dz = zp - s->zs[q];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      double r = sqrt(r2);
+      rho += m * W(r, h, p->W_norm);
+      if (r < h * 0.0001) r = h * 0.0001;
+      const double g = m * DelW(r, h, p->DelW_norm);
+      const double gx = g * dx / r, gy = g * dy / r, gz = g * dz / r;
+      sgx += gx; sgy += gy; sgz += gz;
+      sC += gx * gx + gy * gy + gz * gz;
+      o[0] -= dx; o[1] -= dy; o[2] -= dz;
+      u[0] += s->vx[q] - s->vx[i];
+      u[1] += s->vy[q] - s->vy[i];
+      u[2] += s->vz[q] - s->vz[i];
+      if (r2 < rmin2) rmin2 = r2;
+    }
+    const double C0 = rho / rho0 - 1.0;
+    const double C = C0 < 0.0 ? 0.0 : C0;
+    const double s_pairs = sC / (rho0 * rho0);
+    const double s_self = (sgx * sgx + sgy * sgy + sgz * sgz) / (rho0 * rho0);
+    const double lam = -C / (s_pairs + s_self + p->lambda_epsilon);
+    const double ic = cnt > 0 ? 1.0 / cnt : 0.0;
+    double sdf = 4.0;
+    if (p->sdf && xp > p->ob_min[0] && xp < p->ob_max[0] && yp > p->ob_min[1] &&
+        yp < p->ob_max[1] && zp > p->ob_min[2] && zp < p->ob_max[2]) {
+      const float L = (float)(p->ob_max[0] - p->ob_min[0]);
+      const float H = (float)(p->ob_max[1] - p->ob_min[1]);
+      const float D = (float)(p->ob_max[2] - p->ob_min[2]);
+      const float d = oracle_sdf_sample(p, (float)((xp - p->ob_min[0]) / L),
+                                        (float)((yp - p->ob_min[1]) / H),
+                                        (float)((zp - p->ob_min[2]) / D));
+      const double m2w = (double)(L / (float)(p->sdim[0] * p->sdf_spacing));
+      sdf = d * m2w / h;
+      if (sdf < -4.0) sdf = -4.0;
+      if (sdf > 4.0) sdf = 4.0;
+    }
+    double wall = xp - p->bmin[0];
+    const double wl[5] = {p->bmax[0] - xp, yp - p->bmin[1], p->bmax[1] - yp,
+                          zp - p->bmin[2], p->bmax[2] - zp};
+    for (int k = 0; k < 5; ++k) if (wl[k] < wall) wall = wl[k];
+    wall /= h;
+    if (wall < 0.0) wall = 0.0;
+    if (wall > 4.0) wall = 4.0;
+    const double *vg = p->gravity_axis == 0 ? s->vx : (p->gravity_axis == 1 ? s->vy : s->vz);
+    double *f = feat + (size_t)i * 16;
+    f[0] = C0; f[1] = C; f[2] = lam; f[3] = s_pairs; f[4] = s_self; f[5] = cnt;
+    for (int k = 0; k < 3; ++k) {
+      f[6 + k] = o[k] * ic / h;
+      f[9 + k] = u[k] * ic * p->dt / h;
+    }
+    f[12] = sdf;
+    f[13] = sqrt(rmin2) / h;
+    f[14] = wall;
+    f[15] = vg[i] * p->dt / h;
+  }
+}
+
+/* Training target of the warm start: one plain solve of `iterations`
+ * substeps (ComputeDensities, ComputeLambda, UpdateDPs,
+ * UpdatePositionStars; simulation.c:72-82) from the predicted state, with
+ * target[i] = sum_k s_k lambda_k, s_k the stiffness of substep k
+ * (particles.c:693-694).  Leaves s advanced by the solve. */
+void oracle_lambda_target(const OracleParams *p, OracleState *s,
+                          const OracleNeighbors *nb, int iterations, double *target) {
+  for (int i = 0; i < s->n; ++i) target[i] = 0.0;
+  for (int k = 0; k < iterations; ++k) {
+    const double stiff = 1.0 - pow(1.0 - p->k_stiff, 1.0 / (double)k);
+    oracle_compute_densities(p, s, nb);
+    oracle_compute_lambda(p, s, nb);
+    for (int i = 0; i < s->n; ++i) target[i] += stiff * s->lam[i];
+    oracle_update_dps(p, s, nb, k);
+    oracle_update_position_stars(p, s);
+  }
+}
+
 void oracle_diagnostics(const OracleParams *p, const OracleState *s,
                         OracleDiag *d) {
   double mx = 0.0, sum = 0.0, ke = 0.0;

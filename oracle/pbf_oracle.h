@@ -176,6 +176,11 @@ void oracle_update_positions(OracleState *s);
 
 /* One full time step (simulation.c:56-116 loop body). */
 void oracle_step(const OracleParams *p, OracleState *s, OracleNeighbors *nb);
+/* warm-start features [n][16] and plain-solve multiplier-sum target */
+void oracle_features(const OracleParams *p, const OracleState *s,
+                     const OracleNeighbors *nb, double *feat);
+void oracle_lambda_target(const OracleParams *p, OracleState *s,
+                          const OracleNeighbors *nb, int iterations, double *target);
 void oracle_diagnostics(const OracleParams *p, const OracleState *s,
                         OracleDiag *d);
 

@@ -114,6 +114,8 @@ def oracle_lib(fp32: bool = False):
                    "oracle_fill_neighbors", "oracle_step"):
             getattr(lib, nm).argtypes = [P, S, N]
         lib.oracle_update_dps.argtypes = [P, S, N, C.c_int]
+        lib.oracle_features.argtypes = [P, S, N, _DP]
+        lib.oracle_lambda_target.argtypes = [P, S, N, C.c_int, _DP]
         lib.oracle_update_positions.argtypes = [S]
         lib.oracle_diagnostics.argtypes = [P, S, C.POINTER(OracleDiag)]
         lib.oracle_real_size.restype = C.c_int
@@ -330,6 +332,19 @@ class OracleSim:
         d = OracleDiag()
         self.lib.oracle_diagnostics(C.byref(self.p), C.byref(self.s), C.byref(d))
         return d.as_dict()
+
+    def features(self):
+        """Warm-start features [n][16] of the current (predicted) state."""
+        f = np.zeros((self.n, 16), np.float64)
+        self.lib.oracle_features(C.byref(self.p), C.byref(self.s), C.byref(self.nb), _ptr(f))
+        return f
+
+    def lambda_target(self, iterations):
+        """Plain solve of `iterations` substeps; returns sum_k s_k lambda_k."""
+        t = np.zeros(self.n, np.float64)
+        self.lib.oracle_lambda_target(C.byref(self.p), C.byref(self.s), C.byref(self.nb),
+                                      iterations, _ptr(t))
+        return t
 
     def neighbor_lists(self):
         cnt = self.nb_arrays["count"]

@@ -94,7 +94,7 @@ class Diag(C.Structure):
 
 class StepInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int),
-                ("warm_start_used", C.c_int), ("pad", C.c_int),
+                ("warm_start_used", C.c_int), ("warm_start_rejected", C.c_int),
                 ("max_density_error", C.c_double), ("mean_density_error", C.c_double)]
 
 
@@ -156,6 +156,10 @@ SIGNATURES = {
     "FinalizeObstacle": ([PO], C.c_int),
     "sphpc_read_sdf": ([PO], C.c_int),
     "sphpc_step": ([PP, P, PN, PA, PO, C.c_int], C.c_int),
+    "sphpc_mlp_collect": ([PP, P, PN, PA, PO, C.c_int], C.c_int),
+    "sphpc_mlp_load": ([PP, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+    "sphpc_mlp_unload": ([PP], C.c_int),
+    "sphpc_mlp_features": ([PP, P, PA, PO, C.POINTER(C.c_float)], C.c_int),
     "sphpc_diagnostics": ([PP, C.POINTER(Diag)], C.c_int),
     "sphpc_device_errors": ([PP, U], C.c_int),
     "sphpc_step_info": ([PP, C.POINTER(StepInfo)], C.c_int),
@@ -163,6 +167,17 @@ SIGNATURES = {
     "sphpc_profile_read": ([PP, C.POINTER(KernelTime), C.c_int, C.POINTER(C.c_int)], C.c_int),
     "sphpc_mlp_forward": ([C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
                            C.c_void_p, C.c_void_p], C.c_int),
+    "sphpc_mlp_grad": ([C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_void_p],
+                       C.c_int),
+    "sphpc_mlp_dataset_reserve": ([C.c_longlong], C.c_int),
+    "sphpc_mlp_dataset_size": ([C.POINTER(C.c_longlong)], C.c_int),
+    "sphpc_mlp_dataset_clear": ([], C.c_int),
+    "sphpc_mlp_dataset_free": ([], C.c_int),
+    "sphpc_mlp_dataset_append": ([C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_longlong], C.c_int),
+    "sphpc_mlp_dataset_read": ([C.c_longlong, C.c_longlong, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+    "sphpc_mlp_dataset_stats": ([C.POINTER(C.c_float)], C.c_int),
+    "sphpc_mlp_train": ([C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_float, C.c_float, C.c_ulonglong,
+                         C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
     "SortByKey": ([U, U, C.c_int, C.c_void_p], C.c_int),
     "SortByKeyNoAlloc": ([U, U, C.c_int, C.c_void_p], C.c_int),
     "FindLowerBounds": ([U, C.c_int, C.c_int, U, C.c_void_p], C.c_int),

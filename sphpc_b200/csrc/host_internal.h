@@ -5,6 +5,22 @@
 
 #include "../../include/sphpc.h"
 
+// Return the CUDA call's error as SPHPC_ECUDA with its text and location.
+#define SPHPC_CK(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return ::sphpc::set_error(SPHPC_ECUDA, "%s: %s (%s:%d)", #call,                  \
+                                cudaGetErrorString(e_), __FILE__, __LINE__);            \
+  } while (0)
+
+// Return a non-zero status code unchanged.
+#define SPHPC_RC(expr)      \
+  do {                      \
+    const int rc_ = (expr); \
+    if (rc_) return rc_;    \
+  } while (0)
+
 namespace sphpc {
 
 // Records a formatted error message for sphpc_last_error() and returns code.

@@ -80,6 +80,12 @@ struct PassArgs {
 // rho[]).
 void launch_density_lambda(const DevParams& P, const NbrView& V, const PassArgs& a, int mode,
                            bool residual, cudaStream_t st);
+// First density/lambda pass of a step (mode 0 with residual) that also writes
+// the warm-start network's 16 features of particles p < limit to feat[p][16].
+void launch_features(const DevParams& P, const NbrView& V, const PassArgs& a, float* feat,
+                     int limit, cudaStream_t st);
+// target[p] += s * lambda_p (lambda in rec[p].d.w), p < limit.
+void launch_accum_lambda(const PD* rec, float s, float* target, int limit, cudaStream_t st);
 // Position pass: UpdateDPs (:668-746) with lambda from d.w; mode 0 fuses
 // UpdatePositionStars (:529-564, clamp + SDF collision) and, if a.last,
 // UpdateVelocities (:787-838); mode 1 writes dp[] only.

@@ -8,7 +8,10 @@
 // and completed through tcgen05.commit on an mbarrier.  Thread t then owns
 // particle t of the tile: it reads row t of D (tcgen05.ld 32x32b), adds the
 // bias, applies GELU and writes row t of the next layer's A.
+#include <cmath>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "host_internal.h"
 #include "mlp.cuh"
@@ -32,10 +35,13 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major,
-// M = 128, N = 64.
-constexpr uint32_t kIdescM128N64 = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) |
-                                   ((128u >> 4) << 24);
+// Instruction descriptor of kind::f16 with A = B = BF16 and D = F32: M x N,
+// A and B each K-major (0) or MN-major (1).
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int a_mn, int b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+constexpr uint32_t kIdescM128N64 = idesc_bf16(128, 64, 0, 0);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -261,7 +267,7 @@ __global__ void __launch_bounds__(kMlpTile)
       if (pd_out) {
         float4 x, d;
         ld_pd(pd_in, p, x, d);
-        d.w = y;
+        d.w = fminf(y, 0.0f);
         st_pd(pd_out, p, x, d);
       }
     }
@@ -269,6 +275,425 @@ __global__ void __launch_bounds__(kMlpTile)
   tc::fence_before();
   __syncthreads();
   if (t < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(taddr));
+}
+
+// ---------------------------------------------------------------------------
+// Training: one batch of rows through forward, backward and the weight
+// gradients, all on the tensor cores.  Shared-memory operands (BF16, core
+// matrices of 8 rows x 16 bytes, K-adjacent core matrices 128 bytes apart):
+//   x0 [128 x 32]  normalised features, column 16 = 1 (bias), rest 0
+//   h1, h2, h3 [128 x 80]  activations, column 64 = 1, rest 0
+//   dz [128 x 128] the current layer's pre-activation gradient, columns
+//                  64..127 = 0
+// Forward   z_l  = h_{l-1} W_l^T            A, B K-major
+// Backward  dh_l = dz_l W_l                 A K-major, B = W_l read MN-major
+// Gradient  G_l += dz_l^T [h_{l-1} | 1]     A = dz read MN-major (M = 128 over
+//           output neurons, rows 64..127 unused), B = h read MN-major, K =
+//           the 128 rows of the tile; column 64 (16 for the input layer) of
+//           the result is the bias gradient.
+// The gradients accumulate in tensor memory over every tile the CTA takes;
+// each CTA writes its sums once, in parameter-vector order, to its slice of
+// `partial`; k_mlp_update reduces the slices and applies AdamW.
+// Tensor-memory columns (512 allocated, one CTA per SM):
+//   z1 0..63, z2 64..127, z3 128..191 (dh2 reuses z3, dh1 reuses z2),
+//   G4 192..271, G3 272..351, G2 352..431, G1 432..463.
+// ---------------------------------------------------------------------------
+constexpr int kKcX = 4, kKcH = 10, kKcD = 16;
+constexpr uint32_t kTZ1 = 0, kTZ2 = 64, kTZ3 = 128, kTG4 = 192, kTG3 = 272, kTG2 = 352,
+                   kTG1 = 432;
+constexpr uint32_t kTrainCols = 512;
+
+struct TrainSmem {
+  alignas(1024) uint8_t w1[kMlpHidden * kMlpIn * 2];
+  alignas(128) uint8_t w2[kMlpHidden * kMlpHidden * 2];
+  alignas(128) uint8_t w3[kMlpHidden * kMlpHidden * 2];
+  alignas(128) uint8_t x0[kMlpTile * kKcX * 16];
+  alignas(128) uint8_t h1[kMlpTile * kKcH * 16];
+  alignas(128) uint8_t h2[kMlpTile * kKcH * 16];
+  alignas(128) uint8_t h3[kMlpTile * kKcH * 16];
+  alignas(128) uint8_t dz[kMlpTile * kKcD * 16];
+  float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpHidden], w4[kMlpHidden];
+  float mean[kMlpIn], istd[kMlpIn];
+  float red[kMlpTile / 32];
+  // keeps every operand read of the descriptors above inside the CTA's shared
+  // memory even if the strides were read with the other core-matrix order
+  uint8_t guard[28 * 1024];
+  alignas(8) uint64_t mbar;
+  uint32_t taddr;
+};
+
+__device__ __forceinline__ float gelu_grad(float z) {
+  const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+  return 0.5f * (1.0f + t) +
+         0.5f * z * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 3.0f * 0.044715f * z * z);
+}
+
+// 8 consecutive values of row r starting at column k0 (multiple of 8).
+__device__ __forceinline__ void put8(uint8_t* buf, int kc, int r, int k0, const float* v) {
+  __align__(16) __nv_bfloat16 pk[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) pk[i] = __float2bfloat16_rn(v[i]);
+  *reinterpret_cast<uint4*>(buf + tc::core_off(r, k0, kc)) = *reinterpret_cast<const uint4*>(pk);
+}
+
+__device__ __forceinline__ void put8_const(uint8_t* buf, int kc, int r, int k0, float first) {
+  float v[8] = {first, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  put8(buf, kc, r, k0, v);
+}
+
+// 64 FP32 columns starting at TMEM column `col` of this thread's lane.
+__device__ __forceinline__ void tmem_row64(uint32_t lane_base, uint32_t col, float* v) {
+#pragma unroll
+  for (int c = 0; c < 64; c += 16) tc::tmem_ld16(lane_base + col + c, v + c);
+  tc::tmem_wait_ld();
+}
+
+// K-major A [128 x K] x K-major B [N x K]^T, K in steps of 16.
+__device__ __forceinline__ void mma_kk(uint32_t d, uint32_t a, int kca, uint32_t b, int kcb, int K,
+                                       uint32_t idesc) {
+  for (int st = 0; st < K / 16; ++st)
+    tc::mma_bf16(d, tc::smem_desc(a + st * 256, 128, kca * 128),
+                 tc::smem_desc(b + st * 256, 128, kcb * 128), idesc, st > 0);
+}
+
+// Weight gradient over the 128 rows of a tile: D[M=128][N] (+)= A^T B with A
+// = dz [rows x 128] and B = activations [rows x N], both read MN-major.
+__device__ __forceinline__ void mma_grad(uint32_t d, uint32_t a, uint32_t b, int kcb, int N,
+                                         bool acc) {
+  const uint32_t idesc = tc::idesc_bf16(128, N, 1, 1);
+  for (int st = 0; st < kMlpTile / 16; ++st)
+    tc::mma_bf16(d, tc::smem_desc(a + st * 2 * kKcD * 128, kKcD * 128, 128),
+                 tc::smem_desc(b + st * 2 * kcb * 128, kcb * 128, 128), idesc, acc || st > 0);
+}
+
+// dh [128 x 64] = dz [128 x 64] . W [64 x 64] with W (row-major [out][in],
+// core layout K-major for the forward) read MN-major.
+__device__ __forceinline__ void mma_dh(uint32_t d, uint32_t a, uint32_t w) {
+  const uint32_t idesc = tc::idesc_bf16(128, 64, 0, 1);
+  for (int st = 0; st < kMlpHidden / 16; ++st)
+    tc::mma_bf16(d, tc::smem_desc(a + st * 256, 128, kKcD * 128),
+                 tc::smem_desc(w + st * 2 * 8 * 128, 8 * 128, 128), idesc, st > 0);
+}
+
+__global__ void __launch_bounds__(kMlpTile, 1)
+    k_mlp_grad(const float* __restrict__ params, const float* __restrict__ norm,
+               const __nv_bfloat16* __restrict__ wbf, const float* __restrict__ feat,
+               const float* __restrict__ target, long long n_data, long long base,
+               unsigned long long mul, unsigned long long add, int batch,
+               float* __restrict__ partial, uint32_t* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  const uint32_t mis = tc::smem_u32(smem_raw) & 1023u;
+  TrainSmem& s = *reinterpret_cast<TrainSmem*>(smem_raw + ((1024u - mis) & 1023u));
+  const int t = threadIdx.x, warp = t >> 5;
+  load_weights(wbf, kMlpIn, s.w1);
+  load_weights(wbf + kMlpHidden * kMlpIn, kMlpHidden, s.w2);
+  load_weights(wbf + kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden, kMlpHidden, s.w3);
+  for (int i = t; i < kMlpHidden; i += blockDim.x) {
+    s.b1[i] = params[kOffB1 + i];
+    s.b2[i] = params[kOffB2 + i];
+    s.b3[i] = params[kOffB3 + i];
+    s.w4[i] = params[kOffW4 + i];
+  }
+  if (t < kMlpIn) {
+    s.mean[t] = norm[t];
+    s.istd[t] = norm[kMlpIn + t];
+  }
+  const float b4 = params[kOffB4];
+  const float inv_scale = 1.0f / norm[2 * kMlpIn];
+  const float inv_batch = 1.0f / (float)batch;
+  // constant columns of this thread's rows: bias ones and zero padding
+  put8_const(s.x0, kKcX, t, 16, 1.0f);
+  put8_const(s.x0, kKcX, t, 24, 0.0f);
+  put8_const(s.h1, kKcH, t, 64, 1.0f);
+  put8_const(s.h1, kKcH, t, 72, 0.0f);
+  put8_const(s.h2, kKcH, t, 64, 1.0f);
+  put8_const(s.h2, kKcH, t, 72, 0.0f);
+  put8_const(s.h3, kKcH, t, 64, 1.0f);
+  put8_const(s.h3, kKcH, t, 72, 0.0f);
+  for (int k0 = 64; k0 < 128; k0 += 8) put8_const(s.dz, kKcD, t, k0, 0.0f);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32(&s.taddr)),
+                 "r"(kTrainCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_u32(&s.mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t taddr = s.taddr;
+  const uint32_t lane_base = taddr + ((uint32_t)(warp * 32) << 16);
+  const uint32_t sx0 = tc::smem_u32(s.x0), sh1 = tc::smem_u32(s.h1), sh2 = tc::smem_u32(s.h2),
+                 sh3 = tc::smem_u32(s.h3), sdz = tc::smem_u32(s.dz), sw1 = tc::smem_u32(s.w1),
+                 sw2 = tc::smem_u32(s.w2), sw3 = tc::smem_u32(s.w3);
+  uint32_t phase = 0;
+  bool ok = true, acc = false;
+  float loss = 0.0f;
+  float v[kMlpHidden];
+  // Makes this thread's shared-memory writes visible to the tensor cores,
+  // lets thread 0 issue `body` and commit, and waits (bounded) for it; the
+  // whole CTA sees the same outcome.
+  auto run = [&](auto body) -> bool {
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+      body();
+      tc::commit(&s.mbar);
+    }
+    const bool done = __syncthreads_and(tc::mbar_wait(&s.mbar, phase) ? 1 : 0) != 0;
+    phase ^= 1u;
+    tc::fence_after();
+    return done;
+  };
+  const int ntiles = (batch + kMlpTile - 1) / kMlpTile;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r = tile * kMlpTile + t;
+    const bool valid = r < batch;
+    float tgt = 0.0f;
+    {
+      float f[kMlpIn];
+      if (valid) {
+        const unsigned long long row = (unsigned long long)((base + r) % n_data);
+        const unsigned long long idx = (row * mul + add) % (unsigned long long)n_data;
+        const float4* fp = reinterpret_cast<const float4*>(feat + idx * kMlpIn);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 a4 = __ldg(fp + q);
+          f[4 * q] = a4.x; f[4 * q + 1] = a4.y; f[4 * q + 2] = a4.z; f[4 * q + 3] = a4.w;
+        }
+        tgt = __ldg(target + idx) * inv_scale;
+      } else {
+#pragma unroll
+        for (int k = 0; k < kMlpIn; ++k) f[k] = s.mean[k];
+      }
+#pragma unroll
+      for (int k = 0; k < kMlpIn; ++k) f[k] = (f[k] - s.mean[k]) * s.istd[k];
+      put8(s.x0, kKcX, t, 0, f);
+      put8(s.x0, kKcX, t, 8, f + 8);
+    }
+    // forward
+    if (!(ok = run([&] { mma_kk(taddr + kTZ1, sx0, kKcX, sw1, 2, kMlpIn, tc::kIdescM128N64); })))
+      break;
+    tmem_row64(lane_base, kTZ1, v);
+#pragma unroll
+    for (int j = 0; j < kMlpHidden; ++j) v[j] = gelu_tanh(v[j] + s.b1[j]);
+#pragma unroll
+    for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.h1, kKcH, t, k0, v + k0);
+    if (!(ok = run([&] { mma_kk(taddr + kTZ2, sh1, kKcH, sw2, 8, kMlpHidden, tc::kIdescM128N64); })))
+      break;
+    tmem_row64(lane_base, kTZ2, v);
+#pragma unroll
+    for (int j = 0; j < kMlpHidden; ++j) v[j] = gelu_tanh(v[j] + s.b2[j]);
+#pragma unroll
+    for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.h2, kKcH, t, k0, v + k0);
+    if (!(ok = run([&] { mma_kk(taddr + kTZ3, sh2, kKcH, sw3, 8, kMlpHidden, tc::kIdescM128N64); })))
+      break;
+    tmem_row64(lane_base, kTZ3, v);
+    float u = b4;
+#pragma unroll
+    for (int j = 0; j < kMlpHidden; ++j) {
+      v[j] = gelu_tanh(v[j] + s.b3[j]);
+      u = fmaf(s.w4[j], v[j], u);
+    }
+#pragma unroll
+    for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.h3, kKcH, t, k0, v + k0);
+    const float res = valid ? u - tgt : 0.0f;
+    loss = fmaf(res, res, loss);
+    const float g = res * inv_batch;
+    // output layer: dz column 0 = g
+    put8_const(s.dz, kKcD, t, 0, g);
+#pragma unroll
+    for (int k0 = 8; k0 < kMlpHidden; k0 += 8) put8_const(s.dz, kKcD, t, k0, 0.0f);
+    if (!(ok = run([&] { mma_grad(taddr + kTG4, sdz, sh3, kKcH, 80, acc); }))) break;
+    // layer 3
+    tmem_row64(lane_base, kTZ3, v);
+#pragma unroll
+    for (int j = 0; j < kMlpHidden; ++j) v[j] = g * s.w4[j] * gelu_grad(v[j] + s.b3[j]);
+#pragma unroll
+    for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.dz, kKcD, t, k0, v + k0);
+    if (!(ok = run([&] {
+          mma_grad(taddr + kTG3, sdz, sh2, kKcH, 80, acc);
+          mma_dh(taddr + kTZ3, sdz, sw3);
+        })))
+      break;
+    // layer 2: dz2 = dh2 * gelu'(z2)
+#pragma unroll
+    for (int c = 0; c < kMlpHidden; c += 16) {
+      float dh[16], z[16];
+      tc::tmem_ld16(lane_base + kTZ3 + c, dh);
+      tc::tmem_ld16(lane_base + kTZ2 + c, z);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) dh[i] *= gelu_grad(z[i] + s.b2[c + i]);
+      put8(s.dz, kKcD, t, c, dh);
+      put8(s.dz, kKcD, t, c + 8, dh + 8);
+    }
+    if (!(ok = run([&] {
+          mma_grad(taddr + kTG2, sdz, sh1, kKcH, 80, acc);
+          mma_dh(taddr + kTZ2, sdz, sw2);
+        })))
+      break;
+    // layer 1
+#pragma unroll
+    for (int c = 0; c < kMlpHidden; c += 16) {
+      float dh[16], z[16];
+      tc::tmem_ld16(lane_base + kTZ2 + c, dh);
+      tc::tmem_ld16(lane_base + kTZ1 + c, z);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) dh[i] *= gelu_grad(z[i] + s.b1[c + i]);
+      put8(s.dz, kKcD, t, c, dh);
+      put8(s.dz, kKcD, t, c + 8, dh + 8);
+    }
+    if (!(ok = run([&] { mma_grad(taddr + kTG1, sdz, sx0, kKcX, 32, acc); }))) break;
+    acc = true;
+  }
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  if (!ok) {
+    if (t == 0) atomicOr(err, kErrMlpWait);
+  } else {
+    float* out = partial + (size_t)blockIdx.x * (kMlpParams + 1);
+    if (warp < 2) {
+      const int j = t;  // gradient row = output neuron
+#pragma unroll 1
+      for (int l = 0; l < 3; ++l) {
+        const uint32_t col = l == 0 ? kTG3 : (l == 1 ? kTG2 : kTG1);
+        const int ncol = l == 2 ? 32 : 80, nin = l == 2 ? kMlpIn : kMlpHidden;
+        const int ow = l == 0 ? kOffW3 : (l == 1 ? kOffW2 : kOffW1);
+        const int ob = l == 0 ? kOffB3 : (l == 1 ? kOffB2 : kOffB1);
+        for (int c = 0; c < ncol; c += 16) {
+          float g16[16];
+          tc::tmem_ld16(lane_base + col + c, g16);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int k = c + i;
+            if (k < nin) out[ow + j * nin + k] = g16[i];
+            else if (k == nin) out[ob + j] = g16[i];
+          }
+        }
+      }
+    }
+    if (warp == 0) {
+      for (int c = 0; c < 80; c += 16) {
+        float g16[16];
+        tc::tmem_ld16(lane_base + kTG4 + c, g16);
+        tc::tmem_wait_ld();
+        if (t == 0) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int k = c + i;
+            if (k < kMlpHidden) out[kOffW4 + k] = g16[i];
+            else if (k == kMlpHidden) out[kOffB4] = g16[i];
+          }
+        }
+      }
+    }
+    // sum of squared residuals of the CTA's rows
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+    if ((t & 31) == 0) s.red[warp] = loss;
+    __syncthreads();
+    if (t == 0) {
+      float tot = 0.0f;
+      for (int w = 0; w < kMlpTile / 32; ++w) tot += s.red[w];
+      out[kMlpParams] = tot;
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr),
+                 "r"(kTrainCols));
+}
+
+__device__ __forceinline__ bool mlp_is_weight(int k) {
+  return (k >= kOffW1 && k < kOffB1) || (k >= kOffW2 && k < kOffB2) ||
+         (k >= kOffW3 && k < kOffB3) || (k >= kOffW4 && k < kOffB4);
+}
+
+// Sums the CTAs' gradient slices (FP64, fixed order) and, when m is given,
+// applies one AdamW step (decoupled weight decay on weights only) and
+// refreshes the BF16 copy of W1..W3.  Slot kMlpParams of each slice is the
+// CTA's sum of squared residuals; its total goes to *loss_sum.
+__global__ void k_mlp_update(const float* __restrict__ partial, int nparts,
+                             float* __restrict__ params, float* __restrict__ m,
+                             float* __restrict__ v, __nv_bfloat16* __restrict__ wbf,
+                             float* __restrict__ grad_out, float* __restrict__ loss_sum,
+                             float lr, float beta1, float beta2, float eps, float wd, float bc1,
+                             float bc2) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > kMlpParams) return;
+  double g = 0.0;
+  for (int c = 0; c < nparts; ++c) g += (double)partial[(size_t)c * (kMlpParams + 1) + k];
+  if (k == kMlpParams) {
+    if (loss_sum) *loss_sum = (float)g;
+    return;
+  }
+  const float gf = (float)g;
+  if (grad_out) grad_out[k] = gf;
+  if (!m) return;
+  const float mk = beta1 * m[k] + (1.0f - beta1) * gf;
+  const float vk = beta2 * v[k] + (1.0f - beta2) * gf * gf;
+  m[k] = mk;
+  v[k] = vk;
+  float p = params[k];
+  const float upd = (mk * bc1) / (sqrtf(vk * bc2) + eps) + (mlp_is_weight(k) ? wd * p : 0.0f);
+  p -= lr * upd;
+  params[k] = p;
+  const int n1 = kMlpHidden * kMlpIn, n2 = kMlpHidden * kMlpHidden;
+  if (k < kOffB1) wbf[k] = __float2bfloat16_rn(p);
+  else if (k >= kOffW2 && k < kOffB2) wbf[n1 + (k - kOffW2)] = __float2bfloat16_rn(p);
+  else if (k >= kOffW3 && k < kOffB3) wbf[n1 + n2 + (k - kOffW3)] = __float2bfloat16_rn(p);
+}
+
+// Per-column FP64 sums and sums of squares of feat[n][16] and target[n]
+// (17 columns) for the normalisation.
+__global__ void k_mlp_moments(const float* __restrict__ feat, const float* __restrict__ target,
+                              long long n, double* __restrict__ acc) {
+  double s[17], q[17];
+#pragma unroll
+  for (int c = 0; c < 17; ++c) s[c] = q[c] = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float4* fp = reinterpret_cast<const float4*>(feat + i * kMlpIn);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float4 a = __ldg(fp + k);
+      const float e[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        s[4 * k + c] += e[c];
+        q[4 * k + c] += (double)e[c] * e[c];
+      }
+    }
+    const double tv = __ldg(target + i);
+    s[16] += tv;
+    q[16] += tv * tv;
+  }
+#pragma unroll
+  for (int c = 0; c < 17; ++c) {
+    double a = s[c], b = q[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(acc + c, a);
+      atomicAdd(acc + 17 + c, b);
+    }
+  }
 }
 
 __global__ void k_to_bf16(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, int n) {
@@ -329,10 +754,92 @@ void launch_mlp_forward(const MlpDevice& d, const float* feat, int n, float* out
                                            err);
 }
 
-int mlp_warm_start(MlpState& m, const DevParams&, const NbrView&, const PD*, PD*, const float4*,
-                   const uint8_t*, cudaStream_t) {
-  if (!m.ready) return set_error(SPHPC_ENOTREADY, "warm start: no network loaded");
-  return set_error(SPHPC_ENOTREADY, "warm start: features not built yet");
+// ---- device-resident training set (one per process, on the device that
+// made it) ----
+namespace {
+struct MlpDataset {
+  float* feat = nullptr;    // [cap][16]
+  float* target = nullptr;  // [cap]
+  long long n = 0, cap = 0;
+  int device = -1;
+};
+MlpDataset g_ds;
+std::mutex g_ds_mu;
+
+int dataset_check_device() {
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (g_ds.cap > 0 && dev != g_ds.device)
+    return set_error(SPHPC_EINVAL, "training set lives on device %d, current device is %d",
+                     g_ds.device, dev);
+  return SPHPC_OK;
+}
+
+size_t train_smem_bytes() { return sizeof(TrainSmem) + 1024; }
+
+int set_train_attr() {
+  static int done = -1;
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (done == dev) return SPHPC_OK;
+  const cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)train_smem_bytes());
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "MLP training kernel: %s", cudaGetErrorString(e));
+  done = dev;
+  return SPHPC_OK;
+}
+
+int train_grid(int batch) {
+  const int tiles = (batch + kMlpTile - 1) / kMlpTile;
+  return tiles < 148 ? tiles : 148;
+}
+
+// Scratch of a gradient/AdamW run.
+struct TrainBufs {
+  float* partial = nullptr;
+  float* m = nullptr;
+  float* v = nullptr;
+  float* grad = nullptr;
+  float* loss = nullptr;
+  uint32_t* err = nullptr;
+  ~TrainBufs() {
+    if (partial) cudaFree(partial);
+    if (m) cudaFree(m);
+    if (v) cudaFree(v);
+    if (grad) cudaFree(grad);
+    if (loss) cudaFree(loss);
+    if (err) cudaFree(err);
+  }
+};
+
+uint64_t splitmix64(uint64_t& x) {
+  uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+uint64_t gcd_u64(uint64_t a, uint64_t b) {
+  while (b) {
+    const uint64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+}  // namespace
+
+int mlp_dataset_claim(long long want, float** feat, float** target, long long* got) {
+  std::lock_guard<std::mutex> lk(g_ds_mu);
+  *got = 0;
+  if (g_ds.cap == 0) return set_error(SPHPC_ENOTREADY, "no training set reserved");
+  SPHPC_RC(dataset_check_device());
+  const long long room = g_ds.cap - g_ds.n;
+  *got = want < room ? want : room;
+  *feat = g_ds.feat + g_ds.n * kMlpIn;
+  *target = g_ds.target + g_ds.n;
+  g_ds.n += *got;
+  return SPHPC_OK;
 }
 
 }  // namespace sphpc
@@ -360,6 +867,240 @@ extern "C" int sphpc_mlp_forward(const float* d_feat, int n, const float* params
     else if (h) rc = set_error(SPHPC_EKERNEL, "sphpc_mlp_forward: tensor-core wait gave up (0x%x)", h);
   }
   if (err) cudaFree(err);
+  mlp_free(d);
+  return rc;
+}
+
+// Gradient of the batch loss L = 1/(2n) sum (u - t/out_scale)^2 over n rows
+// of device memory, through the training kernels; grad_out[9473] and
+// *loss_out on the host.
+extern "C" int sphpc_mlp_grad(const float* d_feat, const float* d_target, int n,
+                              const float* params, const float* norm, float* grad_out,
+                              float* loss_out, void* cuda_stream) {
+  if (n <= 0 || !d_feat || !d_target || !params || !norm || !grad_out)
+    return set_error(SPHPC_EINVAL, "sphpc_mlp_grad: bad arguments");
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  SPHPC_RC(set_train_attr());
+  MlpDevice d;
+  TrainBufs b;
+  int rc = mlp_upload(d, params, norm, st);
+  const int grid = train_grid(n);
+  if (!rc && (cudaMalloc(&b.partial, sizeof(float) * (size_t)grid * (kMlpParams + 1)) != cudaSuccess ||
+              cudaMalloc(&b.grad, sizeof(float) * kMlpParams) != cudaSuccess ||
+              cudaMalloc(&b.loss, sizeof(float)) != cudaSuccess ||
+              cudaMalloc(&b.err, sizeof(uint32_t)) != cudaSuccess))
+    rc = set_error(SPHPC_ENOMEM, "sphpc_mlp_grad: scratch");
+  if (!rc) {
+    cudaMemsetAsync(b.err, 0, sizeof(uint32_t), st);
+    k_mlp_grad<<<grid, kMlpTile, train_smem_bytes(), st>>>(d.params, d.norm, d.wbf, d_feat, d_target,
+                                                         n, 0, 1, 0, n, b.partial, b.err);
+    k_mlp_update<<<(kMlpParams + 256) / 256, 256, 0, st>>>(b.partial, grid, nullptr, nullptr, nullptr,
+                                                          nullptr, b.grad, b.loss, 0.f, 0.f, 0.f,
+                                                          0.f, 0.f, 0.f, 0.f);
+    uint32_t h = 0;
+    float ls = 0.0f;
+    cudaError_t e = cudaMemcpyAsync(grad_out, b.grad, sizeof(float) * kMlpParams,
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&ls, b.loss, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, b.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = set_error(SPHPC_ECUDA, "sphpc_mlp_grad: %s", cudaGetErrorString(e));
+    else if (h) rc = set_error(SPHPC_EKERNEL, "sphpc_mlp_grad: tensor-core wait gave up (0x%x)", h);
+    if (!rc && loss_out) *loss_out = ls / (2.0f * (float)n);
+  }
+  mlp_free(d);
+  return rc;
+}
+
+extern "C" int sphpc_mlp_dataset_reserve(long long capacity) {
+  std::lock_guard<std::mutex> lk(g_ds_mu);
+  if (capacity <= 0 || capacity > (1ll << 31))
+    return set_error(SPHPC_EINVAL, "sphpc_mlp_dataset_reserve: capacity %lld out of (0, 2^31]",
+                     capacity);
+  if (g_ds.cap > 0) SPHPC_RC(dataset_check_device());
+  if (capacity <= g_ds.cap) return SPHPC_OK;
+  float *f = nullptr, *t = nullptr;
+  if (cudaMalloc(&f, sizeof(float) * kMlpIn * (size_t)capacity) != cudaSuccess ||
+      cudaMalloc(&t, sizeof(float) * (size_t)capacity) != cudaSuccess) {
+    if (f) cudaFree(f);
+    cudaGetLastError();
+    return set_error(SPHPC_ENOMEM, "sphpc_mlp_dataset_reserve: %lld rows", capacity);
+  }
+  if (g_ds.n > 0) {
+    cudaMemcpy(f, g_ds.feat, sizeof(float) * kMlpIn * (size_t)g_ds.n, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(t, g_ds.target, sizeof(float) * (size_t)g_ds.n, cudaMemcpyDeviceToDevice);
+  }
+  if (g_ds.feat) cudaFree(g_ds.feat);
+  if (g_ds.target) cudaFree(g_ds.target);
+  g_ds.feat = f;
+  g_ds.target = t;
+  g_ds.cap = capacity;
+  cudaGetDevice(&g_ds.device);
+  return SPHPC_OK;
+}
+
+extern "C" int sphpc_mlp_dataset_size(long long* n) {
+  if (!n) return set_error(SPHPC_EINVAL, "sphpc_mlp_dataset_size: null");
+  std::lock_guard<std::mutex> lk(g_ds_mu);
+  *n = g_ds.n;
+  return SPHPC_OK;
+}
+
+extern "C" int sphpc_mlp_dataset_clear(void) {
+  std::lock_guard<std::mutex> lk(g_ds_mu);
+  g_ds.n = 0;
+  return SPHPC_OK;
+}
+
+extern "C" int sphpc_mlp_dataset_free(void) {
+  std::lock_guard<std::mutex> lk(g_ds_mu);
+  if (g_ds.feat) cudaFree(g_ds.feat);
+  if (g_ds.target) cudaFree(g_ds.target);
+  g_ds = MlpDataset{};
+  return SPHPC_OK;
+}
+
+// Appends rows from host memory (feat[count][16], target[count]).
+extern "C" int sphpc_mlp_dataset_append(const float* feat, const float* target, long long count) {
+  if (count < 0 || (count > 0 && (!feat || !target)))
+    return set_error(SPHPC_EINVAL, "sphpc_mlp_dataset_append: bad arguments");
+  float *f = nullptr, *t = nullptr;
+  long long got = 0;
+  SPHPC_RC(mlp_dataset_claim(count, &f, &t, &got));
+  if (got < count)
+    return set_error(SPHPC_ENOMEM, "sphpc_mlp_dataset_append: %lld of %lld rows fit", got, count);
+  cudaError_t e = cudaMemcpy(f, feat, sizeof(float) * kMlpIn * (size_t)count, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(t, target, sizeof(float) * (size_t)count, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "sphpc_mlp_dataset_append: %s", cudaGetErrorString(e));
+  return SPHPC_OK;
+}
+
+// Copies rows [offset, offset + count) to host memory.
+extern "C" int sphpc_mlp_dataset_read(long long offset, long long count, float* feat, float* target) {
+  std::lock_guard<std::mutex> lk(g_ds_mu);
+  if (offset < 0 || count < 0 || offset + count > g_ds.n)
+    return set_error(SPHPC_EINVAL, "sphpc_mlp_dataset_read: rows [%lld, %lld) outside [0, %lld)",
+                     offset, offset + count, g_ds.n);
+  cudaError_t e = cudaSuccess;
+  if (feat)
+    e = cudaMemcpy(feat, g_ds.feat + offset * kMlpIn, sizeof(float) * kMlpIn * (size_t)count,
+                   cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && target)
+    e = cudaMemcpy(target, g_ds.target + offset, sizeof(float) * (size_t)count, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "sphpc_mlp_dataset_read: %s", cudaGetErrorString(e));
+  return SPHPC_OK;
+}
+
+// Normalisation of the training set: norm[0..15] = feature means,
+// norm[16..31] = 1 / standard deviations (1 for a constant feature),
+// norm[32] = standard deviation of the targets (1 if constant).
+extern "C" int sphpc_mlp_dataset_stats(float* norm) {
+  if (!norm) return set_error(SPHPC_EINVAL, "sphpc_mlp_dataset_stats: null");
+  std::lock_guard<std::mutex> lk(g_ds_mu);
+  if (g_ds.n < 2) return set_error(SPHPC_ENOTREADY, "sphpc_mlp_dataset_stats: fewer than 2 rows");
+  SPHPC_RC(dataset_check_device());
+  double* acc = nullptr;
+  if (cudaMalloc(&acc, sizeof(double) * 34) != cudaSuccess)
+    return set_error(SPHPC_ENOMEM, "sphpc_mlp_dataset_stats: scratch");
+  cudaMemset(acc, 0, sizeof(double) * 34);
+  k_mlp_moments<<<148 * 4, 256>>>(g_ds.feat, g_ds.target, g_ds.n, acc);
+  double h[34];
+  const cudaError_t e = cudaMemcpy(h, acc, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(acc);
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "sphpc_mlp_dataset_stats: %s", cudaGetErrorString(e));
+  const double nn = (double)g_ds.n;
+  for (int c = 0; c < 17; ++c) {
+    const double mean = h[c] / nn;
+    const double var = std::max(h[17 + c] / nn - mean * mean, 0.0);
+    const double sd = std::sqrt(var);
+    if (c < kMlpIn) {
+      norm[c] = (float)mean;
+      norm[kMlpIn + c] = sd > 1e-12 * std::max(1.0, std::fabs(mean)) ? (float)(1.0 / sd) : 1.0f;
+    } else {
+      norm[2 * kMlpIn] = sd > 0.0 ? (float)sd : 1.0f;
+    }
+  }
+  return SPHPC_OK;
+}
+
+// AdamW training on the training set: `steps` steps of `batch` rows drawn
+// without replacement within each pass over the set (a fresh affine
+// permutation of the row indices per pass, seeded by `seed`), learning rate
+// lr, decoupled weight decay on the weights, beta = (0.9, 0.999), eps 1e-8.
+// params_out[9473] receives the trained parameters; loss_out[steps], if
+// given, the batch loss of every step (before its update).
+extern "C" int sphpc_mlp_train(const float* params_in, const float* norm, int steps, int batch,
+                               float lr, float weight_decay, unsigned long long seed,
+                               float* params_out, float* loss_out) {
+  if (!params_in || !norm || !params_out || steps < 0 || batch <= 0 || !(lr > 0.0f) ||
+      weight_decay < 0.0f)
+    return set_error(SPHPC_EINVAL, "sphpc_mlp_train: bad arguments");
+  long long N = 0;
+  float *feat = nullptr, *target = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_ds_mu);
+    N = g_ds.n;
+    feat = g_ds.feat;
+    target = g_ds.target;
+    if (N > 0) SPHPC_RC(dataset_check_device());
+  }
+  if (N < 1) return set_error(SPHPC_ENOTREADY, "sphpc_mlp_train: empty training set");
+  SPHPC_RC(set_train_attr());
+  cudaStream_t st = 0;
+  MlpDevice d;
+  TrainBufs b;
+  int rc = mlp_upload(d, params_in, norm, st);
+  const int grid = train_grid(batch);
+  if (!rc && (cudaMalloc(&b.partial, sizeof(float) * (size_t)grid * (kMlpParams + 1)) != cudaSuccess ||
+              cudaMalloc(&b.m, sizeof(float) * kMlpParams) != cudaSuccess ||
+              cudaMalloc(&b.v, sizeof(float) * kMlpParams) != cudaSuccess ||
+              cudaMalloc(&b.loss, sizeof(float) * (size_t)(steps > 0 ? steps : 1)) != cudaSuccess ||
+              cudaMalloc(&b.err, sizeof(uint32_t)) != cudaSuccess))
+    rc = set_error(SPHPC_ENOMEM, "sphpc_mlp_train: scratch");
+  if (rc) {
+    mlp_free(d);
+    return rc;
+  }
+  cudaMemsetAsync(b.m, 0, sizeof(float) * kMlpParams, st);
+  cudaMemsetAsync(b.v, 0, sizeof(float) * kMlpParams, st);
+  cudaMemsetAsync(b.err, 0, sizeof(uint32_t), st);
+  const float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
+  uint64_t rng = seed;
+  long long epoch = -1;
+  unsigned long long mul = 1, add = 0;
+  for (int k = 1; k <= steps; ++k) {
+    const long long first = (long long)(k - 1) * batch;
+    const long long e = first / N;
+    if (e != epoch) {
+      epoch = e;
+      if (N > 1) {
+        do {
+          mul = 1 + splitmix64(rng) % (uint64_t)(N - 1);
+        } while (gcd_u64(mul, (uint64_t)N) != 1);
+      }
+      add = splitmix64(rng) % (uint64_t)N;
+    }
+    k_mlp_grad<<<grid, kMlpTile, train_smem_bytes(), st>>>(d.params, d.norm, d.wbf, feat, target, N,
+                                                         first % N, mul, add, batch, b.partial,
+                                                         b.err);
+    const float bc1 = (float)(1.0 / (1.0 - std::pow((double)beta1, (double)k)));
+    const float bc2 = (float)(1.0 / (1.0 - std::pow((double)beta2, (double)k)));
+    k_mlp_update<<<(kMlpParams + 256) / 256, 256, 0, st>>>(b.partial, grid, d.params, b.m, b.v,
+                                                          d.wbf, nullptr, b.loss + (k - 1), lr,
+                                                          beta1, beta2, eps, weight_decay, bc1,
+                                                          bc2);
+  }
+  uint32_t h = 0;
+  cudaError_t ce = cudaMemcpyAsync(params_out, d.params, sizeof(float) * kMlpParams,
+                                   cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess && loss_out && steps > 0)
+    ce = cudaMemcpyAsync(loss_out, b.loss, sizeof(float) * steps, cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(&h, b.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  if (ce != cudaSuccess) rc = set_error(SPHPC_ECUDA, "sphpc_mlp_train: %s", cudaGetErrorString(ce));
+  else if (h) rc = set_error(SPHPC_EKERNEL, "sphpc_mlp_train: tensor-core wait gave up (0x%x)", h);
+  if (!rc && loss_out)
+    for (int k = 0; k < steps; ++k) loss_out[k] /= 2.0f * (float)batch;
   mlp_free(d);
   return rc;
 }

@@ -57,14 +57,13 @@ int mlp_upload(MlpDevice& d, const float* params, const float* norm, cudaStream_
 void mlp_free(MlpDevice& d);
 
 // Forward pass of n feature rows feat[n][16] -> out[n] (lambda0), or when
-// pd_in/pd_out are given, records pd_out[p] = {x, (d, lambda0)} from pd_in.
+// pd_in/pd_out are given, records pd_out[p] = {x, (d, min(lambda0, 0))} from
+// pd_in (the plain solver's multipliers are never positive).
 void launch_mlp_forward(const MlpDevice& d, const float* feat, int n, float* out,
                         const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st);
 
-// Warm start of one step: features of the predicted state, then the
-// network's lambda0 into pd_out; returns a negative code when no network is
-// loaded.
-int mlp_warm_start(MlpState& m, const DevParams& P, const NbrView& V, const PD* pd, PD* pd_out,
-                   const float4* vel, const uint8_t* ncount, cudaStream_t st);
+// Reserves `want` rows of the process's training set (fewer when it is
+// nearly full: *got) and returns their feature and target pointers.
+int mlp_dataset_claim(long long want, float** feat, float** target, long long* got);
 
 }  // namespace sphpc

@@ -117,6 +117,102 @@ __global__ void __launch_bounds__(kBlock)
   if (RESID) block_resid(err, a.resid);
 }
 
+// The first density/lambda pass of a step (mode 0, with residual) that also
+// writes the 16 warm-start features of each particle p < limit to
+// feat[p][16]:
+//   0 rho/rho0 - 1       1 C = max(rho/rho0 - 1, 0)     2 lambda
+//   3 sum_q |grad_q C|^2 4 |grad_p C|^2 (both with the 1/rho0^2 of lambda)
+//   5 neighbour count    6-8 mean neighbour offset (x_q - x_p) / h
+//   9-11 mean relative velocity (v_q - v_p) dt / h
+//   12 SDF distance at x* / h, clamped to [-4, 4] (4 without an obstacle)
+//   13 nearest-neighbour distance / h (1 without neighbours)
+//   14 distance to the nearest box wall / h, clamped to [0, 4]
+//   15 velocity along the gravity axis * dt / h
+__global__ void __launch_bounds__(kBlock)
+    k_features(const DevParams P, const NbrView V, const PassArgs a, float* __restrict__ feat,
+               int limit) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  double err = 0.0;
+  if (p < P.n) {
+    float4 xp, dp;
+    ld_pd(a.pd, p, xp, dp);
+    const float4 vp = a.vel[p];
+    float rho = P.W0m, comp = 0.0f;
+    float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
+    float ox = 0.f, oy = 0.f, oz = 0.f, ux = 0.f, uy = 0.f, uz = 0.f, rmin2 = P.h2;
+    int cnt = 0;
+    for_each_neighbor(V, p, [&](int q) {
+      float4 xq, dq;
+      ld_pd(a.pd, q, xq, dq);
+      const Pair g = pair_geom(xp, dp, xq, dq);
+      const float t = P.h2 - g.r2;
+      const float w = t > 0.0f ? P.Wn_m * t * t * t : 0.0f;
+      const float y = w - comp;
+      const float s = rho + y;
+      comp = (s - rho) - y;
+      rho = s;
+      float r, rinv;
+      floored_r(P, g.r2, r, rinv);
+      const float hm = P.h - r;
+      const float c = hm > 0.0f ? P.DWn_m * hm * hm * rinv : 0.0f;
+      const float gx = c * g.dx, gy = c * g.dy, gz = c * g.dz;
+      sgx += gx;
+      sgy += gy;
+      sgz += gz;
+      sC += gx * gx + gy * gy + gz * gz;
+      const float4 vq = __ldg(a.vel + q);
+      ox -= g.dx;
+      oy -= g.dy;
+      oz -= g.dz;
+      ux += vq.x - vp.x;
+      uy += vq.y - vp.y;
+      uz += vq.z - vp.z;
+      rmin2 = fminf(rmin2, g.r2);
+      ++cnt;
+    });
+    a.rho[p] = rho;
+    const float C = (float)fmax(__ddiv_rn((double)rho, P.rho0_d) - 1.0, 0.0);
+    const float s_pairs = sC * P.inv_rho0_sq;
+    const float s_self = (sgx * sgx + sgy * sgy + sgz * sgz) * P.inv_rho0_sq;
+    const float lam = -C / ((sC + sgx * sgx + sgy * sgy + sgz * sgz) * P.inv_rho0_sq + P.lambda_eps);
+    st_pd(a.pd_out, p, xp, make_float4(dp.x, dp.y, dp.z, lam));
+    err = fmax((double)rho / (double)P.rho0 - 1.0, 0.0);
+    if (p < limit) {
+      const float inv_h = 1.0f / P.h;
+      const float inv_cnt = cnt > 0 ? 1.0f / (float)cnt : 0.0f;
+      const float vs = P.dt * inv_h * inv_cnt;
+      const double xs = xstar_d(xp.x, dp.x), ys = xstar_d(xp.y, dp.y), zs = xstar_d(xp.z, dp.z);
+      float sdf = 4.0f;
+      if (P.has_sdf && xs > P.ob_min[0] && xs < P.ob_max[0] && ys > P.ob_min[1] &&
+          ys < P.ob_max[1] && zs > P.ob_min[2] && zs < P.ob_max[2]) {
+        const float xt = (float)((xs - P.ob_min[0]) / (double)P.ob_len[0]);
+        const float yt = (float)((ys - P.ob_min[1]) / (double)P.ob_len[1]);
+        const float zt = (float)((zs - P.ob_min[2]) / (double)P.ob_len[2]);
+        sdf = fminf(fmaxf(sdf_sample(P, xt, yt, zt) * P.model_to_world * inv_h, -4.0f), 4.0f);
+      }
+      double wall = fmin(fmin(xs - P.bmin[0], P.bmax[0] - xs),
+                         fmin(fmin(ys - P.bmin[1], P.bmax[1] - ys), fmin(zs - P.bmin[2], P.bmax[2] - zs)));
+      const float fw = fminf(fmaxf((float)(wall / P.hd), 0.0f), 4.0f);
+      const float vg = (P.gaxis == 0 ? vp.x : (P.gaxis == 1 ? vp.y : vp.z)) * P.dt * inv_h;
+      float4* out = reinterpret_cast<float4*>(feat + (size_t)p * 16);
+      out[0] = make_float4(rho * P.inv_rho0 - 1.0f, C, lam, s_pairs);
+      out[1] = make_float4(s_self, (float)cnt, ox * inv_h * inv_cnt, oy * inv_h * inv_cnt);
+      out[2] = make_float4(oz * inv_h * inv_cnt, ux * vs, uy * vs, uz * vs);
+      out[3] = make_float4(sdf, sqrtf(rmin2) * inv_h, fw, vg);
+    }
+  }
+  block_resid(err, a.resid);
+}
+
+// target[p] += s * lambda_p (lambda in d.w of the records) for p < limit:
+// the stiffness-weighted multiplier sum of a plain solve, the warm-start
+// network's training target.
+__global__ void k_accum_lambda(const PD* __restrict__ rec, float s, float* __restrict__ target,
+                               int limit) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < limit) target[p] += s * rec[p].d.w;
+}
+
 template <int MODE, int SCORR_N, bool SDF>
 __global__ void __launch_bounds__(kBlock)
     k_position(const DevParams P, const NbrView V, const PassArgs a) {
@@ -455,6 +551,15 @@ void launch_density_lambda(const DevParams& P, const NbrView& V, const PassArgs&
   } else {
     k_density_lambda<2, false><<<g, kBlock, 0, st>>>(P, V, a);
   }
+}
+
+void launch_features(const DevParams& P, const NbrView& V, const PassArgs& a, float* feat,
+                     int limit, cudaStream_t st) {
+  k_features<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a, feat, limit);
+}
+
+void launch_accum_lambda(const PD* rec, float s, float* target, int limit, cudaStream_t st) {
+  if (limit > 0) k_accum_lambda<<<(limit + kBlock - 1) / kBlock, kBlock, 0, st>>>(rec, s, target, limit);
 }
 
 void launch_position(const DevParams& P, const NbrView& V, const PassArgs& a, int mode,

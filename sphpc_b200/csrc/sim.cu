@@ -26,20 +26,6 @@ struct Obstacle_CUDA {
 
 namespace sphpc {
 
-#define SPHPC_CK(call)                                                                  \
-  do {                                                                                  \
-    cudaError_t e_ = (call);                                                            \
-    if (e_ != cudaSuccess)                                                              \
-      return set_error(SPHPC_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
-                       __FILE__, __LINE__);                                             \
-  } while (0)
-
-#define SPHPC_RC(expr)      \
-  do {                      \
-    const int rc_ = (expr); \
-    if (rc_) return rc_;    \
-  } while (0)
-
 template <class T>
 static int dalloc(T** p, size_t n) {
   if (n == 0) n = 1;
@@ -100,6 +86,13 @@ class DeviceSim {
   bool nbr_valid = false;
 
   MlpState mlp{};
+  PD* pd_w = nullptr;            // third record buffer of the warm start
+  int last_warm_rejected = 0;
+  // training-set collection of the current step (collect_iters > 0)
+  int collect_iters = 0;
+  long long collect_rows = 0;
+  float* collect_feat = nullptr;
+  float* collect_target = nullptr;
 
   unsigned long long launches = 0;  // kernels launched by this particle set
   double last_iterations = 0.0;
@@ -133,6 +126,7 @@ class DeviceSim {
     dfree(nbr); dfree(xsa); dfree(cstart); dfree(ncount); dfree(gaps); dfree(small);
     dfree(resid); dfree(sort.keys_alt); dfree(sort.vals_alt); dfree(sort_aux); dfree(stage);
     mlp_release(mlp);
+    dfree(pd_w);
     for (auto& p : pending) {
       cudaEventDestroy(p.a);
       cudaEventDestroy(p.b);
@@ -295,6 +289,18 @@ class DeviceSim {
 
   int find_neighbors(const DevParams& P, bool predict, bool full, bool move_vel);
   int run_step(const DevParams& P, const Params& prm);
+
+  int ensure_warm_buffers() {
+    if (!pd_w) SPHPC_RC(dalloc(&pd_w, n));
+    if (mlp.feat_cap < n) {
+      if (mlp.feat) cudaFree(mlp.feat);
+      mlp.feat = nullptr;
+      mlp.feat_cap = 0;
+      SPHPC_RC(dalloc(&mlp.feat, (size_t)n * kMlpIn));
+      mlp.feat_cap = n;
+    }
+    return SPHPC_OK;
+  }
 };
 
 DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob) const {
@@ -449,78 +455,144 @@ static float stiffness_of(double k_stiff, int substep) {
 }
 
 int DeviceSim::run_step(const DevParams& P, const Params& prm) {
-  const bool warm = solver.warm_start && mlp.ready;
-  SPHPC_RC(find_neighbors(P, true, false, warm));
+  const bool collect = collect_iters > 0;
+  const bool warm = !collect && solver.warm_start && mlp.ready;
+  SPHPC_RC(find_neighbors(P, true, false, warm || collect));
   const NbrView V = view();
   PassArgs a{};
   a.rho = rho;
   a.vel = vel;
   a.vel_out = vel;
   a.resid = resid;
-  const int fixed_iters = solver.solve_iterations;
-  const bool adaptive = solver.adaptive != 0;
-  const int max_iters = adaptive ? solver.max_iterations : fixed_iters;
+  const bool adaptive = solver.adaptive != 0 && !collect;
+  const int plain_cap =
+      collect ? collect_iters : (adaptive ? solver.max_iterations : solver.solve_iterations);
+  const double tol = solver.density_tolerance;
   last_warm = 0.0;
-  // The current records are always in `pd`; the density/lambda pass writes
-  // pd_alt and the position pass writes back into pd.
-  if (warm) {
-    // warm start: features -> MLP lambda0 -> one position pass (stiffness 1)
-    Scope sc(this, "mlp_warm_start");
-    SPHPC_RC(mlp_warm_start(mlp, P, V, pd, pd_alt, vel, ncount, stream));
-    a.pd = pd_alt;
+  last_warm_rejected = 0;
+  // The current positions are always the records in `pd`.  A density/lambda
+  // pass (A) reads pd and writes records with lambda in d.w; a position pass
+  // (B) reads such records and writes the new positions into pd.
+  auto pass_a = [&](PD* out, bool with_resid) -> int {
+    Scope sc(this, "density_lambda");
+    if (with_resid) SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
+    a.pd = pd;
+    a.pd_out = out;
+    a.lam = nullptr;
+    launch_density_lambda(P, V, a, 0, with_resid, stream);
+    launches += 1;
+    return SPHPC_OK;
+  };
+  auto read_resid = [&](double& max_err) -> int {
+    double h_res[2];
+    SPHPC_CK(cudaMemcpyAsync(h_res, resid, sizeof(h_res), cudaMemcpyDeviceToHost, stream));
+    SPHPC_CK(cudaStreamSynchronize(stream));
+    last_max_err = max_err = h_res[0];
+    last_mean_err = h_res[1] / (n > 0 ? n : 1);
+    return SPHPC_OK;
+  };
+  auto pass_b = [&](const PD* in, float stiffness, bool last) {
+    Scope sc(this, "position");
+    a.pd = in;
     a.pd_out = pd;
-    a.stiffness = 1.0f;
-    a.last = 0;
+    a.stiffness = stiffness;
+    a.last = last ? 1 : 0;
     launch_position(P, V, a, 0, stream);
     launches += 1;
-    last_warm = 1.0;
-  }
-  int iters = 0;
+  };
+  int iters = 0, plain = 0;
   bool converged = false;
-  for (int k = 0; k < max_iters; ++k) {
+  const PD* ready = nullptr;  // records with lambda for the next B (its A already run)
+  if (collect) {
+    // the first A also writes the features of the (predicted) state; the
+    // target accumulates s_k * lambda_k over the fixed iterations
+    Scope sc(this, "mlp_collect");
+    SPHPC_CK(cudaMemsetAsync(collect_target, 0, sizeof(float) * (size_t)collect_rows, stream));
+    SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
+    a.pd = pd;
+    a.pd_out = pd_alt;
+    launch_features(P, V, a, collect_feat, (int)collect_rows, stream);
+    launches += 1;
+    ready = pd_alt;
+  } else if (warm) {
+    SPHPC_RC(ensure_warm_buffers());
+    double err0 = 0.0, err1 = 0.0;
     {
-      Scope sc(this, "density_lambda");
+      Scope sc(this, "mlp_features");
       SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
       a.pd = pd;
       a.pd_out = pd_alt;
-      a.lam = nullptr;
-      launch_density_lambda(P, V, a, 0, true, stream);
+      launch_features(P, V, a, mlp.feat, n, stream);
       launches += 1;
     }
-    if (adaptive) {
-      double h_res[2];
-      SPHPC_CK(cudaMemcpyAsync(h_res, resid, sizeof(h_res), cudaMemcpyDeviceToHost, stream));
-      SPHPC_CK(cudaStreamSynchronize(stream));
-      last_max_err = h_res[0];
-      last_mean_err = h_res[1] / (n > 0 ? n : 1);
-      if (h_res[0] <= solver.density_tolerance) {
+    SPHPC_RC(read_resid(err0));
+    if (err0 <= tol && adaptive) {
+      converged = true;
+    } else {
+      {
+        Scope sc(this, "mlp_forward");
+        launch_mlp_forward(mlp.dev, mlp.feat, n, nullptr, pd_alt, pd_w, err(), stream);
+        launches += 1;
+      }
+      // the network's multipliers, applied at full stiffness in one pass
+      pass_b(pd_w, 1.0f, false);
+      ++iters;
+      last_warm = 1.0;
+      SPHPC_RC(pass_a(pd_w, true));
+      SPHPC_RC(read_resid(err1));
+      if (adaptive && err1 <= tol) {
         converged = true;
-        break;
+      } else if (!(err1 < err0)) {
+        // FP64 residual gate: the warm pass did not lower the maximum density
+        // error, so it is discarded and the plain solve restarts from the
+        // predicted positions (pd_alt still holds them with lambda_0)
+        last_warm_rejected = 1;
+        ready = pd_alt;
+      } else {
+        ready = pd_w;
+        plain = 1;  // the warm pass takes the place of plain substep 0
       }
     }
-    {
-      Scope sc(this, "position");
-      a.pd = pd_alt;
-      a.pd_out = pd;
-      // the warm-started pass counts as substep 0; plain iterations continue
-      a.stiffness = stiffness_of(solver.stiffness_k, warm ? k + 1 : k);
-      a.last = (!adaptive && k == max_iters - 1) ? 1 : 0;
-      launch_position(P, V, a, 0, stream);
+  }
+  const int first_plain = plain;
+  while (!converged && plain - first_plain < plain_cap) {
+    const PD* src = ready;
+    ready = nullptr;
+    if (!src) {
+      SPHPC_RC(pass_a(pd_alt, adaptive));
+      if (adaptive) {
+        double e = 0.0;
+        SPHPC_RC(read_resid(e));
+        if (e <= tol) {
+          converged = true;
+          break;
+        }
+      }
+      src = pd_alt;
+    }
+    const float stiff = stiffness_of(solver.stiffness_k, plain);
+    if (collect) {
+      launch_accum_lambda(src, stiff, collect_target, (int)collect_rows, stream);
       launches += 1;
     }
+    const bool last = !adaptive && plain - first_plain == plain_cap - 1;
+    pass_b(src, stiff, last);
+    ++plain;
     ++iters;
   }
-  if (adaptive || max_iters == 0) {
-    // converged (or cap reached): velocities from x* and the freshest density
+  const bool fused_velocity = !adaptive && plain - first_plain == plain_cap && plain_cap > 0;
+  if (!fused_velocity) {
+    // converged (or capped, or no plain pass): velocities from x* and the
+    // freshest density
     Scope sc(this, "velocity");
-    if (converged || max_iters == 0) {
+    if (converged || iters == 0) {
       launch_pack_w(P, pd, rho, stream);
       launches += 1;
     }
     launch_update_velocities(P, pd, vel, stream);
     launches += 1;
   }
-  last_iterations = iters + (warm ? 1 : 0);
+  last_iterations = iters;
   last_converged = converged ? 1 : 0;
   // post-solve passes (simulation.c:93-106); the last one writes x = x*,
   // d = 0 (UpdatePositions) into pd_alt
@@ -1123,6 +1195,88 @@ int sphpc_step(struct Particles* particles, const struct Params* params,
   return SPHPC_OK;
 }
 
+// ---- learned warm start ----
+
+int sphpc_mlp_load(struct Particles* particles, const float* params, const float* norm) {
+  SPHPC_SIM(s, particles);
+  if (!params || !norm) return set_error(SPHPC_EINVAL, "sphpc_mlp_load: null argument");
+  SPHPC_RC(mlp_upload(s->mlp.dev, params, norm, s->stream));
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  s->mlp.ready = true;
+  return SPHPC_OK;
+}
+
+int sphpc_mlp_unload(struct Particles* particles) {
+  SPHPC_SIM(s, particles);
+  mlp_release(s->mlp);
+  return SPHPC_OK;
+}
+
+int sphpc_mlp_collect(struct Particles* particles, const struct Params* params,
+                      struct Neighbors* neighbors, const struct AABB* boundary_global,
+                      const struct Obstacle* obstacle, int iterations) {
+  (void)neighbors;
+  SPHPC_SIM(s, particles);
+  if (!params || !boundary_global) return set_error(SPHPC_EINVAL, "sphpc_mlp_collect: null argument");
+  if (iterations < 1 || iterations > 64)
+    return set_error(SPHPC_EINVAL, "sphpc_mlp_collect: iterations %d outside [1, 64]", iterations);
+  if (!s->grid_ready) SPHPC_RC(s->init_grid(*boundary_global, params->smoothing_radius));
+  float *f = nullptr, *t = nullptr;
+  long long got = 0;
+  SPHPC_RC(mlp_dataset_claim(s->n, &f, &t, &got));
+  const DevParams P = s->params(*params, boundary_global, obstacle);
+  s->collect_iters = iterations;
+  s->collect_rows = got;
+  s->collect_feat = f;
+  s->collect_target = t;
+  const int rc = s->run_step(P, *params);
+  s->collect_iters = 0;
+  s->collect_rows = 0;
+  s->collect_feat = s->collect_target = nullptr;
+  if (rc) return rc;
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  return (int)got;
+}
+
+__global__ void k_scatter_rows16(int n, const uint32_t* __restrict__ ids,
+                                 const float4* __restrict__ src, float4* __restrict__ dst) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const uint32_t id = ids[p];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) dst[(size_t)id * 4 + k] = src[(size_t)p * 4 + k];
+}
+
+int sphpc_mlp_features(struct Particles* particles, const struct Params* params,
+                       const struct AABB* boundary_global, const struct Obstacle* obstacle,
+                       float* features) {
+  SPHPC_SIM(s, particles);
+  if (!params || !boundary_global || !features)
+    return set_error(SPHPC_EINVAL, "sphpc_mlp_features: null argument");
+  if (!s->nbr_valid) return set_error(SPHPC_ENOTREADY, "sphpc_mlp_features: call FindAllNeighbors first");
+  SPHPC_RC(s->ensure_warm_buffers());
+  const DevParams P = s->params(*params, boundary_global, obstacle);
+  PassArgs a{};
+  a.pd = s->pd;
+  a.pd_out = s->pd_w;
+  a.rho = s->rho_alt ? s->rho_alt : s->rho;
+  a.vel = s->vel;
+  a.resid = s->resid;
+  SPHPC_CK(cudaMemsetAsync(s->resid, 0, 2 * sizeof(double), s->stream));
+  launch_features(P, s->view(), a, s->mlp.feat, s->n, s->stream);
+  float4* out = nullptr;
+  SPHPC_RC(dalloc(&out, (size_t)s->n * 4));
+  k_scatter_rows16<<<(s->n + 255) / 256, 256, 0, s->stream>>>(
+      s->n, s->ids, reinterpret_cast<const float4*>(s->mlp.feat), out);
+  cudaError_t e = cudaMemcpyAsync(features, out, sizeof(float) * 16 * (size_t)s->n,
+                                  cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  dfree(out);
+  s->launches += 2;
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "sphpc_mlp_features: %s", cudaGetErrorString(e));
+  return SPHPC_OK;
+}
+
 int sphpc_diagnostics(const struct Particles* particles, struct SphpcDiag* diag) {
   SPHPC_SIM(s, particles);
   if (!diag) return set_error(SPHPC_EINVAL, "sphpc_diagnostics: null");
@@ -1153,6 +1307,7 @@ int sphpc_step_info(const struct Particles* particles, struct SphpcStepInfo* inf
   info->iterations = (int)s->last_iterations;
   info->converged = s->last_converged;
   info->warm_start_used = s->last_warm != 0.0;
+  info->warm_start_rejected = s->last_warm_rejected;
   info->max_density_error = s->last_max_err;
   info->mean_density_error = s->last_mean_err;
   return SPHPC_OK;

@@ -136,6 +136,7 @@ class Simulation:
         call("sphpc_step_info", C.byref(self.particles), C.byref(i))
         return {"iterations": i.iterations, "converged": i.converged,
                 "warm_start_used": i.warm_start_used,
+                "warm_start_rejected": i.warm_start_rejected,
                 "max_density_error": i.max_density_error,
                 "mean_density_error": i.mean_density_error}
 
@@ -203,6 +204,24 @@ class Simulation:
 
     def update_positions(self):
         call("UpdatePositions", C.byref(self.particles))
+
+    # ---------------- learned warm start ----------------
+    def mlp_load(self, params, norm):
+        """Installs the warm-start network (params[9473], norm[33])."""
+        p = np.ascontiguousarray(params, np.float32)
+        q = np.ascontiguousarray(norm, np.float32)
+        F = C.POINTER(C.c_float)
+        call("sphpc_mlp_load", C.byref(self.particles), p.ctypes.data_as(F), q.ctypes.data_as(F))
+
+    def mlp_unload(self):
+        call("sphpc_mlp_unload", C.byref(self.particles))
+
+    def mlp_features(self) -> np.ndarray:
+        """Warm-start features [N][16] by particle id (after find_all_neighbors)."""
+        f = np.zeros((self.n, 16), np.float32)
+        call("sphpc_mlp_features", C.byref(self.particles), C.byref(self.params),
+             C.byref(self.boundary), self._ob(), f.ctypes.data_as(C.POINTER(C.c_float)))
+        return f
 
     def neighbor_buckets(self):
         idx = np.zeros(self.n * _lib.MAX_NEIGHBORS, np.uint32)

@@ -1,0 +1,148 @@
+"""Generate the warm start's training set with the plain solver and train the
+network on the device.
+
+    python -m sphpc_b200.train_warm_start [--out sphpc_b200/weights/warm_start.npz]
+
+Training rows come from the plain PBF solve of two scenes, each with eight
+jitter seeds (1-8): the 1,048,576-particle dam break (dam_break_1m) and the
+4,194,304-particle obstacle scene with surface tension (obstacle_4m).  Every
+scene runs `--steps` steps with the adaptive plain solver (max density error
+<= 1%); every `--every` steps one step is taken by sphpc_mlp_collect, which
+solves with `--iterations` fixed plain substeps and appends one row per
+particle: the 16 features of the predicted state and the target
+Lambda = sum_k s_k lambda_k.  The network is then trained with AdamW (lr 1e-3,
+batch 65,536) by the library's tensor-core kernels, and evaluated on a
+collected step of a seed that was not trained on (seed 9).  The network file
+and a JSON log (loss curve, data sizes, held-out fit) are written.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import warm_start as ws
+from .simulation import Simulation
+
+SCENES = ("dam_break_1m", "obstacle_4m")
+
+
+def collect_scene(config, seed, steps, every, iterations, tol, log):
+    solver = {"adaptive": 1, "density_tolerance": tol, "max_iterations": 12, "seed": seed}
+    rows = 0
+    t0 = time.perf_counter()
+    with Simulation(config, solver) as sim:
+        for k in range(steps):
+            if k % every == every // 2:
+                rows += ws.collect(sim, iterations)
+            else:
+                sim.step(1)
+        d = sim.diagnostics()
+    log(f"  {config} seed {seed}: {rows} rows, {time.perf_counter() - t0:.1f} s, "
+        f"final max density error {d['max_density_error']:.4f}")
+    return rows
+
+
+def held_out_fit(params, norm, config, seed, steps, every, iterations, tol):
+    """R^2 and relative RMS error of the network on rows of an unseen seed."""
+    import ctypes as C
+    import torch
+    from ._lib import call
+    ws.dataset_clear()
+    collect_scene(config, seed, steps, every, iterations, tol, lambda *a: None)
+    n = ws.dataset_size()
+    feat, target = ws.dataset_read(0, n)
+    d_feat = torch.from_numpy(feat).cuda()
+    d_out = torch.zeros(n, device="cuda")
+    F = C.POINTER(C.c_float)
+    call("sphpc_mlp_forward", C.c_void_p(d_feat.data_ptr()), n, params.ctypes.data_as(F),
+         norm.ctypes.data_as(F), C.c_void_p(d_out.data_ptr()),
+         C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    pred = np.minimum(d_out.cpu().numpy().astype(np.float64), 0.0)
+    t = target.astype(np.float64)
+    ss_res = np.sum((pred - t) ** 2)
+    ss_tot = np.sum((t - t.mean()) ** 2)
+    lam0 = feat[:, 2].astype(np.float64)
+    # the first plain multiplier, best scaled, as the no-learning baseline
+    a = float(lam0 @ t / max(lam0 @ lam0, 1e-300))
+    ss_lin = np.sum((a * lam0 - t) ** 2)
+    return {"config": config, "seed": seed, "rows": int(n), "r2": float(1 - ss_res / ss_tot),
+            "rel_rms": float(np.sqrt(ss_res / max(np.sum(t * t), 1e-300))),
+            "baseline_scaled_lambda0_r2": float(1 - ss_lin / ss_tot),
+            "baseline_scale": a}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--out", default=ws.DEFAULT_WEIGHTS)
+    ap.add_argument("--log", default=None, help="JSON log (default: next to --out)")
+    ap.add_argument("--seeds", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--every", type=int, default=100)
+    ap.add_argument("--iterations", type=int, default=6)
+    ap.add_argument("--tol", type=float, default=0.01)
+    ap.add_argument("--epochs", type=float, default=3.0)
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--weight-decay", type=float, default=1e-4)
+    ap.add_argument("--capacity", type=int, default=230_000_000)
+    ap.add_argument("--scenes", default=",".join(SCENES))
+    args = ap.parse_args(argv)
+    logf = args.log or os.path.splitext(args.out)[0] + "_log.json"
+    lines = []
+
+    def log(msg):
+        print(msg, flush=True)
+        lines.append(msg)
+
+    scenes = args.scenes.split(",")
+    t0 = time.perf_counter()
+    ws.dataset_reserve(args.capacity)
+    ws.dataset_clear()
+    log(f"collecting: scenes {scenes}, seeds 1-{args.seeds}, {args.steps} steps, "
+        f"one collected step every {args.every}, {args.iterations} plain substeps")
+    for config in scenes:
+        for seed in range(1, args.seeds + 1):
+            collect_scene(config, seed, args.steps, args.every, args.iterations, args.tol, log)
+    n = ws.dataset_size()
+    t_collect = time.perf_counter() - t0
+    norm = ws.dataset_stats()
+    log(f"training set: {n} rows in {t_collect:.1f} s; target std {norm[32]:.4g}")
+    steps = int(args.epochs * n / args.batch)
+    params = ws.init_params(0)
+    t1 = time.perf_counter()
+    params, loss = ws.train(params, norm, steps, batch=args.batch, lr=args.lr,
+                            weight_decay=args.weight_decay, seed=1)
+    t_train = time.perf_counter() - t1
+    log(f"trained {steps} AdamW steps of {args.batch} rows in {t_train:.1f} s "
+        f"({steps * args.batch / t_train:.3g} rows/s); loss {loss[:10].mean():.4g} -> "
+        f"{loss[-100:].mean():.4g}")
+    if not np.all(np.isfinite(params)):
+        raise SystemExit("training diverged (non-finite parameters)")
+    fit = [held_out_fit(params, norm, c, args.seeds + 1, args.steps, args.every,
+                        args.iterations, args.tol) for c in scenes]
+    for f in fit:
+        log(f"held-out {f['config']} seed {f['seed']}: R^2 {f['r2']:.4f} (scaled lambda_0: "
+            f"{f['baseline_scaled_lambda0_r2']:.4f}), relative RMS {f['rel_rms']:.4f}")
+    meta = {"features": list(ws.FEATURES), "rows": int(n), "steps": steps,
+            "batch": args.batch, "lr": args.lr, "weight_decay": args.weight_decay,
+            "scenes": scenes, "seeds": list(range(1, args.seeds + 1)),
+            "collect_every": args.every, "sim_steps": args.steps,
+            "target": f"sum_k s_k lambda_k over {args.iterations} plain substeps"}
+    ws.save_network(args.out, params, norm, meta)
+    every = max(1, steps // 200)
+    with open(logf, "w") as fh:
+        json.dump({"meta": meta, "collect_seconds": t_collect, "train_seconds": t_train,
+                   "rows_per_second": steps * args.batch / t_train,
+                   "loss_every": every, "loss": [float(x) for x in loss[::every]],
+                   "held_out": fit, "log": lines}, fh, indent=1)
+    ws.dataset_free()
+    log(f"wrote {args.out} and {logf}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,101 @@
+"""Warm start of the constraint solve on the device: the 16 features and the
+training target against the FP64 oracle, and the FP64 residual gate."""
+import numpy as np
+import pytest
+
+from helpers import assert_close, oracle_for
+from sphpc_b200 import Simulation
+from sphpc_b200 import warm_start as ws
+
+pytestmark = pytest.mark.gpu
+
+# per-feature tolerance: rtol, fraction of the column's max |value|
+FEATURE_TOL = {0: (0, 1e-5), 1: (0, 1e-5), 2: (1e-4, 1e-4), 3: (1e-4, 1e-5), 4: (1e-3, 1e-4),
+               5: (0, 0), 6: (0, 1e-4), 7: (0, 1e-4), 8: (0, 1e-4), 9: (0, 1e-4),
+               10: (0, 1e-4), 11: (0, 1e-4), 12: (1e-5, 1e-5), 13: (1e-5, 1e-6),
+               14: (1e-6, 1e-6), 15: (1e-6, 1e-6)}
+
+
+def _check_features(got, want, what):
+    for k, (rtol, frac) in FEATURE_TOL.items():
+        assert_close(got[:, k], want[:, k], rtol, frac, atol=1e-7, what=f"{what}: feature {k}")
+
+
+@pytest.mark.parametrize("config", ["small_dam", "small_obstacle"])
+def test_features_match_oracle(config):
+    with Simulation(config) as sim:
+        sim.step(6)
+        st = sim.fetch()
+        o = oracle_for(sim, st)
+        sim.apply_gravity()
+        sim.predict_positions()
+        sim.find_all_neighbors()
+        got = sim.mlp_features()
+        o.call("apply_gravity")
+        o.call("predict_positions")
+        o.call("find_all_neighbors")
+        want = o.features()
+        _check_features(got, want, config)
+        if config == "small_obstacle":
+            assert np.any(want[:, 12] < 4.0)  # some particles inside the obstacle box
+        assert sim.device_errors() == 0
+
+
+@pytest.mark.parametrize("config,iterations", [("small_dam", 4), ("small_obstacle", 6)])
+def test_collected_rows_match_oracle(config, iterations):
+    """sphpc_mlp_collect: features of the predicted state and the target
+    sum_k s_k lambda_k of a plain solve, row for row (rows are in the step's
+    cell-sorted order; the step's particle ids map them back)."""
+    with Simulation(config) as sim:
+        sim.step(4)
+        st = sim.fetch()
+        o = oracle_for(sim, st)
+        ws.dataset_reserve(sim.n)
+        ws.dataset_clear()
+        rows = ws.collect(sim, iterations)
+        assert rows == sim.n and ws.dataset_size() == sim.n
+        _, ids, _ = sim.cell_data()
+        feat, target = ws.dataset_read(0, sim.n)
+        o.call("apply_gravity")
+        o.call("predict_positions")
+        o.call("find_all_neighbors")
+        want_f = o.features()[ids]
+        want_t = o.lambda_target(iterations)[ids]
+        _check_features(feat, want_f, config)
+        assert_close(target, want_t, 1e-3, 1e-3, what=f"{config}: target")
+        assert np.all(want_t <= 0.0)
+        ws.dataset_free()
+        assert sim.device_errors() == 0
+
+
+def test_gate_discards_a_bad_warm_start():
+    """A network whose multipliers are 1000x the first plain ones wrecks the
+    warm pass; the FP64 residual gate must discard it and the step must end
+    where the plain solver's step ends."""
+    solver = {"adaptive": 1, "density_tolerance": 0.002, "max_iterations": 12}
+    with Simulation("small_dam", solver) as probe:
+        probe.step(5)
+        probe.apply_gravity()
+        probe.predict_positions()
+        probe.find_all_neighbors()
+        lam0 = probe.mlp_features()[:, 2]
+    params = np.zeros(ws.N_PARAMS, np.float32)
+    params[-1] = 1000.0 * float(lam0.min())
+    norm = np.concatenate([np.zeros(16), np.ones(16), [1.0]]).astype(np.float32)
+    with Simulation("small_dam", solver) as plain, Simulation("small_dam", solver) as warm:
+        plain.step(5)
+        warm.step(5)
+        warm.mlp_load(params, norm)
+        warm.set_solver(warm_start=1)
+        plain.step(1)
+        warm.step(1)
+        info = warm.last_step_info()
+        assert info["warm_start_used"] == 1 and info["warm_start_rejected"] == 1, info
+        p_info = plain.last_step_info()
+        assert info["iterations"] == p_info["iterations"] + 1
+        got, want = warm.fetch(), plain.fetch()
+        for f in ("x", "y", "z"):
+            assert_close(got[f], want[f], 1e-6, 0.0, atol=1e-6, what=f"gate:{f}")
+        for f in ("v_x", "v_y", "v_z"):
+            assert_close(got[f], want[f], 1e-5, 2e-5, what=f"gate:{f}")
+        assert warm.device_errors() == 0
