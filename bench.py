@@ -260,7 +260,8 @@ def run_ours(args, world, rank, local, dist):
         sim.set_stream(stream.cuda_stream)
         if warm:
             sim.mlp_load(net[0], net[1])
-            sim.set_solver(warm_start=1)
+            sim.set_solver(warm_start=1,
+                           warm_start_scale=float(net[2].get("warm_start_scale", 1.0)))
         log(f"[rank {rank}] {args.config}: {sim.n} particles, warm start {warm}, "
             f"init {time.perf_counter()-t_init:.1f}s")
         return sim

@@ -153,6 +153,10 @@ struct SphpcSolver {
   int lambda_epsilon_mass_units; /* 1: lambda_epsilon is added before the
                                     1/rho0^2 normalisation (particles.c:661),
                                     i.e. the effective value is eps/rho0^2 */
+  int warm_start_gate;        /* 1: discard a warm pass that does not lower the
+                                 FP64 max density error (default) */
+  int pad_warm;
+  double warm_start_scale;    /* multiplier on the network's Lambda (1) */
 };
 
 /* FP64 reductions over the local particles. */
@@ -174,6 +178,9 @@ struct SphpcStepInfo {
   int warm_start_rejected;    /* the residual gate discarded the warm pass */
   double max_density_error;   /* FP64, at the last density evaluation */
   double mean_density_error;
+  int trace_len;              /* density evaluations of the step (<= 16) */
+  int pad;
+  double trace[16];           /* FP64 max density error at each of them, in order */
 };
 
 /* Per-kernel device time collected with CUDA events (sphpc_profile). */

@@ -781,10 +781,11 @@ void oracle_step(const OracleParams *p, OracleState *s, OracleNeighbors *nb) {
  *   0 rho/rho0 - 1, 1 C = max(rho/rho0 - 1, 0), 2 lambda (particles.c:616-663),
  *   3 sum_q |grad_q C|^2 / rho0^2, 4 |sum_q grad_q C|^2 / rho0^2,
  *   5 neighbour count, 6-8 mean (x*_q - x*_p) / h,
- *   9-11 mean (v_q - v_p) dt / h, 12 SDF distance at x* / h clamped to
+ *   9-11 mean ((x* - x)_q - (x* - x)_p) / h (the mean relative velocity
+ *   times dt / h away from the box walls), 12 SDF distance at x* / h clamped to
  *   [-4, 4] (4 without an obstacle or outside its box), 13 nearest-neighbour
  *   distance / h (1 without neighbours), 14 distance to the nearest box wall
- *   / h clamped to [0, 4], 15 v along the gravity axis * dt / h. */
+ *   / h clamped to [0, 4], 15 (x* - x) along the gravity axis / h. */
 void oracle_features(const OracleParams *p, const OracleState *s,
                      const OracleNeighbors *nb, double *feat) {
   const double h = p->h, m = p->rest_mass, rho0 = p->rest_density;
@@ -807,9 +808,9 @@ void oracle_features(const OracleParams *p, const OracleState *s,
       sgx += gx; sgy += gy; sgz += gz;
       sC += gx * gx + gy * gy + gz * gz;
       o[0] -= dx; o[1] -= dy; o[2] -= dz;
-      u[0] += s->vx[q] - s->vx[i];
-      u[1] += s->vy[q] - s->vy[i];
-      u[2] += s->vz[q] - s->vz[i];
+      u[0] += (s->xs[q] - s->x[q]) - (s->xs[i] - s->x[i]);
+      u[1] += (s->ys[q] - s->y[q]) - (s->ys[i] - s->y[i]);
+      u[2] += (s->zs[q] - s->z[q]) - (s->zs[i] - s->z[i]);
       if (r2 < rmin2) rmin2 = r2;
     }
     const double C0 = rho / rho0 - 1.0;
@@ -839,17 +840,18 @@ void oracle_features(const OracleParams *p, const OracleState *s,
     wall /= h;
     if (wall < 0.0) wall = 0.0;
     if (wall > 4.0) wall = 4.0;
-    const double *vg = p->gravity_axis == 0 ? s->vx : (p->gravity_axis == 1 ? s->vy : s->vz);
+    const int ga = p->gravity_axis;
+    const double dg = ga == 0 ? xp - s->x[i] : (ga == 1 ? yp - s->y[i] : zp - s->z[i]);
     double *f = feat + (size_t)i * 16;
     f[0] = C0; f[1] = C; f[2] = lam; f[3] = s_pairs; f[4] = s_self; f[5] = cnt;
     for (int k = 0; k < 3; ++k) {
       f[6 + k] = o[k] * ic / h;
-      f[9 + k] = u[k] * ic * p->dt / h;
+      f[9 + k] = u[k] * ic / h;
     }
     f[12] = sdf;
     f[13] = sqrt(rmin2) / h;
     f[14] = wall;
-    f[15] = vg[i] * p->dt / h;
+    f[15] = dg / h;
   }
 }
 

@@ -75,7 +75,9 @@ class Solver(C.Structure):
                 ("jitter", C.c_double), ("seed", C.c_ulonglong),
                 ("rest_density_lattice", C.c_int), ("adaptive", C.c_int),
                 ("density_tolerance", C.c_double), ("max_iterations", C.c_int),
-                ("warm_start", C.c_int), ("lambda_epsilon_mass_units", C.c_int)]
+                ("warm_start", C.c_int), ("lambda_epsilon_mass_units", C.c_int),
+                ("warm_start_gate", C.c_int), ("pad_warm", C.c_int),
+                ("warm_start_scale", C.c_double)]
 
 
 class Diag(C.Structure):
@@ -95,7 +97,8 @@ class Diag(C.Structure):
 class StepInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int),
                 ("warm_start_used", C.c_int), ("warm_start_rejected", C.c_int),
-                ("max_density_error", C.c_double), ("mean_density_error", C.c_double)]
+                ("max_density_error", C.c_double), ("mean_density_error", C.c_double),
+                ("trace_len", C.c_int), ("pad", C.c_int), ("trace", C.c_double * 16)]
 
 
 class KernelTime(C.Structure):

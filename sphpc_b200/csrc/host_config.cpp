@@ -210,6 +210,9 @@ void sphpc_default_solver(struct SphpcSolver* s) {
   s->max_iterations = 32;
   s->warm_start = 0;
   s->lambda_epsilon_mass_units = 0;
+  s->warm_start_gate = 1;
+  s->pad_warm = 0;
+  s->warm_start_scale = 1.0;
 }
 
 void sphpc_set_default_solver(const struct SphpcSolver* s) {

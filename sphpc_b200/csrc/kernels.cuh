@@ -1,6 +1,7 @@
 // kernels.cuh -- host-side launch wrappers of the PBF pipeline kernels.
 #pragma once
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "radix_sort.cuh"
@@ -84,6 +85,10 @@ void launch_density_lambda(const DevParams& P, const NbrView& V, const PassArgs&
 // the warm-start network's 16 features of particles p < limit to feat[p][16].
 void launch_features(const DevParams& P, const NbrView& V, const PassArgs& a, float* feat,
                      int limit, cudaStream_t st);
+// The same pass writing the network's normalised BF16 input rows
+// bf16((f - norm[0:16]) * norm[16:32]) to xbf[p][16] for every particle.
+void launch_features_bf16(const DevParams& P, const NbrView& V, const PassArgs& a,
+                          __nv_bfloat16* xbf, const float* norm, cudaStream_t st);
 // target[p] += s * lambda_p (lambda in rec[p].d.w), p < limit.
 void launch_accum_lambda(const PD* rec, float s, float* target, int limit, cudaStream_t st);
 // Position pass: UpdateDPs (:668-746) with lambda from d.w; mode 0 fuses

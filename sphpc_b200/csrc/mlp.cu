@@ -164,11 +164,14 @@ __device__ __forceinline__ void write_row(MlpSmem& s, const float* h) {
   }
 }
 
+// BF16_IN: rows are already the normalised BF16 input (32 bytes each);
+// otherwise FP32 features normalised here.
+template <bool BF16_IN>
 __global__ void __launch_bounds__(kMlpTile)
     k_mlp_forward(const float* __restrict__ params, const float* __restrict__ norm,
-                  const __nv_bfloat16* __restrict__ wbf, const float* __restrict__ feat, int n,
+                  const __nv_bfloat16* __restrict__ wbf, const void* __restrict__ in, int n,
                   float* __restrict__ out, const PD* __restrict__ pd_in, PD* __restrict__ pd_out,
-                  uint32_t* __restrict__ err) {
+                  uint32_t* __restrict__ err, float extra_scale) {
   __shared__ MlpSmem s;
   const int t = threadIdx.x;
   load_weights(wbf, kMlpIn, s.w1);
@@ -185,7 +188,7 @@ __global__ void __launch_bounds__(kMlpTile)
     s.istd[t] = norm[kMlpIn + t];
   }
   const float b4 = params[kOffB4];
-  const float out_scale = norm[2 * kMlpIn];
+  const float out_scale = norm[2 * kMlpIn] * extra_scale;
   if (t < 32) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(
         tc::smem_u32(&s.taddr)));
@@ -205,7 +208,17 @@ __global__ void __launch_bounds__(kMlpTile)
   for (int tile = blockIdx.x; tile * kMlpTile < n; tile += gridDim.x) {
     const int p = tile * kMlpTile + t;
     // input layer operand: normalised features, K = 16
-    {
+    if (BF16_IN) {
+      uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
+      if (p < n) {
+        const uint4* xr = reinterpret_cast<const uint4*>(in) + (size_t)p * 2;
+        lo = __ldg(xr);
+        hi = __ldg(xr + 1);
+      }
+      *reinterpret_cast<uint4*>(s.act + tc::core_off(t, 0, kMlpIn / 8)) = lo;
+      *reinterpret_cast<uint4*>(s.act + tc::core_off(t, 8, kMlpIn / 8)) = hi;
+    } else {
+      const float* feat = reinterpret_cast<const float*>(in);
       float f[kMlpIn];
       if (p < n) {
         const float4* fp = reinterpret_cast<const float4*>(feat + (size_t)p * kMlpIn);
@@ -746,12 +759,23 @@ void mlp_release(MlpState& m) {
 }
 
 void launch_mlp_forward(const MlpDevice& d, const float* feat, int n, float* out,
-                        const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st) {
+                        const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
+                        float extra_scale) {
   if (n <= 0) return;
   const int tiles = (n + kMlpTile - 1) / kMlpTile;
   const int grid = tiles < 148 * 4 ? tiles : 148 * 4;
-  k_mlp_forward<<<grid, kMlpTile, 0, st>>>(d.params, d.norm, d.wbf, feat, n, out, pd_in, pd_out,
-                                           err);
+  k_mlp_forward<false><<<grid, kMlpTile, 0, st>>>(d.params, d.norm, d.wbf, feat, n, out, pd_in,
+                                                  pd_out, err, extra_scale);
+}
+
+void launch_mlp_forward_bf16(const MlpDevice& d, const __nv_bfloat16* xbf, int n,
+                             const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
+                             float extra_scale) {
+  if (n <= 0) return;
+  const int tiles = (n + kMlpTile - 1) / kMlpTile;
+  const int grid = tiles < 148 * 4 ? tiles : 148 * 4;
+  k_mlp_forward<true><<<grid, kMlpTile, 0, st>>>(d.params, d.norm, d.wbf, xbf, n, nullptr, pd_in,
+                                                 pd_out, err, extra_scale);
 }
 
 // ---- device-resident training set (one per process, on the device that

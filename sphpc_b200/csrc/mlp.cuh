@@ -60,7 +60,13 @@ void mlp_free(MlpDevice& d);
 // pd_in/pd_out are given, records pd_out[p] = {x, (d, min(lambda0, 0))} from
 // pd_in (the plain solver's multipliers are never positive).
 void launch_mlp_forward(const MlpDevice& d, const float* feat, int n, float* out,
-                        const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st);
+                        const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
+                        float extra_scale = 1.0f);
+
+// The same from rows already normalised to BF16 (xbf[n][16]) into records.
+void launch_mlp_forward_bf16(const MlpDevice& d, const __nv_bfloat16* xbf, int n,
+                             const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
+                             float extra_scale = 1.0f);
 
 // Reserves `want` rows of the process's training set (fewer when it is
 // nearly full: *got) and returns their feature and target pointers.

@@ -118,25 +118,27 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // The first density/lambda pass of a step (mode 0, with residual) that also
-// writes the 16 warm-start features of each particle p < limit to
-// feat[p][16]:
+// forms the 16 warm-start features of each particle p < limit:
 //   0 rho/rho0 - 1       1 C = max(rho/rho0 - 1, 0)     2 lambda
 //   3 sum_q |grad_q C|^2 4 |grad_p C|^2 (both with the 1/rho0^2 of lambda)
-//   5 neighbour count    6-8 mean neighbour offset (x_q - x_p) / h
-//   9-11 mean relative velocity (v_q - v_p) dt / h
+//   5 neighbour count    6-8 mean neighbour offset (x*_q - x*_p) / h
+//   9-11 mean relative predicted displacement (d_q - d_p) / h, d = x* - x
+//        (= the mean relative velocity * dt / h away from the box walls)
 //   12 SDF distance at x* / h, clamped to [-4, 4] (4 without an obstacle)
 //   13 nearest-neighbour distance / h (1 without neighbours)
 //   14 distance to the nearest box wall / h, clamped to [0, 4]
-//   15 velocity along the gravity axis * dt / h
+//   15 own predicted displacement along the gravity axis / h
+// RAW: FP32 features to feat[p][16]; otherwise the network's input row
+// bf16((f - mean) * inv_std) (norm = mean[16], inv_std[16]) to xbf[p][16].
+template <bool RAW>
 __global__ void __launch_bounds__(kBlock)
     k_features(const DevParams P, const NbrView V, const PassArgs a, float* __restrict__ feat,
-               int limit) {
+               __nv_bfloat16* __restrict__ xbf, const float* __restrict__ norm, int limit) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   double err = 0.0;
   if (p < P.n) {
     float4 xp, dp;
     ld_pd(a.pd, p, xp, dp);
-    const float4 vp = a.vel[p];
     float rho = P.W0m, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
     float ox = 0.f, oy = 0.f, oz = 0.f, ux = 0.f, uy = 0.f, uz = 0.f, rmin2 = P.h2;
@@ -160,27 +162,28 @@ __global__ void __launch_bounds__(kBlock)
       sgy += gy;
       sgz += gz;
       sC += gx * gx + gy * gy + gz * gz;
-      const float4 vq = __ldg(a.vel + q);
       ox -= g.dx;
       oy -= g.dy;
       oz -= g.dz;
-      ux += vq.x - vp.x;
-      uy += vq.y - vp.y;
-      uz += vq.z - vp.z;
+      ux += dq.x - dp.x;
+      uy += dq.y - dp.y;
+      uz += dq.z - dp.z;
       rmin2 = fminf(rmin2, g.r2);
       ++cnt;
     });
     a.rho[p] = rho;
     const float C = (float)fmax(__ddiv_rn((double)rho, P.rho0_d) - 1.0, 0.0);
     const float s_pairs = sC * P.inv_rho0_sq;
-    const float s_self = (sgx * sgx + sgy * sgy + sgz * sgz) * P.inv_rho0_sq;
-    const float lam = -C / ((sC + sgx * sgx + sgy * sgy + sgz * sgz) * P.inv_rho0_sq + P.lambda_eps);
+    sC += sgx * sgx + sgy * sgy + sgz * sgz;
+    sC *= P.inv_rho0_sq;
+    const float lam = -C / (sC + P.lambda_eps);
     st_pd(a.pd_out, p, xp, make_float4(dp.x, dp.y, dp.z, lam));
     err = fmax((double)rho / (double)P.rho0 - 1.0, 0.0);
     if (p < limit) {
       const float inv_h = 1.0f / P.h;
+      const float s_self = (sgx * sgx + sgy * sgy + sgz * sgz) * P.inv_rho0_sq;
       const float inv_cnt = cnt > 0 ? 1.0f / (float)cnt : 0.0f;
-      const float vs = P.dt * inv_h * inv_cnt;
+      const float sc = inv_h * inv_cnt;
       const double xs = xstar_d(xp.x, dp.x), ys = xstar_d(xp.y, dp.y), zs = xstar_d(xp.z, dp.z);
       float sdf = 4.0f;
       if (P.has_sdf && xs > P.ob_min[0] && xs < P.ob_max[0] && ys > P.ob_min[1] &&
@@ -190,15 +193,32 @@ __global__ void __launch_bounds__(kBlock)
         const float zt = (float)((zs - P.ob_min[2]) / (double)P.ob_len[2]);
         sdf = fminf(fmaxf(sdf_sample(P, xt, yt, zt) * P.model_to_world * inv_h, -4.0f), 4.0f);
       }
-      double wall = fmin(fmin(xs - P.bmin[0], P.bmax[0] - xs),
-                         fmin(fmin(ys - P.bmin[1], P.bmax[1] - ys), fmin(zs - P.bmin[2], P.bmax[2] - zs)));
+      const double wall =
+          fmin(fmin(xs - P.bmin[0], P.bmax[0] - xs),
+               fmin(fmin(ys - P.bmin[1], P.bmax[1] - ys), fmin(zs - P.bmin[2], P.bmax[2] - zs)));
       const float fw = fminf(fmaxf((float)(wall / P.hd), 0.0f), 4.0f);
-      const float vg = (P.gaxis == 0 ? vp.x : (P.gaxis == 1 ? vp.y : vp.z)) * P.dt * inv_h;
-      float4* out = reinterpret_cast<float4*>(feat + (size_t)p * 16);
-      out[0] = make_float4(rho * P.inv_rho0 - 1.0f, C, lam, s_pairs);
-      out[1] = make_float4(s_self, (float)cnt, ox * inv_h * inv_cnt, oy * inv_h * inv_cnt);
-      out[2] = make_float4(oz * inv_h * inv_cnt, ux * vs, uy * vs, uz * vs);
-      out[3] = make_float4(sdf, sqrtf(rmin2) * inv_h, fw, vg);
+      const float vg = (P.gaxis == 0 ? dp.x : (P.gaxis == 1 ? dp.y : dp.z)) * inv_h;
+      const float f[16] = {rho * P.inv_rho0 - 1.0f, C, lam, s_pairs, s_self, (float)cnt,
+                           ox * sc, oy * sc, oz * sc, ux * sc, uy * sc, uz * sc,
+                           sdf, sqrtf(rmin2) * inv_h, fw, vg};
+      if (RAW) {
+        float4* out = reinterpret_cast<float4*>(feat + (size_t)p * 16);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          out[k] = make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]);
+      } else {
+        uint32_t w[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float lo = (f[2 * k] - __ldg(norm + 2 * k)) * __ldg(norm + 16 + 2 * k);
+          const float hi = (f[2 * k + 1] - __ldg(norm + 2 * k + 1)) * __ldg(norm + 17 + 2 * k);
+          const __nv_bfloat162 b2 = __floats2bfloat162_rn(lo, hi);
+          w[k] = *reinterpret_cast<const uint32_t*>(&b2);
+        }
+        uint4* out = reinterpret_cast<uint4*>(xbf + (size_t)p * 16);
+        out[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        out[1] = make_uint4(w[4], w[5], w[6], w[7]);
+      }
     }
   }
   block_resid(err, a.resid);
@@ -555,7 +575,12 @@ void launch_density_lambda(const DevParams& P, const NbrView& V, const PassArgs&
 
 void launch_features(const DevParams& P, const NbrView& V, const PassArgs& a, float* feat,
                      int limit, cudaStream_t st) {
-  k_features<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a, feat, limit);
+  k_features<true><<<grid_for(P.n), kBlock, 0, st>>>(P, V, a, feat, nullptr, nullptr, limit);
+}
+
+void launch_features_bf16(const DevParams& P, const NbrView& V, const PassArgs& a,
+                          __nv_bfloat16* xbf, const float* norm, cudaStream_t st) {
+  k_features<false><<<grid_for(P.n), kBlock, 0, st>>>(P, V, a, nullptr, xbf, norm, P.n);
 }
 
 void launch_accum_lambda(const PD* rec, float s, float* target, int limit, cudaStream_t st) {

@@ -88,6 +88,7 @@ class DeviceSim {
   MlpState mlp{};
   PD* pd_w = nullptr;            // third record buffer of the warm start
   int last_warm_rejected = 0;
+  std::vector<double> trace;     // max density error at each evaluation of the step
   // training-set collection of the current step (collect_iters > 0)
   int collect_iters = 0;
   long long collect_rows = 0;
@@ -470,6 +471,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   const double tol = solver.density_tolerance;
   last_warm = 0.0;
   last_warm_rejected = 0;
+  trace.clear();
   // The current positions are always the records in `pd`.  A density/lambda
   // pass (A) reads pd and writes records with lambda in d.w; a position pass
   // (B) reads such records and writes the new positions into pd.
@@ -489,6 +491,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     SPHPC_CK(cudaStreamSynchronize(stream));
     last_max_err = max_err = h_res[0];
     last_mean_err = h_res[1] / (n > 0 ? n : 1);
+    if (trace.size() < 16) trace.push_back(max_err);
     return SPHPC_OK;
   };
   auto pass_b = [&](const PD* in, float stiffness, bool last) {
@@ -522,7 +525,8 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
       a.pd = pd;
       a.pd_out = pd_alt;
-      launch_features(P, V, a, mlp.feat, n, stream);
+      launch_features_bf16(P, V, a, reinterpret_cast<__nv_bfloat16*>(mlp.feat), mlp.dev.norm,
+                           stream);
       launches += 1;
     }
     SPHPC_RC(read_resid(err0));
@@ -531,7 +535,8 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     } else {
       {
         Scope sc(this, "mlp_forward");
-        launch_mlp_forward(mlp.dev, mlp.feat, n, nullptr, pd_alt, pd_w, err(), stream);
+        launch_mlp_forward_bf16(mlp.dev, reinterpret_cast<const __nv_bfloat16*>(mlp.feat), n,
+                                pd_alt, pd_w, err(), stream, (float)solver.warm_start_scale);
         launches += 1;
       }
       // the network's multipliers, applied at full stiffness in one pass
@@ -542,7 +547,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       SPHPC_RC(read_resid(err1));
       if (adaptive && err1 <= tol) {
         converged = true;
-      } else if (!(err1 < err0)) {
+      } else if (solver.warm_start_gate && !(err1 < err0)) {
         // FP64 residual gate: the warm pass did not lower the maximum density
         // error, so it is discarded and the plain solve restarts from the
         // predicted positions (pd_alt still holds them with lambda_0)
@@ -1310,6 +1315,8 @@ int sphpc_step_info(const struct Particles* particles, struct SphpcStepInfo* inf
   info->warm_start_rejected = s->last_warm_rejected;
   info->max_density_error = s->last_max_err;
   info->mean_density_error = s->last_mean_err;
+  info->trace_len = (int)s->trace.size();
+  for (size_t k = 0; k < s->trace.size() && k < 16; ++k) info->trace[k] = s->trace[k];
   return SPHPC_OK;
 }
 

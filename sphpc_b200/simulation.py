@@ -138,7 +138,8 @@ class Simulation:
                 "warm_start_used": i.warm_start_used,
                 "warm_start_rejected": i.warm_start_rejected,
                 "max_density_error": i.max_density_error,
-                "mean_density_error": i.mean_density_error}
+                "mean_density_error": i.mean_density_error,
+                "trace": list(i.trace[:i.trace_len])}
 
     def device_errors(self) -> int:
         bits = C.c_uint(0)

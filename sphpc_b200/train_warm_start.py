@@ -6,13 +6,16 @@ network on the device.
 Training rows come from the plain PBF solve of two scenes, each with eight
 jitter seeds (1-8): the 1,048,576-particle dam break (dam_break_1m) and the
 4,194,304-particle obstacle scene with surface tension (obstacle_4m).  Every
-scene runs `--steps` steps with the adaptive plain solver (max density error
-<= 1%); every `--every` steps one step is taken by sphpc_mlp_collect, which
-solves with `--iterations` fixed plain substeps and appends one row per
-particle: the 16 features of the predicted state and the target
+scene runs with the adaptive plain solver (max density error <= 1%); the
+steps listed in `--collect-at` (early-heavy: the first steps of a dam break
+are the most compressed) are taken by sphpc_mlp_collect instead, which solves
+with `--iterations` fixed plain substeps and appends one row per particle:
+the 16 features of the predicted state and the target
 Lambda = sum_k s_k lambda_k.  The network is then trained with AdamW (lr 1e-3,
 batch 65,536) by the library's tensor-core kernels, and evaluated on a
-collected step of a seed that was not trained on (seed 9).  The network file
+collected step of a seed that was not trained on (seed 9); runs of that seed
+also choose the multiplier applied to the network's Lambda (0.5, 0.75 or 1:
+the fewest mean iterations), stored with the network.  The network file
 and a JSON log (loss curve, data sizes, held-out fit) are written.
 """
 from __future__ import annotations
@@ -30,13 +33,13 @@ from .simulation import Simulation
 SCENES = ("dam_break_1m", "obstacle_4m")
 
 
-def collect_scene(config, seed, steps, every, iterations, tol, log):
+def collect_scene(config, seed, collect_at, iterations, tol, log):
     solver = {"adaptive": 1, "density_tolerance": tol, "max_iterations": 12, "seed": seed}
     rows = 0
     t0 = time.perf_counter()
     with Simulation(config, solver) as sim:
-        for k in range(steps):
-            if k % every == every // 2:
+        for k in range(max(collect_at) + 1):
+            if k in collect_at:
                 rows += ws.collect(sim, iterations)
             else:
                 sim.step(1)
@@ -46,13 +49,13 @@ def collect_scene(config, seed, steps, every, iterations, tol, log):
     return rows
 
 
-def held_out_fit(params, norm, config, seed, steps, every, iterations, tol):
+def held_out_fit(params, norm, config, seed, collect_at, iterations, tol):
     """R^2 and relative RMS error of the network on rows of an unseen seed."""
     import ctypes as C
     import torch
     from ._lib import call
     ws.dataset_clear()
-    collect_scene(config, seed, steps, every, iterations, tol, lambda *a: None)
+    collect_scene(config, seed, collect_at, iterations, tol, lambda *a: None)
     n = ws.dataset_size()
     feat, target = ws.dataset_read(0, n)
     d_feat = torch.from_numpy(feat).cuda()
@@ -76,20 +79,54 @@ def held_out_fit(params, norm, config, seed, steps, every, iterations, tol):
             "baseline_scale": a}
 
 
+def iterations_with(params, norm, config, seed, scale, pre, steps, tol):
+    """Mean constraint iterations per step over `steps` steps after `pre`
+    plain steps; scale None = the plain solver."""
+    solver = {"adaptive": 1, "density_tolerance": tol, "max_iterations": 12, "seed": seed}
+    with Simulation(config, solver) as sim:
+        sim.step(pre)
+        if scale is not None:
+            sim.mlp_load(params, norm)
+            sim.set_solver(warm_start=1, warm_start_scale=scale)
+        its = []
+        for _ in range(steps):
+            sim.step(1)
+            its.append(sim.last_step_info()["iterations"])
+    return float(np.mean(its))
+
+
+def choose_scale(params, norm, scenes, seed, tol, scales=(0.5, 0.75, 1.0),
+                 cases=((3, 8), (150, 8))):
+    """The multiplier on the network's Lambda with the fewest iterations on
+    held-out runs (seed not trained on), early and later in each scene."""
+    table = {}
+    for sc in (None,) + tuple(scales):
+        tot = 0.0
+        for config in scenes:
+            for pre, steps in cases:
+                it = iterations_with(params, norm, config, seed, sc, pre, steps, tol)
+                table[f"{config}@{pre} {'plain' if sc is None else f'x{sc}'}"] = it
+                tot += it
+        table[f"total {'plain' if sc is None else f'x{sc}'}"] = tot
+    best = min(scales, key=lambda s: table[f"total x{s}"])
+    return best, table
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--out", default=ws.DEFAULT_WEIGHTS)
     ap.add_argument("--log", default=None, help="JSON log (default: next to --out)")
     ap.add_argument("--seeds", type=int, default=8)
-    ap.add_argument("--steps", type=int, default=500)
-    ap.add_argument("--every", type=int, default=100)
-    ap.add_argument("--iterations", type=int, default=6)
+    ap.add_argument("--collect-at", default="3,10,40,150,400",
+                    help="steps of each scene taken by the collecting solve")
+    ap.add_argument("--iterations", type=int, default=2)
     ap.add_argument("--tol", type=float, default=0.01)
     ap.add_argument("--epochs", type=float, default=3.0)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--weight-decay", type=float, default=1e-4)
     ap.add_argument("--capacity", type=int, default=230_000_000)
+    ap.add_argument("--no-held-out", action="store_true")
     ap.add_argument("--scenes", default=",".join(SCENES))
     args = ap.parse_args(argv)
     logf = args.log or os.path.splitext(args.out)[0] + "_log.json"
@@ -100,14 +137,15 @@ def main(argv=None):
         lines.append(msg)
 
     scenes = args.scenes.split(",")
+    collect_at = sorted({int(x) for x in args.collect_at.split(",")})
     t0 = time.perf_counter()
     ws.dataset_reserve(args.capacity)
     ws.dataset_clear()
-    log(f"collecting: scenes {scenes}, seeds 1-{args.seeds}, {args.steps} steps, "
-        f"one collected step every {args.every}, {args.iterations} plain substeps")
+    log(f"collecting: scenes {scenes}, seeds 1-{args.seeds}, collected steps {collect_at}, "
+        f"{args.iterations} plain substeps")
     for config in scenes:
         for seed in range(1, args.seeds + 1):
-            collect_scene(config, seed, args.steps, args.every, args.iterations, args.tol, log)
+            collect_scene(config, seed, collect_at, args.iterations, args.tol, log)
     n = ws.dataset_size()
     t_collect = time.perf_counter() - t0
     norm = ws.dataset_stats()
@@ -123,15 +161,22 @@ def main(argv=None):
         f"{loss[-100:].mean():.4g}")
     if not np.all(np.isfinite(params)):
         raise SystemExit("training diverged (non-finite parameters)")
-    fit = [held_out_fit(params, norm, c, args.seeds + 1, args.steps, args.every,
-                        args.iterations, args.tol) for c in scenes]
+    fit = [] if args.no_held_out else [
+        held_out_fit(params, norm, c, args.seeds + 1, collect_at, args.iterations, args.tol)
+        for c in scenes]
     for f in fit:
         log(f"held-out {f['config']} seed {f['seed']}: R^2 {f['r2']:.4f} (scaled lambda_0: "
             f"{f['baseline_scaled_lambda0_r2']:.4f}), relative RMS {f['rel_rms']:.4f}")
+    scale, table = (1.0, {}) if args.no_held_out else choose_scale(
+        params, norm, scenes, args.seeds + 1, args.tol)
+    for k, v in table.items():
+        log(f"held-out mean iterations {k}: {v:.2f}")
+    log(f"warm-start scale {scale}")
     meta = {"features": list(ws.FEATURES), "rows": int(n), "steps": steps,
+            "warm_start_scale": scale,
             "batch": args.batch, "lr": args.lr, "weight_decay": args.weight_decay,
             "scenes": scenes, "seeds": list(range(1, args.seeds + 1)),
-            "collect_every": args.every, "sim_steps": args.steps,
+            "collected_steps": collect_at,
             "target": f"sum_k s_k lambda_k over {args.iterations} plain substeps"}
     ws.save_network(args.out, params, norm, meta)
     every = max(1, steps // 200)
@@ -139,7 +184,8 @@ def main(argv=None):
         json.dump({"meta": meta, "collect_seconds": t_collect, "train_seconds": t_train,
                    "rows_per_second": steps * args.batch / t_train,
                    "loss_every": every, "loss": [float(x) for x in loss[::every]],
-                   "held_out": fit, "log": lines}, fh, indent=1)
+                   "held_out": fit, "held_out_iterations": table, "log": lines}, fh,
+                  indent=1)
     ws.dataset_free()
     log(f"wrote {args.out} and {logf}")
 

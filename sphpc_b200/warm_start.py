@@ -30,8 +30,9 @@ DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "warm_start.npz")
 FEATURES = (
     "rho/rho0 - 1", "C", "lambda", "sum |grad_q C|^2", "|grad_p C|^2", "neighbour count",
     "mean offset x / h", "mean offset y / h", "mean offset z / h",
-    "mean rel. velocity x dt / h", "mean rel. velocity y dt / h", "mean rel. velocity z dt / h",
-    "SDF / h", "nearest neighbour / h", "wall distance / h", "v_gravity dt / h",
+    "mean rel. displacement x / h", "mean rel. displacement y / h",
+    "mean rel. displacement z / h", "SDF / h", "nearest neighbour / h", "wall distance / h",
+    "own displacement along gravity / h",
 )
 
 _F = C.POINTER(C.c_float)

@@ -99,3 +99,29 @@ def test_gate_discards_a_bad_warm_start():
         for f in ("v_x", "v_y", "v_z"):
             assert_close(got[f], want[f], 1e-5, 2e-5, what=f"gate:{f}")
         assert warm.device_errors() == 0
+
+
+def test_trained_network_reduces_iterations():
+    """The committed network against the plain solver from the same state:
+    early steps of the 4,194,304-particle obstacle scene, at the scene's
+    tolerance (max density error <= 1%), both arms converging every step."""
+    params, norm, meta = ws.load_network()
+    solver = {"adaptive": 1, "density_tolerance": 0.01, "max_iterations": 12}
+    res = {}
+    for arm in ("plain", "warm"):
+        with Simulation("obstacle_4m", solver) as sim:
+            sim.step(3)
+            if arm == "warm":
+                sim.mlp_load(params, norm)
+                sim.set_solver(warm_start=1, warm_start_scale=meta.get("warm_start_scale", 1.0))
+            its, conv = [], 0
+            for _ in range(8):
+                sim.step(1)
+                d = sim.last_step_info()
+                its.append(d["iterations"])
+                conv += d["converged"]
+            assert conv == 8, (arm, its)
+            assert sim.device_errors() == 0
+            res[arm] = float(np.mean(its))
+    print(res)
+    assert res["warm"] <= 0.85 * res["plain"], res
