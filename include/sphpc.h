@@ -203,12 +203,13 @@ int sphpc_mlp_dataset_stats(float *norm);
 
 /* AdamW (beta 0.9/0.999, eps 1e-8, decoupled weight decay on weights only)
  * on the training set: `steps` steps of `batch` rows, each pass over the set
- * in a fresh seeded permutation; params_out[9473] and loss_out[steps] (batch
- * loss before each update, may be NULL) on the host.  No counterpart in the
+ * in a fresh seeded permutation, learning rate from lr to lr_final on a half
+ * cosine (equal: constant); params_out[9473] and loss_out[steps] (batch loss
+ * before each update, may be NULL) on the host.  No counterpart in the
  * reference. */
 int sphpc_mlp_train(const float *params_in, const float *norm, int steps, int batch, float lr,
-                    float weight_decay, unsigned long long seed, float *params_out,
-                    float *loss_out);
+                    float lr_final, float weight_decay, unsigned long long seed,
+                    float *params_out, float *loss_out);
 
 /* One time step like sphpc_step with the plain solver at a fixed
  * `iterations`, appending one training row per particle (as many as fit):

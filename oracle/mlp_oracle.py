@@ -5,10 +5,10 @@ of the PBF constraint solve whose plain iteration is particles.c:588-746
 (ComputeLambda / UpdateDPs).  This file restates, in numpy, what the CUDA
 kernels in sphpc_b200/csrc/mlp.cu compute, so that tests can check them:
 
-  x0 = bf16((f - mean) * inv_std)                      16 features
-  z1 = x0 . bf16(W1)^T + b1,   h1 = bf16(gelu(z1))     64
-  z2 = h1 . bf16(W2)^T + b2,   h2 = bf16(gelu(z2))     64
-  z3 = h2 . bf16(W3)^T + b3,   h3 = gelu(z3)           64 (FP32)
+  x0 = bf16((f - mean) * inv_std)                          16 features
+  z1 = x0 . bf16(W1)^T + bf16(b1),  h1 = bf16(gelu(z1))    64
+  z2 = h1 . bf16(W2)^T + bf16(b2),  h2 = bf16(gelu(z2))    64
+  z3 = h2 . bf16(W3)^T + bf16(b3),  h3 = gelu(z3)          64 (FP32)
   u  = w4 . h3 + b4,           lambda0 = out_scale * u
 
 gelu is the tanh form 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))).
@@ -100,6 +100,10 @@ def forward(params, norm, feat, bf16_emulation=True):
         W = [q["W1"].astype(np.float64), q["W2"].astype(np.float64), q["W3"].astype(np.float64)]
         rnd = lambda a: a
     b = [q["b1"].astype(np.float64), q["b2"].astype(np.float64), q["b3"].astype(np.float64)]
+    if bf16_emulation:
+        # the kernels carry each hidden bias through the MMA as a BF16 weight
+        # against a constant-one input column
+        b = [bf16(v.astype(np.float32)).astype(np.float64) for v in b]
     hs = [x0]
     zs = []
     h = x0

@@ -179,7 +179,8 @@ SIGNATURES = {
     "sphpc_mlp_dataset_append": ([C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_longlong], C.c_int),
     "sphpc_mlp_dataset_read": ([C.c_longlong, C.c_longlong, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
     "sphpc_mlp_dataset_stats": ([C.POINTER(C.c_float)], C.c_int),
-    "sphpc_mlp_train": ([C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_float, C.c_float, C.c_ulonglong,
+    "sphpc_mlp_train": ([C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int,
+                         C.c_float, C.c_float, C.c_float, C.c_ulonglong,
                          C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
     "SortByKey": ([U, U, C.c_int, C.c_void_p], C.c_int),
     "SortByKeyNoAlloc": ([U, U, C.c_int, C.c_void_p], C.c_int),

@@ -99,94 +99,123 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 
 }  // namespace tc
 
-// GELU, tanh form (Hendrycks & Gimpel 2016): 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).
-__device__ __forceinline__ float gelu_tanh(float x) {
-  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+// GELU, tanh form (Hendrycks & Gimpel 2016):
+// 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), with the tanh argument
+// written x (c + c a x^2) and the result hx + hx t, hx = x / 2.
+constexpr float kGeluC = 0.7978845608028654f;
+constexpr float kGeluCA = 0.7978845608028654f * 0.044715f;
+
+__device__ __forceinline__ float tanh_approx(float u) {
   float t;
   asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-  return 0.5f * x * (1.0f + t);
+  return t;
+}
+
+__device__ __forceinline__ float gelu_tanh(float x) {
+  const float t = tanh_approx(x * fmaf(kGeluCA, x * x, kGeluC));
+  const float hx = 0.5f * x;
+  return fmaf(hx, t, hx);
 }
 
 namespace {
 
 constexpr uint32_t kErrMlpWait = 1u << 4;
 
+// Shared-memory operand widths (in 8-element core-matrix columns): the input
+// rows hold 16 features, a ones column (16) and zeros up to 32; hidden rows
+// 64 activations, a ones column (64) and zeros up to 80.  The weight rows
+// match: W | bias | 0, so every bias rides in the MMA (as a BF16 value).
+constexpr int kKcX = 4, kKcH = 10, kKcD = 16;
+constexpr int kKX = kKcX * 8, kKH = kKcH * 8;
+
+// Weight rows [64][kc*8] = W[j][0..K) | bf16(b[j]) | 0 in the core layout.
+__device__ void load_weights_ext(const __nv_bfloat16* __restrict__ w,
+                                 const float* __restrict__ bias, int K, int kc, uint8_t* dst) {
+  const int width = kc * 8;
+  for (int i = threadIdx.x; i < kMlpHidden * width; i += blockDim.x) {
+    const int r = i / width, k = i % width;
+    __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
+    if (k < K) v = w[r * K + k];
+    else if (k == K) v = __float2bfloat16_rn(bias[r]);
+    *reinterpret_cast<__nv_bfloat16*>(dst + tc::core_off(r, k, kc)) = v;
+  }
+}
+
+// 8 consecutive values of row r starting at column k0 (multiple of 8), BF16.
+__device__ __forceinline__ void put8(uint8_t* buf, int kc, int r, int k0, const float* v) {
+  uint32_t w[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    w[i] = *reinterpret_cast<const uint32_t*>(&b2);
+  }
+  *reinterpret_cast<uint4*>(buf + tc::core_off(r, k0, kc)) = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+__device__ __forceinline__ void put8_const(uint8_t* buf, int kc, int r, int k0, float first) {
+  float v[8] = {first, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  put8(buf, kc, r, k0, v);
+}
+
+// 64 FP32 columns starting at TMEM column `col` of this thread's lane.
+__device__ __forceinline__ void tmem_row64(uint32_t lane_base, uint32_t col, float* v) {
+#pragma unroll
+  for (int c = 0; c < 64; c += 16) tc::tmem_ld16(lane_base + col + c, v + c);
+  tc::tmem_wait_ld();
+}
+
+// K-major A [128 x K] x K-major B [N x K]^T, K in steps of 16.
+__device__ __forceinline__ void mma_kk(uint32_t d, uint32_t a, int kca, uint32_t b, int kcb, int K,
+                                       uint32_t idesc) {
+  for (int st = 0; st < K / 16; ++st)
+    tc::mma_bf16(d, tc::smem_desc(a + st * 256, 128, kca * 128),
+                 tc::smem_desc(b + st * 256, 128, kcb * 128), idesc, st > 0);
+}
+
 struct MlpSmem {
-  alignas(128) uint8_t w1[kMlpHidden * kMlpIn * 2];
-  alignas(128) uint8_t w2[kMlpHidden * kMlpHidden * 2];
-  alignas(128) uint8_t w3[kMlpHidden * kMlpHidden * 2];
-  alignas(128) uint8_t act[kMlpTile * kMlpHidden * 2];
-  float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpHidden], w4[kMlpHidden];
+  alignas(128) uint8_t w1[kMlpHidden * kKcX * 16];
+  alignas(128) uint8_t w2[kMlpHidden * kKcH * 16];
+  alignas(128) uint8_t w3[kMlpHidden * kKcH * 16];
+  alignas(128) uint8_t x0[kMlpTile * kKcX * 16];
+  alignas(128) uint8_t h[kMlpTile * kKcH * 16];
+  alignas(16) float w4[kMlpHidden];
   float mean[kMlpIn], istd[kMlpIn];
   alignas(8) uint64_t mbar;
   uint32_t taddr;
 };
 
-// Copies a row-major BF16 [64][K] matrix into its core-matrix layout.
-__device__ void load_weights(const __nv_bfloat16* __restrict__ w, int K, uint8_t* dst) {
-  const int kc = K / 8;
-  for (int i = threadIdx.x; i < kMlpHidden * K; i += blockDim.x) {
-    const int r = i / K, k = i % K;
-    *reinterpret_cast<__nv_bfloat16*>(dst + tc::core_off(r, k, kc)) = w[i];
-  }
-}
+size_t fwd_smem_bytes() { return sizeof(MlpSmem) + 128; }
 
-// One layer on the tensor cores: TMEM[128 x 64] = act[128 x K] * W[64 x K]^T.
-__device__ __forceinline__ void issue_layer(MlpSmem& s, const uint8_t* w, int K, uint32_t taddr) {
-  const int kc = K / 8;
-  const uint32_t a0 = tc::smem_u32(s.act), b0 = tc::smem_u32(w);
-  for (int step = 0; step < K / 16; ++step) {
-    const uint64_t da = tc::smem_desc(a0 + step * 256, 128, kc * 128);
-    const uint64_t db = tc::smem_desc(b0 + step * 256, 128, kc * 128);
-    tc::mma_bf16(taddr, da, db, tc::kIdescM128N64, step > 0);
-  }
-  tc::commit(&s.mbar);
-}
-
-// Row t of D (64 columns) for this thread's lane.
-__device__ __forceinline__ void read_row(uint32_t taddr, float* v) {
-  const uint32_t lane_base = taddr + ((uint32_t)((threadIdx.x >> 5) * 32) << 16);
-#pragma unroll
-  for (int c = 0; c < kMlpHidden; c += 16) tc::tmem_ld16(lane_base + c, v + c);
-  tc::tmem_wait_ld();
-}
-
-// Row t of the next layer's A (K = 64), BF16.
-__device__ __forceinline__ void write_row(MlpSmem& s, const float* h) {
-  const int r = threadIdx.x;
-#pragma unroll
-  for (int k0 = 0; k0 < kMlpHidden; k0 += 8) {
-    __align__(16) __nv_bfloat16 pk[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) pk[i] = __float2bfloat16_rn(h[k0 + i]);
-    *reinterpret_cast<uint4*>(s.act + tc::core_off(r, k0, kMlpHidden / 8)) =
-        *reinterpret_cast<const uint4*>(pk);
-  }
-}
-
-// BF16_IN: rows are already the normalised BF16 input (32 bytes each);
-// otherwise FP32 features normalised here.
+// One CTA of 128 threads per tile of 128 rows, tiles strided over the grid;
+// thread t owns row t.  Per tile: input row to x0, then three layers, each
+// one tcgen05.mma group into tensor memory (64 FP32 columns) followed by the
+// row's GELU epilogue; the last layer's FP32 activations meet w4 on the
+// CUDA cores.  BF16_IN: the rows are already the normalised BF16 input (32
+// bytes each); otherwise FP32 features normalised here.
 template <bool BF16_IN>
 __global__ void __launch_bounds__(kMlpTile)
     k_mlp_forward(const float* __restrict__ params, const float* __restrict__ norm,
                   const __nv_bfloat16* __restrict__ wbf, const void* __restrict__ in, int n,
                   float* __restrict__ out, const PD* __restrict__ pd_in, PD* __restrict__ pd_out,
                   uint32_t* __restrict__ err, float extra_scale) {
-  __shared__ MlpSmem s;
+  extern __shared__ __align__(128) uint8_t fwd_raw[];
+  const uint32_t mis = tc::smem_u32(fwd_raw) & 127u;
+  MlpSmem& s = *reinterpret_cast<MlpSmem*>(fwd_raw + ((128u - mis) & 127u));
   const int t = threadIdx.x;
-  load_weights(wbf, kMlpIn, s.w1);
-  load_weights(wbf + kMlpHidden * kMlpIn, kMlpHidden, s.w2);
-  load_weights(wbf + kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden, kMlpHidden, s.w3);
-  for (int i = t; i < kMlpHidden; i += blockDim.x) {
-    s.b1[i] = params[kOffB1 + i];
-    s.b2[i] = params[kOffB2 + i];
-    s.b3[i] = params[kOffB3 + i];
-    s.w4[i] = params[kOffW4 + i];
-  }
+  load_weights_ext(wbf, params + kOffB1, kMlpIn, kKcX, s.w1);
+  load_weights_ext(wbf + kMlpHidden * kMlpIn, params + kOffB2, kMlpHidden, kKcH, s.w2);
+  load_weights_ext(wbf + kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden, params + kOffB3,
+                   kMlpHidden, kKcH, s.w3);
+  for (int i = t; i < kMlpHidden; i += blockDim.x) s.w4[i] = params[kOffW4 + i];
   if (t < kMlpIn) {
     s.mean[t] = norm[t];
     s.istd[t] = norm[kMlpIn + t];
   }
+  // constant columns of this thread's rows
+  put8_const(s.x0, kKcX, t, 16, 1.0f);
+  put8_const(s.x0, kKcX, t, 24, 0.0f);
+  put8_const(s.h, kKcH, t, 64, 1.0f);
+  put8_const(s.h, kKcH, t, 72, 0.0f);
   const float b4 = params[kOffB4];
   const float out_scale = norm[2 * kMlpIn] * extra_scale;
   if (t < 32) {
@@ -203,11 +232,14 @@ __global__ void __launch_bounds__(kMlpTile)
   __syncthreads();
   tc::fence_after();
   const uint32_t taddr = s.taddr;
+  const uint32_t lane_base = taddr + ((uint32_t)((t >> 5) * 32) << 16);
+  const uint32_t sx0 = tc::smem_u32(s.x0), sh = tc::smem_u32(s.h);
+  const uint32_t sw[3] = {tc::smem_u32(s.w1), tc::smem_u32(s.w2), tc::smem_u32(s.w3)};
   uint32_t phase = 0;
+  bool ok = true;
   float h[kMlpHidden];
   for (int tile = blockIdx.x; tile * kMlpTile < n; tile += gridDim.x) {
     const int p = tile * kMlpTile + t;
-    // input layer operand: normalised features, K = 16
     if (BF16_IN) {
       uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
       if (p < n) {
@@ -215,8 +247,8 @@ __global__ void __launch_bounds__(kMlpTile)
         lo = __ldg(xr);
         hi = __ldg(xr + 1);
       }
-      *reinterpret_cast<uint4*>(s.act + tc::core_off(t, 0, kMlpIn / 8)) = lo;
-      *reinterpret_cast<uint4*>(s.act + tc::core_off(t, 8, kMlpIn / 8)) = hi;
+      *reinterpret_cast<uint4*>(s.x0 + tc::core_off(t, 0, kKcX)) = lo;
+      *reinterpret_cast<uint4*>(s.x0 + tc::core_off(t, 8, kKcX)) = hi;
     } else {
       const float* feat = reinterpret_cast<const float*>(in);
       float f[kMlpIn];
@@ -232,18 +264,10 @@ __global__ void __launch_bounds__(kMlpTile)
         for (int k = 0; k < kMlpIn; ++k) f[k] = s.mean[k];
       }
 #pragma unroll
-      for (int k0 = 0; k0 < kMlpIn; k0 += 8) {
-        __align__(16) __nv_bfloat16 pk[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-          pk[i] = __float2bfloat16_rn((f[k0 + i] - s.mean[k0 + i]) * s.istd[k0 + i]);
-        *reinterpret_cast<uint4*>(s.act + tc::core_off(t, k0, kMlpIn / 8)) =
-            *reinterpret_cast<const uint4*>(pk);
-      }
+      for (int k = 0; k < kMlpIn; ++k) f[k] = (f[k] - s.mean[k]) * s.istd[k];
+      put8(s.x0, kKcX, t, 0, f);
+      put8(s.x0, kKcX, t, 8, f + 8);
     }
-    const uint8_t* layer_w[3] = {s.w1, s.w2, s.w3};
-    const float* layer_b[3] = {s.b1, s.b2, s.b3};
-    bool ok = true;
 #pragma unroll 1
     for (int l = 0; l < 3; ++l) {
       tc::fence_async_smem();
@@ -251,21 +275,22 @@ __global__ void __launch_bounds__(kMlpTile)
       __syncthreads();
       if (t == 0) {
         tc::fence_after();
-        issue_layer(s, layer_w[l], l == 0 ? kMlpIn : kMlpHidden, taddr);
+        if (l == 0) mma_kk(taddr, sx0, kKcX, sw[0], kKcX, kKX, tc::kIdescM128N64);
+        else mma_kk(taddr, sh, kKcH, sw[l], kKcH, kKH, tc::kIdescM128N64);
+        tc::commit(&s.mbar);
       }
       // the whole CTA takes the same branch: a wait that gave up anywhere aborts
       ok = __syncthreads_and(tc::mbar_wait(&s.mbar, phase) ? 1 : 0) != 0;
       phase ^= 1u;
       tc::fence_after();
       if (!ok) break;
-      read_row(taddr, h);
-      const float* b = layer_b[l];
+      tmem_row64(lane_base, 0, h);
 #pragma unroll
-      for (int j = 0; j < kMlpHidden; ++j) h[j] = gelu_tanh(h[j] + b[j]);
-      // every thread has read D and the MMA has consumed act: act may change
-      tc::fence_before();
-      __syncthreads();
-      if (l < 2) write_row(s, h);
+      for (int j = 0; j < kMlpHidden; ++j) h[j] = gelu_tanh(h[j]);
+      if (l < 2) {
+#pragma unroll
+        for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.h, kKcH, t, k0, h + k0);
+      }
     }
     if (!ok) {
       if (t == 0) atomicOr(err, kErrMlpWait);
@@ -273,8 +298,15 @@ __global__ void __launch_bounds__(kMlpTile)
     }
     if (p < n) {
       float y = b4;
+      const float4* w4 = reinterpret_cast<const float4*>(s.w4);
 #pragma unroll
-      for (int j = 0; j < kMlpHidden; ++j) y = fmaf(s.w4[j], h[j], y);
+      for (int j = 0; j < kMlpHidden / 4; ++j) {
+        const float4 w = w4[j];
+        y = fmaf(w.x, h[4 * j], y);
+        y = fmaf(w.y, h[4 * j + 1], y);
+        y = fmaf(w.z, h[4 * j + 2], y);
+        y = fmaf(w.w, h[4 * j + 3], y);
+      }
       y *= out_scale;
       if (out) out[p] = y;
       if (pd_out) {
@@ -298,7 +330,7 @@ __global__ void __launch_bounds__(kMlpTile)
 //   h1, h2, h3 [128 x 80]  activations, column 64 = 1, rest 0
 //   dz [128 x 128] the current layer's pre-activation gradient, columns
 //                  64..127 = 0
-// Forward   z_l  = h_{l-1} W_l^T            A, B K-major
+// Forward   z_l  = [h_{l-1} | 1] [W_l | b_l]^T    A, B K-major (bias in the MMA)
 // Backward  dh_l = dz_l W_l                 A K-major, B = W_l read MN-major
 // Gradient  G_l += dz_l^T [h_{l-1} | 1]     A = dz read MN-major (M = 128 over
 //           output neurons, rows 64..127 unused), B = h read MN-major, K =
@@ -311,21 +343,20 @@ __global__ void __launch_bounds__(kMlpTile)
 //   z1 0..63, z2 64..127, z3 128..191 (dh2 reuses z3, dh1 reuses z2),
 //   G4 192..271, G3 272..351, G2 352..431, G1 432..463.
 // ---------------------------------------------------------------------------
-constexpr int kKcX = 4, kKcH = 10, kKcD = 16;
 constexpr uint32_t kTZ1 = 0, kTZ2 = 64, kTZ3 = 128, kTG4 = 192, kTG3 = 272, kTG2 = 352,
                    kTG1 = 432;
 constexpr uint32_t kTrainCols = 512;
 
 struct TrainSmem {
-  alignas(1024) uint8_t w1[kMlpHidden * kMlpIn * 2];
-  alignas(128) uint8_t w2[kMlpHidden * kMlpHidden * 2];
-  alignas(128) uint8_t w3[kMlpHidden * kMlpHidden * 2];
+  alignas(1024) uint8_t w1[kMlpHidden * kKcX * 16];
+  alignas(128) uint8_t w2[kMlpHidden * kKcH * 16];
+  alignas(128) uint8_t w3[kMlpHidden * kKcH * 16];
   alignas(128) uint8_t x0[kMlpTile * kKcX * 16];
   alignas(128) uint8_t h1[kMlpTile * kKcH * 16];
   alignas(128) uint8_t h2[kMlpTile * kKcH * 16];
   alignas(128) uint8_t h3[kMlpTile * kKcH * 16];
   alignas(128) uint8_t dz[kMlpTile * kKcD * 16];
-  float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpHidden], w4[kMlpHidden];
+  float w4[kMlpHidden];
   float mean[kMlpIn], istd[kMlpIn];
   float red[kMlpTile / 32];
   // keeps every operand read of the descriptors above inside the CTA's shared
@@ -335,40 +366,14 @@ struct TrainSmem {
   uint32_t taddr;
 };
 
+size_t train_smem_bytes() { return sizeof(TrainSmem) + 1024; }
+
+// d/dz of gelu_tanh: 0.5 (1 + t) + 0.5 z (1 - t^2) (c + 3 c a z^2).
 __device__ __forceinline__ float gelu_grad(float z) {
-  const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
-  float t;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-  return 0.5f * (1.0f + t) +
-         0.5f * z * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 3.0f * 0.044715f * z * z);
-}
-
-// 8 consecutive values of row r starting at column k0 (multiple of 8).
-__device__ __forceinline__ void put8(uint8_t* buf, int kc, int r, int k0, const float* v) {
-  __align__(16) __nv_bfloat16 pk[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) pk[i] = __float2bfloat16_rn(v[i]);
-  *reinterpret_cast<uint4*>(buf + tc::core_off(r, k0, kc)) = *reinterpret_cast<const uint4*>(pk);
-}
-
-__device__ __forceinline__ void put8_const(uint8_t* buf, int kc, int r, int k0, float first) {
-  float v[8] = {first, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  put8(buf, kc, r, k0, v);
-}
-
-// 64 FP32 columns starting at TMEM column `col` of this thread's lane.
-__device__ __forceinline__ void tmem_row64(uint32_t lane_base, uint32_t col, float* v) {
-#pragma unroll
-  for (int c = 0; c < 64; c += 16) tc::tmem_ld16(lane_base + col + c, v + c);
-  tc::tmem_wait_ld();
-}
-
-// K-major A [128 x K] x K-major B [N x K]^T, K in steps of 16.
-__device__ __forceinline__ void mma_kk(uint32_t d, uint32_t a, int kca, uint32_t b, int kcb, int K,
-                                       uint32_t idesc) {
-  for (int st = 0; st < K / 16; ++st)
-    tc::mma_bf16(d, tc::smem_desc(a + st * 256, 128, kca * 128),
-                 tc::smem_desc(b + st * 256, 128, kcb * 128), idesc, st > 0);
+  const float z2 = z * z;
+  const float t = tanh_approx(z * fmaf(kGeluCA, z2, kGeluC));
+  const float hz = 0.5f * z;
+  return fmaf(hz * (1.0f - t * t), fmaf(3.0f * kGeluCA, z2, kGeluC), 0.5f + 0.5f * t);
 }
 
 // Weight gradient over the 128 rows of a tile: D[M=128][N] (+)= A^T B with A
@@ -381,13 +386,14 @@ __device__ __forceinline__ void mma_grad(uint32_t d, uint32_t a, uint32_t b, int
                  tc::smem_desc(b + st * 2 * kcb * 128, kcb * 128, 128), idesc, acc || st > 0);
 }
 
-// dh [128 x 64] = dz [128 x 64] . W [64 x 64] with W (row-major [out][in],
-// core layout K-major for the forward) read MN-major.
+// dh [128 x 64] = dz [128 x 64] . W [64 x 64] with the weight rows (W | b,
+// core layout K-major for the forward, kKcH core columns) read MN-major over
+// their first 64 columns.
 __device__ __forceinline__ void mma_dh(uint32_t d, uint32_t a, uint32_t w) {
   const uint32_t idesc = tc::idesc_bf16(128, 64, 0, 1);
   for (int st = 0; st < kMlpHidden / 16; ++st)
     tc::mma_bf16(d, tc::smem_desc(a + st * 256, 128, kKcD * 128),
-                 tc::smem_desc(w + st * 2 * 8 * 128, 8 * 128, 128), idesc, st > 0);
+                 tc::smem_desc(w + st * 2 * kKcH * 128, kKcH * 128, 128), idesc, st > 0);
 }
 
 __global__ void __launch_bounds__(kMlpTile, 1)
@@ -400,15 +406,11 @@ __global__ void __launch_bounds__(kMlpTile, 1)
   const uint32_t mis = tc::smem_u32(smem_raw) & 1023u;
   TrainSmem& s = *reinterpret_cast<TrainSmem*>(smem_raw + ((1024u - mis) & 1023u));
   const int t = threadIdx.x, warp = t >> 5;
-  load_weights(wbf, kMlpIn, s.w1);
-  load_weights(wbf + kMlpHidden * kMlpIn, kMlpHidden, s.w2);
-  load_weights(wbf + kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden, kMlpHidden, s.w3);
-  for (int i = t; i < kMlpHidden; i += blockDim.x) {
-    s.b1[i] = params[kOffB1 + i];
-    s.b2[i] = params[kOffB2 + i];
-    s.b3[i] = params[kOffB3 + i];
-    s.w4[i] = params[kOffW4 + i];
-  }
+  load_weights_ext(wbf, params + kOffB1, kMlpIn, kKcX, s.w1);
+  load_weights_ext(wbf + kMlpHidden * kMlpIn, params + kOffB2, kMlpHidden, kKcH, s.w2);
+  load_weights_ext(wbf + kMlpHidden * kMlpIn + kMlpHidden * kMlpHidden, params + kOffB3,
+                   kMlpHidden, kKcH, s.w3);
+  for (int i = t; i < kMlpHidden; i += blockDim.x) s.w4[i] = params[kOffW4 + i];
   if (t < kMlpIn) {
     s.mean[t] = norm[t];
     s.istd[t] = norm[kMlpIn + t];
@@ -493,27 +495,27 @@ __global__ void __launch_bounds__(kMlpTile, 1)
       put8(s.x0, kKcX, t, 8, f + 8);
     }
     // forward
-    if (!(ok = run([&] { mma_kk(taddr + kTZ1, sx0, kKcX, sw1, 2, kMlpIn, tc::kIdescM128N64); })))
+    if (!(ok = run([&] { mma_kk(taddr + kTZ1, sx0, kKcX, sw1, kKcX, kKX, tc::kIdescM128N64); })))
       break;
     tmem_row64(lane_base, kTZ1, v);
 #pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) v[j] = gelu_tanh(v[j] + s.b1[j]);
+    for (int j = 0; j < kMlpHidden; ++j) v[j] = gelu_tanh(v[j]);
 #pragma unroll
     for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.h1, kKcH, t, k0, v + k0);
-    if (!(ok = run([&] { mma_kk(taddr + kTZ2, sh1, kKcH, sw2, 8, kMlpHidden, tc::kIdescM128N64); })))
+    if (!(ok = run([&] { mma_kk(taddr + kTZ2, sh1, kKcH, sw2, kKcH, kKH, tc::kIdescM128N64); })))
       break;
     tmem_row64(lane_base, kTZ2, v);
 #pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) v[j] = gelu_tanh(v[j] + s.b2[j]);
+    for (int j = 0; j < kMlpHidden; ++j) v[j] = gelu_tanh(v[j]);
 #pragma unroll
     for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.h2, kKcH, t, k0, v + k0);
-    if (!(ok = run([&] { mma_kk(taddr + kTZ3, sh2, kKcH, sw3, 8, kMlpHidden, tc::kIdescM128N64); })))
+    if (!(ok = run([&] { mma_kk(taddr + kTZ3, sh2, kKcH, sw3, kKcH, kKH, tc::kIdescM128N64); })))
       break;
     tmem_row64(lane_base, kTZ3, v);
     float u = b4;
 #pragma unroll
     for (int j = 0; j < kMlpHidden; ++j) {
-      v[j] = gelu_tanh(v[j] + s.b3[j]);
+      v[j] = gelu_tanh(v[j]);
       u = fmaf(s.w4[j], v[j], u);
     }
 #pragma unroll
@@ -529,7 +531,7 @@ __global__ void __launch_bounds__(kMlpTile, 1)
     // layer 3
     tmem_row64(lane_base, kTZ3, v);
 #pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) v[j] = g * s.w4[j] * gelu_grad(v[j] + s.b3[j]);
+    for (int j = 0; j < kMlpHidden; ++j) v[j] = g * s.w4[j] * gelu_grad(v[j]);
 #pragma unroll
     for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.dz, kKcD, t, k0, v + k0);
     if (!(ok = run([&] {
@@ -545,7 +547,7 @@ __global__ void __launch_bounds__(kMlpTile, 1)
       tc::tmem_ld16(lane_base + kTZ2 + c, z);
       tc::tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) dh[i] *= gelu_grad(z[i] + s.b2[c + i]);
+      for (int i = 0; i < 16; ++i) dh[i] *= gelu_grad(z[i]);
       put8(s.dz, kKcD, t, c, dh);
       put8(s.dz, kKcD, t, c + 8, dh + 8);
     }
@@ -562,7 +564,7 @@ __global__ void __launch_bounds__(kMlpTile, 1)
       tc::tmem_ld16(lane_base + kTZ1 + c, z);
       tc::tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) dh[i] *= gelu_grad(z[i] + s.b1[c + i]);
+      for (int i = 0; i < 16; ++i) dh[i] *= gelu_grad(z[i]);
       put8(s.dz, kKcD, t, c, dh);
       put8(s.dz, kKcD, t, c + 8, dh + 8);
     }
@@ -758,23 +760,42 @@ void mlp_release(MlpState& m) {
   m.ready = false;
 }
 
+// Opts the MLP kernels into their dynamic shared memory (once per device).
+static int set_mlp_attrs() {
+  static int done_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 32 && (done_mask >> dev & 1)) return SPHPC_OK;
+  cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)train_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mlp_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)fwd_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mlp_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)fwd_smem_bytes());
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "MLP kernel attributes: %s", cudaGetErrorString(e));
+  if (dev < 32) done_mask |= 1 << dev;
+  return SPHPC_OK;
+}
+
 void launch_mlp_forward(const MlpDevice& d, const float* feat, int n, float* out,
                         const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
                         float extra_scale) {
-  if (n <= 0) return;
+  if (n <= 0 || set_mlp_attrs() != SPHPC_OK) return;
   const int tiles = (n + kMlpTile - 1) / kMlpTile;
   const int grid = tiles < 148 * 4 ? tiles : 148 * 4;
-  k_mlp_forward<false><<<grid, kMlpTile, 0, st>>>(d.params, d.norm, d.wbf, feat, n, out, pd_in,
+  k_mlp_forward<false><<<grid, kMlpTile, fwd_smem_bytes(), st>>>(d.params, d.norm, d.wbf, feat, n, out, pd_in,
                                                   pd_out, err, extra_scale);
 }
 
 void launch_mlp_forward_bf16(const MlpDevice& d, const __nv_bfloat16* xbf, int n,
                              const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
                              float extra_scale) {
-  if (n <= 0) return;
+  if (n <= 0 || set_mlp_attrs() != SPHPC_OK) return;
   const int tiles = (n + kMlpTile - 1) / kMlpTile;
   const int grid = tiles < 148 * 4 ? tiles : 148 * 4;
-  k_mlp_forward<true><<<grid, kMlpTile, 0, st>>>(d.params, d.norm, d.wbf, xbf, n, nullptr, pd_in,
+  k_mlp_forward<true><<<grid, kMlpTile, fwd_smem_bytes(), st>>>(d.params, d.norm, d.wbf, xbf, n, nullptr, pd_in,
                                                  pd_out, err, extra_scale);
 }
 
@@ -796,20 +817,6 @@ int dataset_check_device() {
   if (g_ds.cap > 0 && dev != g_ds.device)
     return set_error(SPHPC_EINVAL, "training set lives on device %d, current device is %d",
                      g_ds.device, dev);
-  return SPHPC_OK;
-}
-
-size_t train_smem_bytes() { return sizeof(TrainSmem) + 1024; }
-
-int set_train_attr() {
-  static int done = -1;
-  int dev = -1;
-  cudaGetDevice(&dev);
-  if (done == dev) return SPHPC_OK;
-  const cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)train_smem_bytes());
-  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "MLP training kernel: %s", cudaGetErrorString(e));
-  done = dev;
   return SPHPC_OK;
 }
 
@@ -904,7 +911,7 @@ extern "C" int sphpc_mlp_grad(const float* d_feat, const float* d_target, int n,
   if (n <= 0 || !d_feat || !d_target || !params || !norm || !grad_out)
     return set_error(SPHPC_EINVAL, "sphpc_mlp_grad: bad arguments");
   cudaStream_t st = (cudaStream_t)cuda_stream;
-  SPHPC_RC(set_train_attr());
+  SPHPC_RC(set_mlp_attrs());
   MlpDevice d;
   TrainBufs b;
   int rc = mlp_upload(d, params, norm, st);
@@ -1050,14 +1057,15 @@ extern "C" int sphpc_mlp_dataset_stats(float* norm) {
 // AdamW training on the training set: `steps` steps of `batch` rows drawn
 // without replacement within each pass over the set (a fresh affine
 // permutation of the row indices per pass, seeded by `seed`), learning rate
-// lr, decoupled weight decay on the weights, beta = (0.9, 0.999), eps 1e-8.
+// from lr down to lr_final on a half cosine (lr_final = lr: constant),
+// decoupled weight decay on the weights, beta = (0.9, 0.999), eps 1e-8.
 // params_out[9473] receives the trained parameters; loss_out[steps], if
 // given, the batch loss of every step (before its update).
 extern "C" int sphpc_mlp_train(const float* params_in, const float* norm, int steps, int batch,
-                               float lr, float weight_decay, unsigned long long seed,
-                               float* params_out, float* loss_out) {
+                               float lr, float lr_final, float weight_decay,
+                               unsigned long long seed, float* params_out, float* loss_out) {
   if (!params_in || !norm || !params_out || steps < 0 || batch <= 0 || !(lr > 0.0f) ||
-      weight_decay < 0.0f)
+      !(lr_final >= 0.0f) || weight_decay < 0.0f)
     return set_error(SPHPC_EINVAL, "sphpc_mlp_train: bad arguments");
   long long N = 0;
   float *feat = nullptr, *target = nullptr;
@@ -1069,7 +1077,7 @@ extern "C" int sphpc_mlp_train(const float* params_in, const float* norm, int st
     if (N > 0) SPHPC_RC(dataset_check_device());
   }
   if (N < 1) return set_error(SPHPC_ENOTREADY, "sphpc_mlp_train: empty training set");
-  SPHPC_RC(set_train_attr());
+  SPHPC_RC(set_mlp_attrs());
   cudaStream_t st = 0;
   MlpDevice d;
   TrainBufs b;
@@ -1107,10 +1115,13 @@ extern "C" int sphpc_mlp_train(const float* params_in, const float* norm, int st
     k_mlp_grad<<<grid, kMlpTile, train_smem_bytes(), st>>>(d.params, d.norm, d.wbf, feat, target, N,
                                                          first % N, mul, add, batch, b.partial,
                                                          b.err);
+    // cosine from lr to lr_final over the run
+    const double frac = steps > 1 ? (double)(k - 1) / (double)(steps - 1) : 0.0;
+    const float lr_k = (float)(lr_final + 0.5 * (lr - lr_final) * (1.0 + std::cos(M_PI * frac)));
     const float bc1 = (float)(1.0 / (1.0 - std::pow((double)beta1, (double)k)));
     const float bc2 = (float)(1.0 / (1.0 - std::pow((double)beta2, (double)k)));
     k_mlp_update<<<(kMlpParams + 256) / 256, 256, 0, st>>>(b.partial, grid, d.params, b.m, b.v,
-                                                          d.wbf, nullptr, b.loss + (k - 1), lr,
+                                                          d.wbf, nullptr, b.loss + (k - 1), lr_k,
                                                           beta1, beta2, eps, weight_decay, bc1,
                                                           bc2);
   }

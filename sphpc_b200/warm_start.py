@@ -112,14 +112,17 @@ def dataset_stats() -> np.ndarray:
 
 
 def train(params: np.ndarray, norm: np.ndarray, steps: int, batch: int = 65536,
-          lr: float = 1e-3, weight_decay: float = 1e-4, seed: int = 0):
-    """AdamW on the training set; returns (params, per-step batch loss)."""
+          lr: float = 1e-3, weight_decay: float = 1e-4, seed: int = 0,
+          lr_final: float | None = None):
+    """AdamW on the training set, learning rate from lr to lr_final (default:
+    constant lr) on a half cosine; returns (params, per-step batch loss)."""
     p_in = np.ascontiguousarray(params, np.float32)
     nrm = np.ascontiguousarray(norm, np.float32)
     out = np.zeros(N_PARAMS, np.float32)
     loss = np.zeros(max(steps, 1), np.float32)
     call("sphpc_mlp_train", _fp(p_in), _fp(nrm), int(steps), int(batch), float(lr),
-         float(weight_decay), C.c_ulonglong(seed), _fp(out), _fp(loss))
+         float(lr if lr_final is None else lr_final), float(weight_decay), C.c_ulonglong(seed),
+         _fp(out), _fp(loss))
     return out, loss[:steps]
 
 
