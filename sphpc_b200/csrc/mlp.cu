@@ -131,13 +131,17 @@ constexpr int kKX = kKcX * 8, kKH = kKcH * 8;
 // Weight rows [64][kc*8] = W[j][0..K) | bf16(b[j]) | 0 in the core layout.
 __device__ void load_weights_ext(const __nv_bfloat16* __restrict__ w,
                                  const float* __restrict__ bias, int K, int kc, uint8_t* dst) {
-  const int width = kc * 8;
-  for (int i = threadIdx.x; i < kMlpHidden * width; i += blockDim.x) {
-    const int r = i / width, k = i % width;
-    __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
-    if (k < K) v = w[r * K + k];
-    else if (k == K) v = __float2bfloat16_rn(bias[r]);
-    *reinterpret_cast<__nv_bfloat16*>(dst + tc::core_off(r, k, kc)) = v;
+  // one 16-byte core-matrix row (8 columns) per iteration; K is a multiple of 8
+  for (int i = threadIdx.x; i < kMlpHidden * kc; i += blockDim.x) {
+    const int r = i / kc, k0 = (i % kc) * 8;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (k0 < K) {
+      v = __ldg(reinterpret_cast<const uint4*>(w + r * K + k0));
+    } else if (k0 == K) {
+      const __nv_bfloat162 b2 = __floats2bfloat162_rn(bias[r], 0.0f);
+      v.x = *reinterpret_cast<const uint32_t*>(&b2);
+    }
+    *reinterpret_cast<uint4*>(dst + tc::core_off(r, k0, kc)) = v;
   }
 }
 
@@ -238,17 +242,32 @@ __global__ void __launch_bounds__(kMlpTile)
   uint32_t phase = 0;
   bool ok = true;
   float h[kMlpHidden];
+  // BF16 rows of the next tile are loaded one tile ahead, so their latency
+  // overlaps the current tile's MMA round trips
+  uint4 nlo = make_uint4(0, 0, 0, 0), nhi = nlo;
+  if (BF16_IN) {
+    const int p0 = blockIdx.x * kMlpTile + t;
+    if (p0 < n) {
+      const uint4* xr = reinterpret_cast<const uint4*>(in) + (size_t)p0 * 2;
+      nlo = __ldg(xr);
+      nhi = __ldg(xr + 1);
+    }
+  }
   for (int tile = blockIdx.x; tile * kMlpTile < n; tile += gridDim.x) {
     const int p = tile * kMlpTile + t;
+    float4 rx, rd;  // this row's record, read early for the same reason
+    if (pd_out && p < n) ld_pd(pd_in, p, rx, rd);
     if (BF16_IN) {
-      uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
-      if (p < n) {
-        const uint4* xr = reinterpret_cast<const uint4*>(in) + (size_t)p * 2;
-        lo = __ldg(xr);
-        hi = __ldg(xr + 1);
+      *reinterpret_cast<uint4*>(s.x0 + tc::core_off(t, 0, kKcX)) = nlo;
+      *reinterpret_cast<uint4*>(s.x0 + tc::core_off(t, 8, kKcX)) = nhi;
+      const int pn = p + gridDim.x * kMlpTile;
+      nlo = make_uint4(0, 0, 0, 0);
+      nhi = nlo;
+      if (pn < n) {
+        const uint4* xr = reinterpret_cast<const uint4*>(in) + (size_t)pn * 2;
+        nlo = __ldg(xr);
+        nhi = __ldg(xr + 1);
       }
-      *reinterpret_cast<uint4*>(s.x0 + tc::core_off(t, 0, kKcX)) = lo;
-      *reinterpret_cast<uint4*>(s.x0 + tc::core_off(t, 8, kKcX)) = hi;
     } else {
       const float* feat = reinterpret_cast<const float*>(in);
       float f[kMlpIn];
@@ -310,10 +329,8 @@ __global__ void __launch_bounds__(kMlpTile)
       y *= out_scale;
       if (out) out[p] = y;
       if (pd_out) {
-        float4 x, d;
-        ld_pd(pd_in, p, x, d);
-        d.w = fminf(y, 0.0f);
-        st_pd(pd_out, p, x, d);
+        rd.w = fminf(y, 0.0f);
+        st_pd(pd_out, p, rx, rd);
       }
     }
   }
