@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(kBlock)
     k_reorder(const DevParams P, const uint32_t* __restrict__ sorted_ids,
               const uint32_t* __restrict__ loc_by_id, const PD* __restrict__ pd_in,
               const float4* __restrict__ vel_in, PD* __restrict__ pd_out,
-              float4* __restrict__ vel_out, float4* __restrict__ xsa,
+              float4* __restrict__ vel_out, float4* __restrict__ xsa, uint4* __restrict__ nr_out,
               uint32_t* __restrict__ cellp, int predict, int move_vel, ReorderExtra ex) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= P.n) return;
@@ -110,6 +110,7 @@ __global__ void __launch_bounds__(kBlock)
   d.w = predict ? 0.0f : dg.w;
   st_pd(pd_out, j, x, d);
   xsa[j] = make_float4((float)xs, (float)ys, (float)zs, 0.0f);
+  nr_out[j] = make_nr(P, xs, ys, zs, d.w);
   cellp[j] = pack_cell(P, cx, cy, cz);
   if (move_vel) {
     if (predict) {
@@ -349,12 +350,12 @@ void launch_hash(const DevParams& P, const PD* pd, const float4* vel, const uint
 
 void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
                     const PD* pd_in, const float4* vel_in, PD* pd_out, float4* vel_out,
-                    float4* xsa, uint32_t* cellp, bool predict, bool move_vel,
+                    float4* xsa, uint4* nr_out, uint32_t* cellp, bool predict, bool move_vel,
                     const ReorderExtra* extra, cudaStream_t st) {
   ReorderExtra ex = {};
   if (extra) ex = *extra;
   k_reorder<<<grid_for(P.n), kBlock, 0, st>>>(P, sorted_ids, loc_by_id, pd_in, vel_in, pd_out,
-                                              vel_out, xsa, cellp, predict ? 1 : 0,
+                                              vel_out, xsa, nr_out, cellp, predict ? 1 : 0,
                                               move_vel ? 1 : 0, ex);
 }
 

@@ -38,7 +38,7 @@ struct ReorderExtra {
 };
 void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
                     const PD* pd_in, const float4* vel_in, PD* pd_out, float4* vel_out,
-                    float4* xsa, uint32_t* cellp, bool predict, bool move_vel,
+                    float4* xsa, uint4* nr_out, uint32_t* cellp, bool predict, bool move_vel,
                     const ReorderExtra* extra, cudaStream_t st);
 
 // Cell start table cstart[0..C] from sorted keys (lower bounds; cstart[C]=n).
@@ -60,8 +60,10 @@ void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr,
 // ---- PBF passes (pbf.cu) ----
 
 struct PassArgs {
-  const PD* pd;        // records {x, d} read by the pass (neighbours included)
-  PD* pd_out;          // records written by the pass (never the same buffer)
+  const PD* pd;        // particle records {x, d} (own reads only)
+  PD* pd_out;          // particle records written by the pass (never pd)
+  const uint4* nr;     // 16-byte neighbour records read by the pass
+  uint4* nr_out;       // neighbour records written by the pass (never nr)
   float4* vel;
   float4* vel_out;
   float* rho;
@@ -90,7 +92,7 @@ void launch_features(const DevParams& P, const NbrView& V, const PassArgs& a, fl
 void launch_features_bf16(const DevParams& P, const NbrView& V, const PassArgs& a,
                           __nv_bfloat16* xbf, const float* norm, cudaStream_t st);
 // target[p] += s * lambda_p (lambda in rec[p].d.w), p < limit.
-void launch_accum_lambda(const PD* rec, float s, float* target, int limit, cudaStream_t st);
+void launch_accum_lambda(const uint4* rec, float s, float* target, int limit, cudaStream_t st);
 // Position pass: UpdateDPs (:668-746) with lambda from d.w; mode 0 fuses
 // UpdatePositionStars (:529-564, clamp + SDF collision) and, if a.last,
 // UpdateVelocities (:787-838); mode 1 writes dp[] only.
@@ -115,8 +117,13 @@ void launch_gravity(const DevParams& P, float4* vel, cudaStream_t st);
 void launch_predict(const DevParams& P, PD* pd, const float4* vel, cudaStream_t st);
 void launch_update_velocities(const DevParams& P, const PD* pd, float4* vel, cudaStream_t st);
 void launch_update_positions(const DevParams& P, PD* pd, cudaStream_t st);
-// d.w <- src[p] (repack a per-particle scalar for the neighbour passes).
-void launch_pack_w(const DevParams& P, PD* pd, const float* src, cudaStream_t st);
+// d.w and/or the record payload <- src[p] (a per-particle scalar for the
+// neighbour passes; null pd or nr skips it).
+void launch_pack_w(const DevParams& P, PD* pd, uint4* nr, const float* src, cudaStream_t st);
+// Neighbour records from particle records: canonical x* and payload src[p]
+// (d.w when src is null).
+void launch_make_nr(const DevParams& P, const PD* pd, const float* src, uint4* nr,
+                    cudaStream_t st);
 // CalculateParticleCollisions seam on device double arrays.
 void launch_collisions_double(const DevParams& P, double* x, double* y, double* z, int n,
                               cudaStream_t st);

@@ -200,8 +200,8 @@ template <bool BF16_IN>
 __global__ void __launch_bounds__(kMlpTile)
     k_mlp_forward(const float* __restrict__ params, const float* __restrict__ norm,
                   const __nv_bfloat16* __restrict__ wbf, const void* __restrict__ in, int n,
-                  float* __restrict__ out, const PD* __restrict__ pd_in, PD* __restrict__ pd_out,
-                  uint32_t* __restrict__ err, float extra_scale) {
+                  float* __restrict__ out, const uint4* __restrict__ rec_in,
+                  uint4* __restrict__ rec_out, uint32_t* __restrict__ err, float extra_scale) {
   extern __shared__ __align__(128) uint8_t fwd_raw[];
   const uint32_t mis = tc::smem_u32(fwd_raw) & 127u;
   MlpSmem& s = *reinterpret_cast<MlpSmem*>(fwd_raw + ((128u - mis) & 127u));
@@ -255,8 +255,8 @@ __global__ void __launch_bounds__(kMlpTile)
   }
   for (int tile = blockIdx.x; tile * kMlpTile < n; tile += gridDim.x) {
     const int p = tile * kMlpTile + t;
-    float4 rx, rd;  // this row's record, read early for the same reason
-    if (pd_out && p < n) ld_pd(pd_in, p, rx, rd);
+    uint4 rec = make_uint4(0, 0, 0, 0);  // this row's record, read early for the same reason
+    if (rec_out && p < n) rec = ld_nr(rec_in, p);
     if (BF16_IN) {
       *reinterpret_cast<uint4*>(s.x0 + tc::core_off(t, 0, kKcX)) = nlo;
       *reinterpret_cast<uint4*>(s.x0 + tc::core_off(t, 8, kKcX)) = nhi;
@@ -328,9 +328,9 @@ __global__ void __launch_bounds__(kMlpTile)
       }
       y *= out_scale;
       if (out) out[p] = y;
-      if (pd_out) {
-        rd.w = fminf(y, 0.0f);
-        st_pd(pd_out, p, rx, rd);
+      if (rec_out) {
+        rec.w = __float_as_uint(fminf(y, 0.0f));
+        rec_out[p] = rec;
       }
     }
   }
@@ -797,23 +797,23 @@ static int set_mlp_attrs() {
 }
 
 void launch_mlp_forward(const MlpDevice& d, const float* feat, int n, float* out,
-                        const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
+                        const uint4* rec_in, uint4* rec_out, uint32_t* err, cudaStream_t st,
                         float extra_scale) {
   if (n <= 0 || set_mlp_attrs() != SPHPC_OK) return;
   const int tiles = (n + kMlpTile - 1) / kMlpTile;
   const int grid = tiles < 148 * 4 ? tiles : 148 * 4;
-  k_mlp_forward<false><<<grid, kMlpTile, fwd_smem_bytes(), st>>>(d.params, d.norm, d.wbf, feat, n, out, pd_in,
-                                                  pd_out, err, extra_scale);
+  k_mlp_forward<false><<<grid, kMlpTile, fwd_smem_bytes(), st>>>(d.params, d.norm, d.wbf, feat, n, out, rec_in,
+                                                  rec_out, err, extra_scale);
 }
 
 void launch_mlp_forward_bf16(const MlpDevice& d, const __nv_bfloat16* xbf, int n,
-                             const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
+                             const uint4* rec_in, uint4* rec_out, uint32_t* err, cudaStream_t st,
                              float extra_scale) {
   if (n <= 0 || set_mlp_attrs() != SPHPC_OK) return;
   const int tiles = (n + kMlpTile - 1) / kMlpTile;
   const int grid = tiles < 148 * 4 ? tiles : 148 * 4;
-  k_mlp_forward<true><<<grid, kMlpTile, fwd_smem_bytes(), st>>>(d.params, d.norm, d.wbf, xbf, n, nullptr, pd_in,
-                                                 pd_out, err, extra_scale);
+  k_mlp_forward<true><<<grid, kMlpTile, fwd_smem_bytes(), st>>>(d.params, d.norm, d.wbf, xbf, n, nullptr, rec_in,
+                                                 rec_out, err, extra_scale);
 }
 
 // ---- device-resident training set (one per process, on the device that

@@ -57,15 +57,16 @@ int mlp_upload(MlpDevice& d, const float* params, const float* norm, cudaStream_
 void mlp_free(MlpDevice& d);
 
 // Forward pass of n feature rows feat[n][16] -> out[n] (lambda0), or when
-// pd_in/pd_out are given, records pd_out[p] = {x, (d, min(lambda0, 0))} from
-// pd_in (the plain solver's multipliers are never positive).
+// rec_in/rec_out are given, 16-byte neighbour records rec_out[p] = rec_in[p]
+// with the payload min(lambda0, 0) (the plain solver's multipliers are never
+// positive).
 void launch_mlp_forward(const MlpDevice& d, const float* feat, int n, float* out,
-                        const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
+                        const uint4* rec_in, uint4* rec_out, uint32_t* err, cudaStream_t st,
                         float extra_scale = 1.0f);
 
 // The same from rows already normalised to BF16 (xbf[n][16]) into records.
 void launch_mlp_forward_bf16(const MlpDevice& d, const __nv_bfloat16* xbf, int n,
-                             const PD* pd_in, PD* pd_out, uint32_t* err, cudaStream_t st,
+                             const uint4* rec_in, uint4* rec_out, uint32_t* err, cudaStream_t st,
                              float extra_scale = 1.0f);
 
 // Reserves `want` rows of the process's training set (fewer when it is

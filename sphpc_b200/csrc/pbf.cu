@@ -4,8 +4,9 @@
 // neighbour loop visits the bucket of the particle in the reference's order
 // (for_each_neighbor).  Sums are FP32 (density with Kahan compensation);
 // the box clamp, the SDF lookup and the position update are FP64 on the
-// canonical double x* = x + d.  Particle records {x, d} are read with one
-// 256-bit load per neighbour.
+// canonical double x* = x + d of the particle's own record.  Neighbours are
+// read from the 16-byte records (fixed-point x* and a payload) with one
+// 128-bit load each; the pair difference is their exact integer difference.
 #include "kernels.cuh"
 
 namespace sphpc {
@@ -21,6 +22,17 @@ struct Pair {
 __device__ __forceinline__ void ld_rw(const PD* base, int i, float4& x, float4& d) {
   x = base[i].x;
   d = base[i].d;
+}
+
+// x*_p - x*_q from two 16-byte records: the wrapping integer difference is
+// exact, its conversion to FP32 rounds like any FP32 difference.
+__device__ __forceinline__ Pair pair_nr(const DevParams& P, const uint4 a, const uint4 b) {
+  Pair g;
+  g.dx = (float)(int)(a.x - b.x) * P.fx_inv;
+  g.dy = (float)(int)(a.y - b.y) * P.fx_inv;
+  g.dz = (float)(int)(a.z - b.z) * P.fx_inv;
+  g.r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
+  return g;
 }
 
 __device__ __forceinline__ Pair pair_geom(const float4 xp, const float4 dp, const float4 xq,
@@ -73,14 +85,11 @@ __global__ void __launch_bounds__(kBlock)
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   double err = 0.0;
   if (p < P.n) {
-    float4 xp, dp;
-    ld_pd(a.pd, p, xp, dp);
+    const uint4 rp = ld_nr(a.nr, p);
     float rho = P.W0m, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
     for_each_neighbor(V, p, [&](int q) {
-      float4 xq, dq;
-      ld_pd(a.pd, q, xq, dq);
-      const Pair g = pair_geom(xp, dp, xq, dq);
+      const Pair g = pair_nr(P, rp, ld_nr(a.nr, q));
       if (MODE != 2) {
         const float t = P.h2 - g.r2;
         const float w = t > 0.0f ? P.Wn_m * t * t * t : 0.0f;
@@ -109,7 +118,7 @@ __global__ void __launch_bounds__(kBlock)
       sC += sgx * sgx + sgy * sgy + sgz * sgz;
       sC *= P.inv_rho0_sq;
       const float lam = -C / (sC + P.lambda_eps);
-      st_pd(a.pd_out, p, xp, make_float4(dp.x, dp.y, dp.z, lam));
+      if (a.nr_out) a.nr_out[p] = make_uint4(rp.x, rp.y, rp.z, __float_as_uint(lam));
       if (a.lam) a.lam[p] = lam;
     }
     if (RESID) err = fmax((double)rho / (double)P.rho0 - 1.0, 0.0);
@@ -177,14 +186,14 @@ __global__ void __launch_bounds__(kBlock)
     sC += sgx * sgx + sgy * sgy + sgz * sgz;
     sC *= P.inv_rho0_sq;
     const float lam = -C / (sC + P.lambda_eps);
-    st_pd(a.pd_out, p, xp, make_float4(dp.x, dp.y, dp.z, lam));
+    const double xs = xstar_d(xp.x, dp.x), ys = xstar_d(xp.y, dp.y), zs = xstar_d(xp.z, dp.z);
+    a.nr_out[p] = make_nr(P, xs, ys, zs, lam);
     err = fmax((double)rho / (double)P.rho0 - 1.0, 0.0);
     if (p < limit) {
       const float inv_h = 1.0f / P.h;
       const float s_self = (sgx * sgx + sgy * sgy + sgz * sgz) * P.inv_rho0_sq;
       const float inv_cnt = cnt > 0 ? 1.0f / (float)cnt : 0.0f;
       const float sc = inv_h * inv_cnt;
-      const double xs = xstar_d(xp.x, dp.x), ys = xstar_d(xp.y, dp.y), zs = xstar_d(xp.z, dp.z);
       float sdf = 4.0f;
       if (P.has_sdf && xs > P.ob_min[0] && xs < P.ob_max[0] && ys > P.ob_min[1] &&
           ys < P.ob_max[1] && zs > P.ob_min[2] && zs < P.ob_max[2]) {
@@ -227,10 +236,10 @@ __global__ void __launch_bounds__(kBlock)
 // target[p] += s * lambda_p (lambda in d.w of the records) for p < limit:
 // the stiffness-weighted multiplier sum of a plain solve, the warm-start
 // network's training target.
-__global__ void k_accum_lambda(const PD* __restrict__ rec, float s, float* __restrict__ target,
+__global__ void k_accum_lambda(const uint4* __restrict__ rec, float s, float* __restrict__ target,
                                int limit) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < limit) target[p] += s * rec[p].d.w;
+  if (p < limit) target[p] += s * __uint_as_float(rec[p].w);
 }
 
 template <int MODE, int SCORR_N, bool SDF>
@@ -238,14 +247,14 @@ __global__ void __launch_bounds__(kBlock)
     k_position(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  float4 xp, dp;
-  ld_pd(a.pd, p, xp, dp);
-  const float lp = dp.w;
+  const uint4 rp = ld_nr(a.nr, p);
+  const float lp = nr_w(rp);
+  float4 xp, dp;  // own particle record, loaded ahead of the neighbour loop
+  if (MODE == 0) ld_pd(a.pd, p, xp, dp);
   float ax = 0.f, ay = 0.f, az = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    float4 xq, dq;
-    ld_pd(a.pd, q, xq, dq);
-    const Pair g = pair_geom(xp, dp, xq, dq);
+    const uint4 rq = ld_nr(a.nr, q);
+    const Pair g = pair_nr(P, rp, rq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float hm = P.h - r;
@@ -263,7 +272,7 @@ __global__ void __launch_bounds__(kBlock)
         for (int e = 0; e < P.scorr_n; ++e) sc *= ratio;
       }
     }
-    const float c = (lp + dq.w + sc) * delW * rinv;
+    const float c = (lp + nr_w(rq) + sc) * delW * rinv;
     ax += c * g.dx;
     ay += c * g.dy;
     az += c * g.dz;
@@ -283,9 +292,12 @@ __global__ void __launch_bounds__(kBlock)
   if (SDF) sdf_collide(P, xs, ys, zs);
   const double ex = __dsub_rn(xs, (double)xp.x), ey = __dsub_rn(ys, (double)xp.y),
                ez = __dsub_rn(zs, (double)xp.z);
-  st_pd(a.pd_out, p, xp,
-        make_float4(__double2float_rn(ex), __double2float_rn(ey), __double2float_rn(ez),
-                    a.rho[p]));
+  const float rho_p = a.rho[p];
+  const float4 dn = make_float4(__double2float_rn(ex), __double2float_rn(ey),
+                                __double2float_rn(ez), rho_p);
+  st_pd(a.pd_out, p, xp, dn);
+  // the record carries the canonical x* = x + d of what was just stored
+  a.nr_out[p] = make_nr(P, xstar_d(xp.x, dn.x), xstar_d(xp.y, dn.y), xstar_d(xp.z, dn.z), rho_p);
   if (a.last) {
     // UpdateVelocities, particles.c:814-837
     float vx = __double2float_rn(__ddiv_rn(ex, P.dt_d));
@@ -321,18 +333,16 @@ __global__ void __launch_bounds__(kBlock)
     k_color(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  float4 xp, dp;
-  ld_pd(a.pd, p, xp, dp);
+  const uint4 rp = ld_nr(a.nr, p);
   float cx = 0.f, cy = 0.f, cz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    float4 xq, dq;
-    ld_pd(a.pd, q, xq, dq);
-    const Pair g = pair_geom(xp, dp, xq, dq);
+    const uint4 rq = ld_nr(a.nr, q);
+    const Pair g = pair_nr(P, rp, rq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float t = P.h2 - r * r;
     const float grad = t > 0.0f ? P.DWPn * t * t * r : 0.0f;
-    const float c = grad * P.m / dq.w * rinv;
+    const float c = grad * P.m / nr_w(rq) * rinv;
     cx += c * g.dx;
     cy += c * g.dy;
     cz += c * g.dz;
@@ -358,22 +368,20 @@ __global__ void __launch_bounds__(kBlock)
     k_tension(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  float4 xp, dp;
-  ld_pd(a.pd, p, xp, dp);
+  const uint4 recp = ld_nr(a.nr, p);
   const float4 cp = __ldg(a.color + p);
-  const float rp = dp.w;
+  const float rp = nr_w(recp);
   const float kcoh = -20.0f * P.gamma * P.m * P.m;
   const float kcur = -P.gamma * P.m;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    float4 xq, dq;
-    ld_pd(a.pd, q, xq, dq);
-    const Pair g = pair_geom(xp, dp, xq, dq);
+    const uint4 rq = ld_nr(a.nr, q);
+    const Pair g = pair_nr(P, recp, rq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float4 cq = __ldg(a.color + q);
     const float coh = kcoh * cohesion(P, r) * rinv;
-    const float K = 2.0f * P.rho0 / (rp + dq.w);
+    const float K = 2.0f * P.rho0 / (rp + nr_w(rq));
     fx += K * (coh * g.dx + kcur * (cp.x - cq.x));
     fy += K * (coh * g.dy + kcur * (cp.y - cq.y));
     fz += K * (coh * g.dz + kcur * (cp.z - cq.z));
@@ -390,18 +398,16 @@ __global__ void __launch_bounds__(kBlock)
     k_xsph(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  float4 xp, dp;
-  ld_pd(a.pd, p, xp, dp);
+  const uint4 rp = ld_nr(a.nr, p);
   const float4 vp = __ldg(a.vel + p);
   float sx = 0.f, sy = 0.f, sz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    float4 xq, dq;
-    ld_pd(a.pd, q, xq, dq);
-    const Pair g = pair_geom(xp, dp, xq, dq);
+    const uint4 rq = ld_nr(a.nr, q);
+    const Pair g = pair_nr(P, rp, rq);
     // particles.c:439 evaluates x^2 + y^2 * z^2 (kept unless xsph_exact)
     const float rr = P.xsph_exact ? g.r2 : g.dx * g.dx + g.dy * g.dy * g.dz * g.dz;
     const float t = P.h2 - rr;
-    const float w = t > 0.0f ? P.Wn_m * t * t * t / dq.w : 0.0f;
+    const float w = t > 0.0f ? P.Wn_m * t * t * t / nr_w(rq) : 0.0f;
     const float4 vq = __ldg(a.vel + q);
     sx += (vq.x - vp.x) * w;
     sy += (vq.y - vp.y) * w;
@@ -409,26 +415,26 @@ __global__ void __launch_bounds__(kBlock)
   });
   a.vel_out[p] = make_float4(vp.x + P.c_xsph * sx, vp.y + P.c_xsph * sy,
                              vp.z + P.c_xsph * sz, 0.0f);
-  if (a.write_pos)
+  if (a.write_pos) {
+    float4 xp, dp;
+    ld_pd(a.pd, p, xp, dp);
     st_pd(a.pd_out, p,
           make_float4(__double2float_rn(xstar_d(xp.x, dp.x)),
                       __double2float_rn(xstar_d(xp.y, dp.y)),
                       __double2float_rn(xstar_d(xp.z, dp.z)), 0.0f),
-          make_float4(0.f, 0.f, 0.f, dp.w));
+          make_float4(0.f, 0.f, 0.f, nr_w(rp)));
+  }
 }
 
 __global__ void __launch_bounds__(kBlock)
     k_vorticity(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  float4 xp, dp;
-  ld_pd(a.pd, p, xp, dp);
+  const uint4 rp = ld_nr(a.nr, p);
   const float4 vp = __ldg(a.vel + p);
   float wx = 0.f, wy = 0.f, wz = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    float4 xq, dq;
-    ld_pd(a.pd, q, xq, dq);
-    const Pair g = pair_geom(xp, dp, xq, dq);
+    const Pair g = pair_nr(P, rp, ld_nr(a.nr, q));
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float hm = P.h - r;
@@ -447,13 +453,10 @@ __global__ void __launch_bounds__(kBlock)
     k_confinement(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  float4 xp, dp;
-  ld_pd(a.pd, p, xp, dp);
+  const uint4 rp = ld_nr(a.nr, p);
   float ex = 0.f, ey = 0.f, ez = 0.f;
   for_each_neighbor(V, p, [&](int q) {
-    float4 xq, dq;
-    ld_pd(a.pd, q, xq, dq);
-    const Pair g = pair_geom(xp, dp, xq, dq);
+    const Pair g = pair_nr(P, rp, ld_nr(a.nr, q));
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float hm = P.h - r;
@@ -472,12 +475,15 @@ __global__ void __launch_bounds__(kBlock)
   v.y += s * (nz * w.x - nx * w.z);
   v.z += s * (nx * w.y - ny * w.x);
   a.vel[p] = v;
-  if (a.write_pos)
+  if (a.write_pos) {
+    float4 xp, dp;
+    ld_pd(a.pd, p, xp, dp);
     st_pd(a.pd_out, p,
           make_float4(__double2float_rn(xstar_d(xp.x, dp.x)),
                       __double2float_rn(xstar_d(xp.y, dp.y)),
                       __double2float_rn(xstar_d(xp.z, dp.z)), 0.0f),
-          make_float4(0.f, 0.f, 0.f, dp.w));
+          make_float4(0.f, 0.f, 0.f, nr_w(rp)));
+  }
 }
 
 __global__ void __launch_bounds__(kBlock) k_gravity(const DevParams P, float4* vel) {
@@ -539,10 +545,24 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 __global__ void __launch_bounds__(kBlock)
-    k_pack_w(const DevParams P, PD* pd, const float* __restrict__ src) {
+    k_pack_w(const DevParams P, PD* pd, uint4* nr, const float* __restrict__ src) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  pd[p].d.w = src[p];
+  const float w = src[p];
+  if (pd) pd[p].d.w = w;
+  if (nr) nr[p].w = __float_as_uint(w);
+}
+
+// 16-byte records from the particle records: canonical x* = x + d and the
+// payload src[p] (d.w without src).
+__global__ void __launch_bounds__(kBlock)
+    k_make_nr(const DevParams P, const PD* __restrict__ pd, const float* __restrict__ src,
+              uint4* __restrict__ nr) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.n) return;
+  const float4 x = pd[p].x, d = pd[p].d;
+  nr[p] = make_nr(P, xstar_d(x.x, d.x), xstar_d(x.y, d.y), xstar_d(x.z, d.z),
+                  src ? src[p] : d.w);
 }
 
 __global__ void __launch_bounds__(kBlock)
@@ -583,7 +603,7 @@ void launch_features_bf16(const DevParams& P, const NbrView& V, const PassArgs& 
   k_features<false><<<grid_for(P.n), kBlock, 0, st>>>(P, V, a, nullptr, xbf, norm, P.n);
 }
 
-void launch_accum_lambda(const PD* rec, float s, float* target, int limit, cudaStream_t st) {
+void launch_accum_lambda(const uint4* rec, float s, float* target, int limit, cudaStream_t st) {
   if (limit > 0) k_accum_lambda<<<(limit + kBlock - 1) / kBlock, kBlock, 0, st>>>(rec, s, target, limit);
 }
 
@@ -638,8 +658,12 @@ void launch_update_velocities(const DevParams& P, const PD* pd, float4* vel, cud
 void launch_update_positions(const DevParams& P, PD* pd, cudaStream_t st) {
   k_update_positions<<<grid_for(P.n), kBlock, 0, st>>>(P, pd);
 }
-void launch_pack_w(const DevParams& P, PD* pd, const float* src, cudaStream_t st) {
-  k_pack_w<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, src);
+void launch_pack_w(const DevParams& P, PD* pd, uint4* nr, const float* src, cudaStream_t st) {
+  k_pack_w<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, nr, src);
+}
+void launch_make_nr(const DevParams& P, const PD* pd, const float* src, uint4* nr,
+                    cudaStream_t st) {
+  k_make_nr<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, src, nr);
 }
 void launch_collisions_double(const DevParams& P, double* x, double* y, double* z, int n,
                               cudaStream_t st) {

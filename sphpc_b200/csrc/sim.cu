@@ -86,7 +86,8 @@ class DeviceSim {
   bool nbr_valid = false;
 
   MlpState mlp{};
-  PD* pd_w = nullptr;            // third record buffer of the warm start
+  uint4 *nr = nullptr, *nr_alt = nullptr;  // 16-byte neighbour records (x* fixed point, payload)
+  uint4* nr_w = nullptr;         // third record buffer (warm start, feature export)
   int last_warm_rejected = 0;
   std::vector<double> trace;     // max density error at each evaluation of the step
   // training-set collection of the current step (collect_iters > 0)
@@ -127,7 +128,7 @@ class DeviceSim {
     dfree(nbr); dfree(xsa); dfree(cstart); dfree(ncount); dfree(gaps); dfree(small);
     dfree(resid); dfree(sort.keys_alt); dfree(sort.vals_alt); dfree(sort_aux); dfree(stage);
     mlp_release(mlp);
-    dfree(pd_w);
+    dfree(nr); dfree(nr_alt); dfree(nr_w);
     for (auto& p : pending) {
       cudaEventDestroy(p.a);
       cudaEventDestroy(p.b);
@@ -140,6 +141,7 @@ class DeviceSim {
   int alloc(int n_) {
     n = n_;
     SPHPC_RC(dalloc(&pd, n)); SPHPC_RC(dalloc(&pd_alt, n));
+    SPHPC_RC(dalloc(&nr, n)); SPHPC_RC(dalloc(&nr_alt, n));
     SPHPC_RC(dalloc(&vel, n)); SPHPC_RC(dalloc(&vel_alt, n));
     SPHPC_RC(dalloc(&color, n)); SPHPC_RC(dalloc(&omega, n)); SPHPC_RC(dalloc(&dp, n));
     SPHPC_RC(dalloc(&rho, n)); SPHPC_RC(dalloc(&lam, n));
@@ -292,7 +294,7 @@ class DeviceSim {
   int run_step(const DevParams& P, const Params& prm);
 
   int ensure_warm_buffers() {
-    if (!pd_w) SPHPC_RC(dalloc(&pd_w, n));
+    if (!nr_w) SPHPC_RC(dalloc(&nr_w, n));
     if (mlp.feat_cap < n) {
       if (mlp.feat) cudaFree(mlp.feat);
       mlp.feat = nullptr;
@@ -317,6 +319,14 @@ DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob
   P.mx = (1u << bx) - 1u;
   P.my = (1u << by) - 1u;
   P.hd = h;
+  {
+    // fixed-point records: 2^k units per length, as fine as keeps every
+    // neighbour difference (< 8h, far more than a step moves a pair) below
+    // 2^31 units, so the wrapping difference is the true one
+    const int k = 28 - (int)ceil(log2(h));
+    P.fx_scale = ldexp(1.0, k);
+    P.fx_inv = (float)ldexp(1.0, -k);
+  }
   P.h2d = h * h;
   P.h = (float)h;
   P.h2 = (float)(h * h);
@@ -423,7 +433,7 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
       ex.in1[1] = lam; ex.out1[1] = lam_alt;
     }
     const bool mv = move_vel || full;
-    launch_reorder(P, R, loc_by_id, pd, vel, pd_alt, vel_alt, xsa, cellp, predict, mv, &ex,
+    launch_reorder(P, R, loc_by_id, pd, vel, pd_alt, vel_alt, xsa, nr, cellp, predict, mv, &ex,
                    stream);
     launches += 1;
     std::swap(pd, pd_alt);
@@ -472,14 +482,16 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   last_warm = 0.0;
   last_warm_rejected = 0;
   trace.clear();
-  // The current positions are always the records in `pd`.  A density/lambda
-  // pass (A) reads pd and writes records with lambda in d.w; a position pass
-  // (B) reads such records and writes the new positions into pd.
-  auto pass_a = [&](PD* out, bool with_resid) -> int {
+  // The current positions are the particle records `pd` and the neighbour
+  // records `nr` (same x*).  A density/lambda pass (A) reads nr and writes
+  // records with lambda in the payload; a position pass (B) reads pd (own)
+  // and such records, and writes the new positions into pd_alt (then
+  // swapped into pd) and nr.
+  auto pass_a = [&](uint4* out, bool with_resid) -> int {
     Scope sc(this, "density_lambda");
     if (with_resid) SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
-    a.pd = pd;
-    a.pd_out = out;
+    a.nr = nr;
+    a.nr_out = out;
     a.lam = nullptr;
     launch_density_lambda(P, V, a, 0, with_resid, stream);
     launches += 1;
@@ -494,18 +506,21 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     if (trace.size() < 16) trace.push_back(max_err);
     return SPHPC_OK;
   };
-  auto pass_b = [&](const PD* in, float stiffness, bool last) {
+  auto pass_b = [&](const uint4* in, float stiffness, bool last) {
     Scope sc(this, "position");
-    a.pd = in;
-    a.pd_out = pd;
+    a.pd = pd;
+    a.pd_out = pd_alt;
+    a.nr = in;
+    a.nr_out = nr;
     a.stiffness = stiffness;
     a.last = last ? 1 : 0;
     launch_position(P, V, a, 0, stream);
     launches += 1;
+    std::swap(pd, pd_alt);
   };
   int iters = 0, plain = 0;
   bool converged = false;
-  const PD* ready = nullptr;  // records with lambda for the next B (its A already run)
+  const uint4* ready = nullptr;  // records with lambda for the next B (its A already run)
   if (collect) {
     // the first A also writes the features of the (predicted) state; the
     // target accumulates s_k * lambda_k over the fixed iterations
@@ -513,10 +528,10 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     SPHPC_CK(cudaMemsetAsync(collect_target, 0, sizeof(float) * (size_t)collect_rows, stream));
     SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
     a.pd = pd;
-    a.pd_out = pd_alt;
+    a.nr_out = nr_alt;
     launch_features(P, V, a, collect_feat, (int)collect_rows, stream);
     launches += 1;
-    ready = pd_alt;
+    ready = nr_alt;
   } else if (warm) {
     SPHPC_RC(ensure_warm_buffers());
     double err0 = 0.0, err1 = 0.0;
@@ -524,7 +539,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       Scope sc(this, "mlp_features");
       SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
       a.pd = pd;
-      a.pd_out = pd_alt;
+      a.nr_out = nr_alt;
       launch_features_bf16(P, V, a, reinterpret_cast<__nv_bfloat16*>(mlp.feat), mlp.dev.norm,
                            stream);
       launches += 1;
@@ -536,35 +551,38 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       {
         Scope sc(this, "mlp_forward");
         launch_mlp_forward_bf16(mlp.dev, reinterpret_cast<const __nv_bfloat16*>(mlp.feat), n,
-                                pd_alt, pd_w, err(), stream, (float)solver.warm_start_scale);
+                                nr_alt, nr_w, err(), stream, (float)solver.warm_start_scale);
         launches += 1;
       }
-      // the network's multipliers, applied at full stiffness in one pass
-      pass_b(pd_w, 1.0f, false);
+      // the network's multipliers, applied at full stiffness in one pass;
+      // pd_alt keeps the predicted positions until the gate has decided
+      pass_b(nr_w, 1.0f, false);
       ++iters;
       last_warm = 1.0;
-      SPHPC_RC(pass_a(pd_w, true));
+      SPHPC_RC(pass_a(nr_w, true));
       SPHPC_RC(read_resid(err1));
       if (adaptive && err1 <= tol) {
         converged = true;
       } else if (solver.warm_start_gate && !(err1 < err0)) {
         // FP64 residual gate: the warm pass did not lower the maximum density
         // error, so it is discarded and the plain solve restarts from the
-        // predicted positions (pd_alt still holds them with lambda_0)
+        // predicted positions (pd_alt and nr_alt still hold them, the latter
+        // with lambda_0)
         last_warm_rejected = 1;
-        ready = pd_alt;
+        std::swap(pd, pd_alt);
+        ready = nr_alt;
       } else {
-        ready = pd_w;
+        ready = nr_w;
         plain = 1;  // the warm pass takes the place of plain substep 0
       }
     }
   }
   const int first_plain = plain;
   while (!converged && plain - first_plain < plain_cap) {
-    const PD* src = ready;
+    const uint4* src = ready;
     ready = nullptr;
     if (!src) {
-      SPHPC_RC(pass_a(pd_alt, adaptive));
+      SPHPC_RC(pass_a(nr_alt, adaptive));
       if (adaptive) {
         double e = 0.0;
         SPHPC_RC(read_resid(e));
@@ -573,7 +591,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
           break;
         }
       }
-      src = pd_alt;
+      src = nr_alt;
     }
     const float stiff = stiffness_of(solver.stiffness_k, plain);
     if (collect) {
@@ -591,7 +609,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     // freshest density
     Scope sc(this, "velocity");
     if (converged || iters == 0) {
-      launch_pack_w(P, pd, rho, stream);
+      launch_pack_w(P, nullptr, nr, rho, stream);
       launches += 1;
     }
     launch_update_velocities(P, pd, vel, stream);
@@ -599,10 +617,12 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   }
   last_iterations = iters;
   last_converged = converged ? 1 : 0;
-  // post-solve passes (simulation.c:93-106); the last one writes x = x*,
-  // d = 0 (UpdatePositions) into pd_alt
+  // post-solve passes (simulation.c:93-106) on the records nr (payload: the
+  // density); the last one writes x = x*, d = 0 (UpdatePositions) into pd_alt
   a.pd = pd;
   a.pd_out = pd_alt;
+  a.nr = nr;
+  a.nr_out = nullptr;
   if (solver.surface_tension) {
     Scope sc(this, "surface_tension");
     a.color = color;
@@ -1057,8 +1077,9 @@ int ComputeDensities(struct Particles* particles, const struct Params* params,
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
+  launch_make_nr(P, s->pd, nullptr, s->nr, s->stream);
   PassArgs a{};
-  a.pd = s->pd;
+  a.nr = s->nr;
   a.rho = s->rho;
   a.resid = s->resid;
   SPHPC_CK(cudaMemsetAsync(s->resid, 0, 2 * sizeof(double), s->stream));
@@ -1072,13 +1093,13 @@ int ComputeLambda(struct Particles* particles, const struct Params* params,
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
+  launch_make_nr(P, s->pd, nullptr, s->nr, s->stream);
   PassArgs a{};
-  a.pd = s->pd;
-  a.pd_out = s->pd_alt;
+  a.nr = s->nr;
   a.rho = s->rho;
   a.lam = s->lam;
   launch_density_lambda(P, s->view(), a, 2, false, s->stream);
-  std::swap(s->pd, s->pd_alt);
+  launch_pack_w(P, s->pd, nullptr, s->lam, s->stream);
   SPHPC_LAUNCH_DONE();
 }
 
@@ -1088,9 +1109,11 @@ int UpdateDPs(struct Particles* particles, const struct Params* params,
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
-  launch_pack_w(P, s->pd, s->lam, s->stream);
+  launch_pack_w(P, s->pd, nullptr, s->lam, s->stream);
+  launch_make_nr(P, s->pd, s->lam, s->nr, s->stream);
   PassArgs a{};
   a.pd = s->pd;
+  a.nr = s->nr;
   a.dp = s->dp;
   a.rho = s->rho;
   a.stiffness = stiffness_of(s->solver.stiffness_k, substep);
@@ -1123,9 +1146,11 @@ int ComputeSurfaceTension(struct Particles* particles, const struct Params* para
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
-  launch_pack_w(P, s->pd, s->rho, s->stream);
+  launch_pack_w(P, s->pd, nullptr, s->rho, s->stream);
+  launch_make_nr(P, s->pd, s->rho, s->nr, s->stream);
   PassArgs a{};
   a.pd = s->pd;
+  a.nr = s->nr;
   a.color = s->color;
   a.vel = s->vel;
   launch_color(P, s->view(), a, s->stream);
@@ -1139,9 +1164,11 @@ int ApplyViscosity(struct Particles* particles, const struct Params* params,
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
-  launch_pack_w(P, s->pd, s->rho, s->stream);
+  launch_pack_w(P, s->pd, nullptr, s->rho, s->stream);
+  launch_make_nr(P, s->pd, s->rho, s->nr, s->stream);
   PassArgs a{};
   a.pd = s->pd;
+  a.nr = s->nr;
   a.vel = s->vel;
   a.vel_out = s->vel_alt;
   launch_xsph(P, s->view(), a, s->stream);
@@ -1155,8 +1182,10 @@ int ComputeVorticity(struct Particles* particles, const struct Params* params,
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
+  launch_make_nr(P, s->pd, nullptr, s->nr, s->stream);
   PassArgs a{};
   a.pd = s->pd;
+  a.nr = s->nr;
   a.vel = s->vel;
   a.omega = s->omega;
   launch_vorticity(P, s->view(), a, s->stream);
@@ -1169,8 +1198,10 @@ int ApplyVorticityConfinement(struct Particles* particles, const struct Params* 
   SPHPC_STAGE_BEGIN(particles, params);
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
+  launch_make_nr(P, s->pd, nullptr, s->nr, s->stream);
   PassArgs a{};
   a.pd = s->pd;
+  a.nr = s->nr;
   a.vel = s->vel;
   a.omega = s->omega;
   launch_confinement(P, s->view(), a, s->stream);
@@ -1263,7 +1294,7 @@ int sphpc_mlp_features(struct Particles* particles, const struct Params* params,
   const DevParams P = s->params(*params, boundary_global, obstacle);
   PassArgs a{};
   a.pd = s->pd;
-  a.pd_out = s->pd_w;
+  a.nr_out = s->nr_w;
   a.rho = s->rho_alt ? s->rho_alt : s->rho;
   a.vel = s->vel;
   a.resid = s->resid;

@@ -8,6 +8,11 @@
 //                    (.w carries lambda after the density/lambda pass and the
 //                    density after the position pass).  A neighbour's record
 //                    is one 256-bit load.
+//   nr[n]    uint4   16-byte neighbour record {X, Y, Z, w}: x* in fixed
+//                    point (2^-k units, wrapping mod 2^32, so the difference
+//                    of two records is exact for any box) and a payload (w:
+//                    lambda after a density/lambda pass, the density after
+//                    a position pass).  Neighbour sums gather only these.
 //   xsa[n]   float4  x* as absolute FP32 (neighbour-build candidate test)
 //   vel[n]   float4  v
 //   ids[n]   u32     original particle index of each slot
@@ -21,9 +26,10 @@
 //
 // The canonical predicted position is the double fl64(x + d): the hash, the
 // neighbour test, the box clamp and the SDF lookup are evaluated on it in
-// FP64 exactly as the reference evaluates its double x_star; pair
-// differences inside the neighbour sums are (x_p - x_q) + (d_p - d_q) in
-// FP32, which keeps relative precision at any box size.
+// FP64 exactly as the reference evaluates its double x_star.  Pair
+// differences inside the neighbour sums are integer differences of the
+// fixed-point records (2^-k units, k = 28 - ceil(log2 h): 7.5e-9 for h = 2)
+// converted to FP32, so their precision does not depend on the box size.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -51,6 +57,17 @@ __device__ __forceinline__ void st_pd(PD* base, int i, const float4 x, const flo
                : "memory");
 }
 
+// 16-byte neighbour record: fixed-point x* and a payload, one 128-bit load.
+__device__ __forceinline__ uint4 ld_nr(const uint4* __restrict__ base, int i) {
+  uint4 r;
+  asm("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(base + i));
+  return r;
+}
+
+__device__ __forceinline__ float nr_w(const uint4 r) { return __uint_as_float(r.w); }
+
 // Error bits raised by kernels (host reads them back).
 enum : uint32_t {
   kErrSortSpin = 1u << 1,          // radix-sort look-back wait gave up
@@ -66,6 +83,8 @@ struct DevParams {
   int bx, by;           // packed-cell bit widths of x and y
   uint32_t mx, my;      // masks for cx and cy
   double hd;            // smoothing radius (double)
+  double fx_scale;      // 2^k: fixed-point units per length of the records
+  float fx_inv;         // 2^-k
   double h2d;
   float h, h2;
   float rmin;           // r floor 1e-4 h (particles.c:636)
@@ -142,6 +161,16 @@ __device__ __forceinline__ double clamp_axis(double x, double lo, double hi,
   if (x < lo) return lo;
   if (x >= hi) return hi_eps;
   return x;
+}
+
+// Fixed-point coordinate of a double position (round to nearest, mod 2^32).
+__device__ __forceinline__ uint32_t fx_of(const DevParams& P, double x) {
+  return (uint32_t)(unsigned long long)__double2ll_rn(__dmul_rn(x, P.fx_scale));
+}
+
+__device__ __forceinline__ uint4 make_nr(const DevParams& P, double x, double y, double z,
+                                         float w) {
+  return make_uint4(fx_of(P, x), fx_of(P, y), fx_of(P, z), __float_as_uint(w));
 }
 
 // HashVal, neighbors.c:79-98, per axis: floor(x / spacing) in FP64.
