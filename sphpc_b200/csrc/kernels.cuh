@@ -110,7 +110,7 @@ void launch_xsph(const DevParams& P, const NbrView& V, const PassArgs& a, cudaSt
 // ComputeVorticity (:207-283) from vel; ApplyVorticityConfinement (:285-381)
 // updates vel in place.
 void launch_vorticity(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st);
-void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a,
+void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a, bool omega_in_nr,
                         cudaStream_t st);
 // Pointwise steps.
 void launch_gravity(const DevParams& P, float4* vel, cudaStream_t st);

@@ -17,6 +17,9 @@ struct Pair {
   float dx, dy, dz, r2;
 };
 
+// neighbours whose list entries and records are fetched together
+constexpr int kNbrBatch = 4;
+
 // x*_p - x*_q as (x_p - x_q) + (d_p - d_q): exact in the first term for any
 // box size, so the FP32 pair geometry keeps its relative precision.
 __device__ __forceinline__ void ld_rw(const PD* base, int i, float4& x, float4& d) {
@@ -88,8 +91,8 @@ __global__ void __launch_bounds__(kBlock)
     const uint4 rp = ld_nr(a.nr, p);
     float rho = P.W0m, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
-    for_each_neighbor(V, p, [&](int q) {
-      const Pair g = pair_nr(P, rp, ld_nr(a.nr, q));
+    for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int, const uint4 rq) {
+      const Pair g = pair_nr(P, rp, rq);
       if (MODE != 2) {
         const float t = P.h2 - g.r2;
         const float w = t > 0.0f ? P.Wn_m * t * t * t : 0.0f;
@@ -152,9 +155,7 @@ __global__ void __launch_bounds__(kBlock)
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
     float ox = 0.f, oy = 0.f, oz = 0.f, ux = 0.f, uy = 0.f, uz = 0.f, rmin2 = P.h2;
     int cnt = 0;
-    for_each_neighbor(V, p, [&](int q) {
-      float4 xq, dq;
-      ld_pd(a.pd, q, xq, dq);
+    for_each_neighbor_pd<kNbrBatch>(V, a.pd, p, [&](int, const float4 xq, const float4 dq) {
       const Pair g = pair_geom(xp, dp, xq, dq);
       const float t = P.h2 - g.r2;
       const float w = t > 0.0f ? P.Wn_m * t * t * t : 0.0f;
@@ -252,8 +253,7 @@ __global__ void __launch_bounds__(kBlock)
   float4 xp, dp;  // own particle record, loaded ahead of the neighbour loop
   if (MODE == 0) ld_pd(a.pd, p, xp, dp);
   float ax = 0.f, ay = 0.f, az = 0.f;
-  for_each_neighbor(V, p, [&](int q) {
-    const uint4 rq = ld_nr(a.nr, q);
+  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int, const uint4 rq) {
     const Pair g = pair_nr(P, rp, rq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
@@ -335,8 +335,7 @@ __global__ void __launch_bounds__(kBlock)
   if (p >= P.n) return;
   const uint4 rp = ld_nr(a.nr, p);
   float cx = 0.f, cy = 0.f, cz = 0.f;
-  for_each_neighbor(V, p, [&](int q) {
-    const uint4 rq = ld_nr(a.nr, q);
+  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int, const uint4 rq) {
     const Pair g = pair_nr(P, rp, rq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
@@ -374,8 +373,7 @@ __global__ void __launch_bounds__(kBlock)
   const float kcoh = -20.0f * P.gamma * P.m * P.m;
   const float kcur = -P.gamma * P.m;
   float fx = 0.f, fy = 0.f, fz = 0.f;
-  for_each_neighbor(V, p, [&](int q) {
-    const uint4 rq = ld_nr(a.nr, q);
+  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int q, const uint4 rq) {
     const Pair g = pair_nr(P, recp, rq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
@@ -401,14 +399,13 @@ __global__ void __launch_bounds__(kBlock)
   const uint4 rp = ld_nr(a.nr, p);
   const float4 vp = __ldg(a.vel + p);
   float sx = 0.f, sy = 0.f, sz = 0.f;
-  for_each_neighbor(V, p, [&](int q) {
-    const uint4 rq = ld_nr(a.nr, q);
+  for_each_neighbor_nr2<kNbrBatch>(V, a.nr, a.vel, p,
+                                   [&](int, const uint4 rq, const float4 vq) {
     const Pair g = pair_nr(P, rp, rq);
     // particles.c:439 evaluates x^2 + y^2 * z^2 (kept unless xsph_exact)
     const float rr = P.xsph_exact ? g.r2 : g.dx * g.dx + g.dy * g.dy * g.dz * g.dz;
     const float t = P.h2 - rr;
     const float w = t > 0.0f ? P.Wn_m * t * t * t / nr_w(rq) : 0.0f;
-    const float4 vq = __ldg(a.vel + q);
     sx += (vq.x - vp.x) * w;
     sy += (vq.y - vp.y) * w;
     sz += (vq.z - vp.z) * w;
@@ -426,6 +423,8 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+// With nr_out, also the records {X, |omega|} the confinement pass gathers
+// (one 16-byte load per neighbour instead of a record and omega[q]).
 __global__ void __launch_bounds__(kBlock)
     k_vorticity(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -433,8 +432,8 @@ __global__ void __launch_bounds__(kBlock)
   const uint4 rp = ld_nr(a.nr, p);
   const float4 vp = __ldg(a.vel + p);
   float wx = 0.f, wy = 0.f, wz = 0.f;
-  for_each_neighbor(V, p, [&](int q) {
-    const Pair g = pair_nr(P, rp, ld_nr(a.nr, q));
+  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int q, const uint4 rq) {
+    const Pair g = pair_nr(P, rp, rq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float hm = P.h - r;
@@ -446,21 +445,26 @@ __global__ void __launch_bounds__(kBlock)
     wy += uz * gx - ux * gz;
     wz += ux * gy - uy * gx;
   });
-  a.omega[p] = make_float4(wx, wy, wz, sqrtf(wx * wx + wy * wy + wz * wz));
+  const float wm = sqrtf(wx * wx + wy * wy + wz * wz);
+  a.omega[p] = make_float4(wx, wy, wz, wm);
+  if (a.nr_out) a.nr_out[p] = make_uint4(rp.x, rp.y, rp.z, __float_as_uint(wm));
 }
 
+// OW: a.nr carries |omega| as its payload (the vorticity pass's records);
+// otherwise |omega_q| comes from omega[q].w.
+template <bool OW>
 __global__ void __launch_bounds__(kBlock)
     k_confinement(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   const uint4 rp = ld_nr(a.nr, p);
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  for_each_neighbor(V, p, [&](int q) {
-    const Pair g = pair_nr(P, rp, ld_nr(a.nr, q));
+  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int q, const uint4 rq) {
+    const Pair g = pair_nr(P, rp, rq);
     float r, rinv;
     floored_r(P, g.r2, r, rinv);
     const float hm = P.h - r;
-    const float wq = __ldg(a.omega + q).w;
+    const float wq = OW ? nr_w(rq) : __ldg(a.omega + q).w;
     const float c = hm > 0.0f ? P.DWn * hm * hm * rinv * wq : 0.0f;
     ex += c * g.dx;
     ey += c * g.dy;
@@ -482,7 +486,7 @@ __global__ void __launch_bounds__(kBlock)
           make_float4(__double2float_rn(xstar_d(xp.x, dp.x)),
                       __double2float_rn(xstar_d(xp.y, dp.y)),
                       __double2float_rn(xstar_d(xp.z, dp.z)), 0.0f),
-          make_float4(0.f, 0.f, 0.f, nr_w(rp)));
+          make_float4(0.f, 0.f, 0.f, OW ? 0.0f : nr_w(rp)));
   }
 }
 
@@ -642,9 +646,10 @@ void launch_xsph(const DevParams& P, const NbrView& V, const PassArgs& a, cudaSt
 void launch_vorticity(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
   k_vorticity<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
 }
-void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a,
+void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a, bool omega_in_nr,
                         cudaStream_t st) {
-  k_confinement<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
+  if (omega_in_nr) k_confinement<true><<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
+  else k_confinement<false><<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
 }
 void launch_gravity(const DevParams& P, float4* vel, cudaStream_t st) {
   k_gravity<<<grid_for(P.n), kBlock, 0, st>>>(P, vel);

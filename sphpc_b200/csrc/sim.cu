@@ -641,12 +641,17 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   }
   if (solver.vorticity) {
     Scope sc(this, "vorticity");
+    // the vorticity pass also writes the records {X, |omega|} (into nr_alt)
+    // that the confinement pass gathers
     a.vel = vel_alt;
     a.omega = omega;
+    a.nr_out = nr_alt;
     a.write_pos = 0;
     launch_vorticity(P, V, a, stream);
+    a.nr = nr_alt;
+    a.nr_out = nullptr;
     a.write_pos = 1;
-    launch_confinement(P, V, a, stream);
+    launch_confinement(P, V, a, true, stream);
     launches += 2;
   }
   std::swap(vel, vel_alt);
@@ -1204,7 +1209,7 @@ int ApplyVorticityConfinement(struct Particles* particles, const struct Params* 
   a.nr = s->nr;
   a.vel = s->vel;
   a.omega = s->omega;
-  launch_confinement(P, s->view(), a, s->stream);
+  launch_confinement(P, s->view(), a, false, s->stream);
   SPHPC_LAUNCH_DONE();
 }
 

@@ -148,6 +148,74 @@ __device__ __forceinline__ void for_each_neighbor(const NbrView& v, int p, F&& f
   for (int j = 0; j < cnt; ++j) f((int)__ldg(lst + (size_t)j * v.n));
 }
 
+// The same visit with each neighbour's 16-byte record loaded for f(q, rq):
+// list entries and records are fetched in batches of B (B list loads, then
+// B record loads, then the B bodies), so a thread keeps B gathers in flight
+// instead of one dependent pair.  Batch slots past the count load the
+// particle's own record and are skipped.
+template <int B, class F>
+__device__ __forceinline__ void for_each_neighbor_nr(const NbrView& v, const uint4* __restrict__ nr,
+                                                     int p, F&& f) {
+  const int cnt = (int)__ldg(v.ncount + p);
+  const uint32_t* lst = v.nbr + p;
+  for (int j0 = 0; j0 < cnt; j0 += B) {
+    int q[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) q[u] = j0 + u < cnt ? (int)__ldg(lst + (size_t)(j0 + u) * v.n) : p;
+    uint4 r[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) r[u] = ld_nr(nr, q[u]);
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (j0 + u < cnt) f(q[u], r[u]);
+  }
+}
+
+// The same with a second per-neighbour array (velocity, colour) fetched in
+// the same batch: f(q, rq, eq).
+template <int B, class F>
+__device__ __forceinline__ void for_each_neighbor_nr2(const NbrView& v,
+                                                      const uint4* __restrict__ nr,
+                                                      const float4* __restrict__ extra, int p,
+                                                      F&& f) {
+  const int cnt = (int)__ldg(v.ncount + p);
+  const uint32_t* lst = v.nbr + p;
+  for (int j0 = 0; j0 < cnt; j0 += B) {
+    int q[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) q[u] = j0 + u < cnt ? (int)__ldg(lst + (size_t)(j0 + u) * v.n) : p;
+    uint4 r[B];
+    float4 e[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      r[u] = ld_nr(nr, q[u]);
+      e[u] = __ldg(extra + q[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (j0 + u < cnt) f(q[u], r[u], e[u]);
+  }
+}
+
+// Batched visit over the 32-byte particle records: f(q, xq, dq).
+template <int B, class F>
+__device__ __forceinline__ void for_each_neighbor_pd(const NbrView& v, const PD* __restrict__ pd,
+                                                     int p, F&& f) {
+  const int cnt = (int)__ldg(v.ncount + p);
+  const uint32_t* lst = v.nbr + p;
+  for (int j0 = 0; j0 < cnt; j0 += B) {
+    int q[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) q[u] = j0 + u < cnt ? (int)__ldg(lst + (size_t)(j0 + u) * v.n) : p;
+    float4 x[B], d[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) ld_pd(pd, q[u], x[u], d[u]);
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (j0 + u < cnt) f(q[u], x[u], d[u]);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Canonical double predicted position and the reference's box clamp.
 // ---------------------------------------------------------------------------
