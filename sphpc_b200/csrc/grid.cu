@@ -280,22 +280,35 @@ __global__ void __launch_bounds__(kBuildBlock, 10)
         const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
         const int b = (int)__ldg(V.cstart + rk + xlo);
         const int e = (int)__ldg(V.cstart + rk + xhi + 1);
-        for (int j = b; j < e; j += 4) {
+        // self can only appear in the particle's own row
+        const bool self_row = dz == 0 && dy == 0;
+        int j = b;
+        for (; j + 4 <= e; j += 4) {
           float r2f[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            const float4 q = j + u < e ? __ldg(xsa + j + u) : make_float4(3e30f, 0.f, 0.f, 0.f);
+            const float4 q = __ldg(xsa + j + u);
             const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
             r2f[u] = fx * fx + fy * fy + fz * fz;
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
+            if (r2f[u] > c.h2hi) continue;
             const int jj = j + u;
-            if (jj >= e || jj == p || r2f[u] > c.h2hi) continue;
+            if (self_row && jj == p) continue;
             if (r2f[u] >= c.h2lo && !exact_neighbor(c, pd, jj)) continue;
             out[(size_t)count * stride] = (uint32_t)jj;
             if (++count == kMaxNeighbors) goto done;
           }
+        }
+        for (; j < e; ++j) {
+          const float4 q = __ldg(xsa + j);
+          const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
+          const float r2 = fx * fx + fy * fy + fz * fz;
+          if (r2 > c.h2hi || (self_row && j == p)) continue;
+          if (r2 >= c.h2lo && !exact_neighbor(c, pd, j)) continue;
+          out[(size_t)count * stride] = (uint32_t)j;
+          if (++count == kMaxNeighbors) goto done;
         }
       }
     }
