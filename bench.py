@@ -424,7 +424,8 @@ def run_e2e(sim, args, dist, world, n):
     d2h = args.steps * 72 + frames * 8 * len(frame_fields) * n + 8 * len(out_fields) * n
     return {"value": world * n * args.steps / dt, "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-            "host_memory": "pageable (the reference's calloc'd arrays)"}
+            "host_memory": "the reference's calloc'd arrays, page-locked in place by the "
+                           "library (cudaHostRegister at enter_data)"}
 
 
 def main():

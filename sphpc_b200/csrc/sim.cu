@@ -83,6 +83,9 @@ class DeviceSim {
   SortScratch sort{};
   uint32_t* sort_aux = nullptr;
   double* stage = nullptr;  // 20 * n doubles for host transfers
+  // host arrays of the particle set page-locked by enter_data (so that the
+  // transfers run at full link speed); released in release()
+  std::vector<void*> pinned;
   bool nbr_valid = false;
 
   MlpState mlp{};
@@ -128,6 +131,8 @@ class DeviceSim {
     dfree(nbr); dfree(xsa); dfree(cstart); dfree(ncount); dfree(gaps); dfree(small);
     dfree(resid); dfree(sort.keys_alt); dfree(sort.vals_alt); dfree(sort_aux); dfree(stage);
     mlp_release(mlp);
+    for (void* h : pinned) cudaHostUnregister(h);
+    pinned.clear();
     dfree(nr); dfree(nr_alt); dfree(nr_w);
     for (auto& p : pending) {
       cudaEventDestroy(p.a);
@@ -680,28 +685,54 @@ static DeviceSim* find_sim(const Particles* p) {
 
 // ---- host <-> device transfers ----
 
+// Gathers the requested fields (mask bit k: field k of struct Particles'
+// FP64 arrays) into stage[k][id], id = original particle index.
 __global__ void k_download(int n, const uint32_t* __restrict__ ids, const PD* __restrict__ pd,
                            const float4* __restrict__ vel,
                            const float4* __restrict__ dp, const float4* __restrict__ omega,
                            const float4* __restrict__ color, const float* __restrict__ rho,
-                           const float* __restrict__ lam, double* __restrict__ out) {
+                           const float* __restrict__ lam, unsigned mask,
+                           double* __restrict__ out) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const size_t N = (size_t)n;
   const uint32_t id = ids[p];
-  const float4 x = pd[p].x;
-  const float4 d = pd[p].d;
-  const float4 v = vel[p], q = dp[p], w = omega[p], c = color[p];
-  out[0 * N + id] = xstar_d(x.x, d.x);
-  out[1 * N + id] = xstar_d(x.y, d.y);
-  out[2 * N + id] = xstar_d(x.z, d.z);
-  out[3 * N + id] = x.x; out[4 * N + id] = x.y; out[5 * N + id] = x.z;
-  out[6 * N + id] = v.x; out[7 * N + id] = v.y; out[8 * N + id] = v.z;
-  out[9 * N + id] = q.x; out[10 * N + id] = q.y; out[11 * N + id] = q.z;
-  out[12 * N + id] = w.x; out[13 * N + id] = w.y; out[14 * N + id] = w.z;
-  out[15 * N + id] = c.x; out[16 * N + id] = c.y; out[17 * N + id] = c.z;
-  out[18 * N + id] = rho[p];
-  out[19 * N + id] = lam[p];
+  if (mask & 0x3Fu) {
+    const float4 x = pd[p].x;
+    const float4 d = pd[p].d;
+    if (mask & 1u) out[0 * N + id] = xstar_d(x.x, d.x);
+    if (mask & 2u) out[1 * N + id] = xstar_d(x.y, d.y);
+    if (mask & 4u) out[2 * N + id] = xstar_d(x.z, d.z);
+    if (mask & 8u) out[3 * N + id] = x.x;
+    if (mask & 16u) out[4 * N + id] = x.y;
+    if (mask & 32u) out[5 * N + id] = x.z;
+  }
+  if (mask & (7u << 6)) {
+    const float4 v = vel[p];
+    if (mask & (1u << 6)) out[6 * N + id] = v.x;
+    if (mask & (1u << 7)) out[7 * N + id] = v.y;
+    if (mask & (1u << 8)) out[8 * N + id] = v.z;
+  }
+  if (mask & (7u << 9)) {
+    const float4 q = dp[p];
+    if (mask & (1u << 9)) out[9 * N + id] = q.x;
+    if (mask & (1u << 10)) out[10 * N + id] = q.y;
+    if (mask & (1u << 11)) out[11 * N + id] = q.z;
+  }
+  if (mask & (7u << 12)) {
+    const float4 w = omega[p];
+    if (mask & (1u << 12)) out[12 * N + id] = w.x;
+    if (mask & (1u << 13)) out[13 * N + id] = w.y;
+    if (mask & (1u << 14)) out[14 * N + id] = w.z;
+  }
+  if (mask & (7u << 15)) {
+    const float4 c = color[p];
+    if (mask & (1u << 15)) out[15 * N + id] = c.x;
+    if (mask & (1u << 16)) out[16 * N + id] = c.y;
+    if (mask & (1u << 17)) out[17 * N + id] = c.z;
+  }
+  if (mask & (1u << 18)) out[18 * N + id] = rho[p];
+  if (mask & (1u << 19)) out[19 * N + id] = lam[p];
 }
 
 __global__ void k_upload(int n, const uint32_t* __restrict__ ids, const double* __restrict__ in,
@@ -781,6 +812,26 @@ static int enter_data(Particles* particles, const Params* params, DeviceSim** ou
   s->mass = particles->rest_mass;
   int rc = s->alloc(particles->local_count);
   if (!rc) {
+    // Page-lock the large host arrays in place: the reference's calloc'd
+    // arrays stay the caller's, only their transfers get faster.  Arrays
+    // below 64 MB may share pages with other allocations and are left
+    // pageable, as is any array the driver refuses to register.
+    const size_t bytes = sizeof(double) * (size_t)particles->max_local;
+    if (bytes >= ((size_t)64 << 20)) {
+      double* fields[20] = {particles->x_star, particles->y_star, particles->z_star, particles->x,
+                            particles->y, particles->z, particles->v_x, particles->v_y,
+                            particles->v_z, particles->dp_x, particles->dp_y, particles->dp_z,
+                            particles->w_x, particles->w_y, particles->w_z, particles->color_x,
+                            particles->color_y, particles->color_z, particles->density,
+                            particles->lambda};
+      for (double* f : fields) {
+        if (!f) continue;
+        if (cudaHostRegister(f, bytes, cudaHostRegisterDefault) == cudaSuccess)
+          s->pinned.push_back(f);
+        else
+          cudaGetLastError();
+      }
+    }
     k_iota<<<grid_for(s->n), kBlock, 0, s->stream>>>(s->ids, s->n);
     {
       std::lock_guard<std::mutex> lk(g_mu);
@@ -861,19 +912,24 @@ int sphpc_update_host_fields(struct Particles* p, unsigned int field_mask) {
   SPHPC_SIM(s, p);
   SPHPC_RC(s->ensure_stage());
   const int n = s->n;
-  k_download<<<grid_for(n), kBlock, 0, s->stream>>>(n, s->ids, s->pd, s->vel, s->dp,
-                                                    s->omega, s->color, s->rho, s->lam,
-                                                    s->stage);
-  SPHPC_CK(cudaGetLastError());
   double* fields[20] = {p->x_star, p->y_star, p->z_star, p->x, p->y, p->z, p->v_x, p->v_y,
                         p->v_z, p->dp_x, p->dp_y, p->dp_z, p->w_x, p->w_y, p->w_z,
                         p->color_x, p->color_y, p->color_z, p->density, p->lambda};
+  unsigned mask = 0;
+  for (int k = 0; k < 20; ++k)
+    if (fields[k] && (field_mask & (1u << k))) mask |= 1u << k;
+  k_download<<<grid_for(n), kBlock, 0, s->stream>>>(n, s->ids, s->pd, s->vel, s->dp,
+                                                    s->omega, s->color, s->rho, s->lam, mask,
+                                                    s->stage);
+  SPHPC_CK(cudaGetLastError());
   for (int k = 0; k < 20; ++k)
     if (fields[k] && (field_mask & (1u << k)))
       SPHPC_CK(cudaMemcpyAsync(fields[k], s->stage + (size_t)k * n, sizeof(double) * n,
                                cudaMemcpyDeviceToHost, s->stream));
   SPHPC_CK(cudaStreamSynchronize(s->stream));
-  if (p->id)
+  // the host arrays are in original order: ids are the identity (written on
+  // full updates; a field subset leaves them as they are)
+  if (p->id && field_mask == 0xFFFFFFFFu)
     for (int i = 0; i < n; ++i) p->id[i] = i;
   return SPHPC_OK;
 }
