@@ -284,20 +284,28 @@ __global__ void __launch_bounds__(kBuildBlock, 10)
         const bool self_row = dz == 0 && dy == 0;
         int j = b;
         for (; j + 4 <= e; j += 4) {
-          float r2f[4];
+          // hit and band masks of four candidates without branches; the exact
+          // test only for the rare in-band bits, then the hits in order
+          uint32_t hit = 0u, band = 0u;
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             const float4 q = __ldg(xsa + j + u);
             const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
-            r2f[u] = fx * fx + fy * fy + fz * fz;
+            const float r2 = fx * fx + fy * fy + fz * fz;
+            hit |= (uint32_t)(r2 <= c.h2hi) << u;
+            band |= (uint32_t)(r2 >= c.h2lo) << u;
           }
+          if (self_row && (unsigned)(p - j) < 4u) hit &= ~(1u << (p - j));
+          band &= hit;
+          if (band) {
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            if (r2f[u] > c.h2hi) continue;
-            const int jj = j + u;
-            if (self_row && jj == p) continue;
-            if (r2f[u] >= c.h2lo && !exact_neighbor(c, pd, jj)) continue;
-            out[(size_t)count * stride] = (uint32_t)jj;
+            for (int u = 0; u < 4; ++u)
+              if (((band >> u) & 1u) && !exact_neighbor(c, pd, j + u)) hit &= ~(1u << u);
+          }
+          while (hit) {
+            const int u = __ffs(hit) - 1;
+            hit &= hit - 1u;
+            out[(size_t)count * stride] = (uint32_t)(j + u);
             if (++count == kMaxNeighbors) goto done;
           }
         }
