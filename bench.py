@@ -113,7 +113,10 @@ class ClockSampler:
                 "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_init(args):
+def dist_init(args, backend="nccl"):
+    """One process per GPU (torchrun's RANK/LOCAL_RANK/WORLD_SIZE); replicas
+    only: the process group carries the barriers and the max-over-ranks time,
+    no data.  backend "gloo" runs the same host logic on CPU."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -122,11 +125,28 @@ def dist_init(args):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=timedelta(seconds=60))
         pg = dist
     return world, rank, local, pg
+
+
+def max_over_ranks(value, dist, device):
+    """The largest `value` of all ranks (the job's time is its slowest rank's)."""
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, n, steps, seconds):
+    """Whole-job particle-steps/s of `world` replicas of n particles."""
+    return world * n * steps / seconds
 
 
 # --------------------------------------------------------------------------
@@ -227,14 +247,11 @@ def timed_arm(sim, args, stream, dist, local, dev):
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     errs = sim.device_errors()
     if errs:
         raise RuntimeError(f"device error bits 0x{errs:x} during the timed region")
-    return {"ms": float(t.item()), "iters": iters, "converged": conv, "rejected": rejected,
+    return {"ms": ms, "iters": iters, "converged": conv, "rejected": rejected,
             "warm_used": used, "launches": sim.launches() - launches0,
             "clocks": clk.summary(), "diag": sim.diagnostics()}
 
@@ -277,7 +294,7 @@ def run_ours(args, world, rank, local, dist):
         warm = timed_arm(sim, args, stream, dist, local, dev)
     head = warm if warm is not None else plain
     ms_max = head["ms"]
-    value = world * n * args.steps / (ms_max / 1e3)
+    value = job_rate(world, n, args.steps, ms_max / 1e3)
     iters = head["iters"]
     conv = head["converged"]
     launches = head["launches"]
@@ -331,7 +348,7 @@ def run_ours(args, world, rank, local, dist):
     def arm_summary(a):
         if a is None:
             return None
-        return {"value": world * n * args.steps / (a["ms"] / 1e3),
+        return {"value": job_rate(world, n, args.steps, a["ms"] / 1e3),
                 "ms_per_step": a["ms"] / args.steps,
                 "mean_iterations": float(np.mean(a["iters"])) if a["iters"] else None,
                 "steps_converged": a["converged"] if a["iters"] else None,
@@ -415,14 +432,10 @@ def run_e2e(sim, args, dist, world, n):
             frames += 1
     sim.fetch_fields(out_fields)
     torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
-    t = torch.tensor([dt], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dt = float(t.item())
+    dt = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
     h2d = 8 * len(fields_in) * n
     d2h = args.steps * 72 + frames * 8 * len(frame_fields) * n + 8 * len(out_fields) * n
-    return {"value": world * n * args.steps / dt, "unit": UNIT,
+    return {"value": job_rate(world, n, args.steps, dt), "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
             "host_memory": "the reference's calloc'd arrays, page-locked in place by the "
                            "library (cudaHostRegister at enter_data)"}
