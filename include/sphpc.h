@@ -170,6 +170,21 @@ int sphpc_step_info(const struct Particles *particles, struct SphpcStepInfo *inf
 /* Kernel-reported error bits since the last call (0 = none); clears them. */
 int sphpc_device_errors(const struct Particles *particles, unsigned int *bits);
 
+/* ---------------- snapshot output ---------------- */
+
+/* fileio_MPI_IO.h:15-27: output/sim-N.bin under the working directory, the
+ * particles' x, y, z as interleaved doubles in original particle order.
+ * WriteParticles gathers on the device and returns once the copy to the
+ * page-locked write_buffer is queued; a host thread writes the file.  The
+ * next WriteParticles, sphpc_fileio_wait and FinalizeFileIO wait for it and
+ * return its outcome. */
+int AllocInitFileIO(struct FileIO *const file_io, const struct Particles *const particles,
+                    const struct Params *params);
+int WriteParticles(const struct Particles *const particles, const struct Params *const params,
+                   struct FileIO *const file_io);
+int sphpc_fileio_wait(struct FileIO *file_io);
+int FinalizeFileIO(struct FileIO *const file_io);
+
 /* ---------------- learned warm start ---------------- */
 
 /* Forward pass of the warm-start network on n feature rows d_feat[n][16]

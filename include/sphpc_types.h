@@ -107,6 +107,15 @@ struct Neighbors {
  * holds a linear device copy of the SDF). */
 struct Obstacle_CUDA;
 
+/* Snapshot output state, fileio_MPI_IO.h:8-12 (same fields): write_buffer
+ * holds 3 * max_local doubles (page-locked here), output_path the output
+ * directory, file_num the number of the next file. */
+struct FileIO {
+  double *write_buffer;
+  char *output_path;
+  int file_num;
+};
+
 struct Obstacle {
   char SDF_file_name[128];
   double origin_x;

@@ -80,6 +80,11 @@ class Solver(C.Structure):
                 ("warm_start_scale", C.c_double)]
 
 
+class FileIO(C.Structure):
+    _fields_ = [("write_buffer", C.POINTER(C.c_double)), ("output_path", C.c_char_p),
+                ("file_num", C.c_int)]
+
+
 class Diag(C.Structure):
     _fields_ = [("max_density_error", C.c_double), ("mean_density_error", C.c_double),
                 ("kinetic_energy", C.c_double), ("com", C.c_double * 3),
@@ -159,6 +164,10 @@ SIGNATURES = {
     "FinalizeObstacle": ([PO], C.c_int),
     "sphpc_read_sdf": ([PO], C.c_int),
     "sphpc_step": ([PP, P, PN, PA, PO, C.c_int], C.c_int),
+    "AllocInitFileIO": ([C.POINTER(FileIO), PP, P], C.c_int),
+    "WriteParticles": ([PP, P, C.POINTER(FileIO)], C.c_int),
+    "sphpc_fileio_wait": ([C.POINTER(FileIO)], C.c_int),
+    "FinalizeFileIO": ([C.POINTER(FileIO)], C.c_int),
     "sphpc_mlp_collect": ([PP, P, PN, PA, PO, C.c_int], C.c_int),
     "sphpc_mlp_load": ([PP, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
     "sphpc_mlp_unload": ([PP], C.c_int),

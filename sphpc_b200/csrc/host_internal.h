@@ -41,6 +41,12 @@ double lattice_poly6_sum(double h, double W_norm, double spacing);
 // OOPSLA 2014).
 double counter_uniform01(uint64_t seed, uint64_t index, uint32_t axis);
 
+// Launches, on the particle set's stream, the gather of its positions x, y, z
+// as interleaved doubles d_out[3 * id + k] in original particle order;
+// returns the particle count and the stream.
+int sim_interleave_positions(const struct Particles* particles, double* d_out, int* n,
+                             void** stream);
+
 // Kernel norms of SetParameters (simulation.c:173-177).
 void set_kernel_norms(Params* p);
 

@@ -860,6 +860,29 @@ struct SeamScratch {
 static std::mutex g_seam_mu;
 static std::map<int, SeamScratch> g_seam;
 
+// ---- snapshot gather (WriteParticles) ----
+
+__global__ void k_interleave_xyz(int n, const uint32_t* __restrict__ ids,
+                                 const PD* __restrict__ pd, double* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const float4 x = pd[p].x;
+  double* o = out + 3 * (size_t)__ldg(ids + p);
+  o[0] = x.x;
+  o[1] = x.y;
+  o[2] = x.z;
+}
+
+int sim_interleave_positions(const struct Particles* particles, double* d_out, int* n,
+                             void** stream) {
+  SPHPC_SIM(s, particles);
+  k_interleave_xyz<<<grid_for(s->n), kBlock, 0, s->stream>>>(s->n, s->ids, s->pd, d_out);
+  SPHPC_CK(cudaGetLastError());
+  *n = s->n;
+  *stream = (void*)s->stream;
+  return SPHPC_OK;
+}
+
 }  // namespace sphpc
 
 using namespace sphpc;

@@ -12,8 +12,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (AABB, Diag, KernelTime, Neighbors, Obstacle, Params, Particles, Solver,
-                   StepInfo, PARTICLE_FIELDS, call, load)
+from ._lib import (AABB, Diag, FileIO, KernelTime, Neighbors, Obstacle, Params, Particles,
+                   Solver, StepInfo, PARTICLE_FIELDS, call, load)
 from .scenes import config_path
 
 
@@ -205,6 +205,22 @@ class Simulation:
 
     def update_positions(self):
         call("UpdatePositions", C.byref(self.particles))
+
+    # ---------------- snapshot output (fileio_MPI_IO.c) ----------------
+    def fileio_open(self) -> FileIO:
+        """AllocInitFileIO: snapshots go to ./output/sim-N.bin."""
+        f = FileIO()
+        call("AllocInitFileIO", C.byref(f), C.byref(self.particles), C.byref(self.params))
+        return f
+
+    def write_particles(self, f: FileIO):
+        call("WriteParticles", C.byref(self.particles), C.byref(self.params), C.byref(f))
+
+    def fileio_wait(self, f: FileIO):
+        call("sphpc_fileio_wait", C.byref(f))
+
+    def fileio_close(self, f: FileIO):
+        call("FinalizeFileIO", C.byref(f))
 
     # ---------------- learned warm start ----------------
     def mlp_load(self, params, norm):
