@@ -170,6 +170,18 @@ int sphpc_step_info(const struct Particles *particles, struct SphpcStepInfo *inf
 /* Kernel-reported error bits since the last call (0 = none); clears them. */
 int sphpc_device_errors(const struct Particles *particles, unsigned int *bits);
 
+/* ---------------- obstacle tooling ---------------- */
+
+/* Signed distance field of a closed triangle mesh on the device, in the
+ * sample layout of the SDFGen files AllocInitObstacle reads (obstacle.c:13-79):
+ * phi[i + dims[0] * (j + dims[1] * k)] at origin + (i, j, k) * dx, negative
+ * inside; |phi| is the exact distance to the nearest triangle, the sign the
+ * generalized winding number.  vertices[3 * n_vertices], triangles[3 *
+ * n_triangles] (vertex indices) and phi are host memory.  The reference has
+ * no counterpart (it reads files made by an external tool). */
+int sphpc_mesh_sdf(const float *vertices, int n_vertices, const int *triangles, int n_triangles,
+                   const int *dims, const double *origin, double dx, float *phi);
+
 /* ---------------- snapshot output ---------------- */
 
 /* fileio_MPI_IO.h:15-27: output/sim-N.bin under the working directory, the
