@@ -182,6 +182,17 @@ int sphpc_device_errors(const struct Particles *particles, unsigned int *bits);
 int sphpc_mesh_sdf(const float *vertices, int n_vertices, const int *triangles, int n_triangles,
                    const int *dims, const double *origin, double dx, float *phi);
 
+/* Particle-to-level-set surface of a snapshot on a dense device grid (the
+ * operations of PostProcessing/OpenVDB/src/ConstructSurface.cc:39-72, which
+ * uses OpenVDB sparse grids on the CPU): voxel size radius / 2, spheres of
+ * the given radius rasterised as min(|x - p| - radius) within a band of
+ * half_width voxels + radius, then dilated by radius, smoothed (three passes
+ * of a 3-tap mean per axis) and eroded by radius.  xyz[3 * np] interleaved
+ * doubles (the sim-N.bin layout), phi[i + dims[0] * (j + dims[1] * k)] at
+ * origin + (i, j, k) * radius / 2, negative inside; host memory. */
+int sphpc_particle_surface(const double *xyz, int np, double radius, int half_width,
+                           const int *dims, const double *origin, float *phi);
+
 /* ---------------- snapshot output ---------------- */
 
 /* fileio_MPI_IO.h:15-27: output/sim-N.bin under the working directory, the

@@ -182,6 +182,9 @@ SIGNATURES = {
     "sphpc_mesh_sdf": ([C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int), C.c_int,
                         C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_double,
                         C.POINTER(C.c_float)], C.c_int),
+    "sphpc_particle_surface": ([C.POINTER(C.c_double), C.c_int, C.c_double, C.c_int,
+                                C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                C.POINTER(C.c_float)], C.c_int),
     "sphpc_mlp_grad": ([C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_void_p],
                        C.c_int),
     "sphpc_mlp_dataset_reserve": ([C.c_longlong], C.c_int),
