@@ -329,7 +329,9 @@ __global__ void __launch_bounds__(kMlpTile)
       y *= out_scale;
       if (out) out[p] = y;
       if (rec_out) {
-        rec.w = __float_as_uint(fminf(y, 0.0f));
+        // the record carries lambda_0 of the plain first substep; the target
+        // sum_k s_k lambda_k (s_0 = 1, lambda_k <= 0) never exceeds it
+        rec.w = __float_as_uint(fminf(y, __uint_as_float(rec.w)));
         rec_out[p] = rec;
       }
     }

@@ -58,8 +58,9 @@ void mlp_free(MlpDevice& d);
 
 // Forward pass of n feature rows feat[n][16] -> out[n] (lambda0), or when
 // rec_in/rec_out are given, 16-byte neighbour records rec_out[p] = rec_in[p]
-// with the payload min(lambda0, 0) (the plain solver's multipliers are never
-// positive).
+// with the payload min(Lambda, rec_in[p] payload): the input records carry
+// the plain first multiplier lambda_0 <= 0, and the target sum_k s_k lambda_k
+// (s_0 = 1, every lambda_k <= 0) never exceeds it.
 void launch_mlp_forward(const MlpDevice& d, const float* feat, int n, float* out,
                         const uint4* rec_in, uint4* rec_out, uint32_t* err, cudaStream_t st,
                         float extra_scale = 1.0f);
