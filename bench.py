@@ -263,7 +263,7 @@ def run_ours(args, world, rank, local, dist):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     overrides = {"adaptive": 1, "density_tolerance": args.tol,
-                 "max_iterations": args.max_iters}
+                 "max_iterations": args.max_iters, "min_progress": args.min_progress}
     if args.fixed:
         overrides = {"adaptive": 0}
     net = None
@@ -362,7 +362,10 @@ def run_ours(args, world, rank, local, dist):
         "data": "synthetic",
         "config": {"workload": args.config, "particles_per_gpu": n,
                    "solver": ("fixed iterations" if args.fixed else
-                              f"iterate to max density err <= {args.tol} (cap {args.max_iters})")
+                              f"iterate to max density err <= {args.tol} (cap {args.max_iters}"
+                              + (f"; stop when an iteration lowers it by < "
+                                 f"{100 * args.min_progress:g}%" if args.min_progress > 0 else "")
+                              + ")")
                    + (", MLP warm start" if warm is not None else ", plain (no network file)"),
                    "plain": arm_summary(plain),
                    "warm_start": arm_summary(warm),
@@ -444,12 +447,15 @@ def run_e2e(sim, args, dist, world, n):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="full_16m")
     ap.add_argument("--tol", type=float, default=0.01)
     ap.add_argument("--max-iters", type=int, default=12)
+    ap.add_argument("--min-progress", type=float, default=0.02,
+                    help="adaptive solver: stop (step not converged) when an iteration lowers "
+                         "the max density error by less than this fraction; 0: off")
     ap.add_argument("--fixed", action="store_true", help="configured iteration count")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -213,6 +213,7 @@ void sphpc_default_solver(struct SphpcSolver* s) {
   s->warm_start_gate = 1;
   s->pad_warm = 0;
   s->warm_start_scale = 1.0;
+  s->min_progress = 0.0;
 }
 
 void sphpc_set_default_solver(const struct SphpcSolver* s) {

@@ -524,7 +524,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     std::swap(pd, pd_alt);
   };
   int iters = 0, plain = 0;
-  bool converged = false;
+  bool converged = false, stalled = false;
   const uint4* ready = nullptr;  // records with lambda for the next B (its A already run)
   if (collect) {
     // the first A also writes the features of the (predicted) state; the
@@ -595,6 +595,14 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
           converged = true;
           break;
         }
+        // stall: the last iteration barely lowered the maximum error (the
+        // relaxed constraint's fixed point lies above the tolerance)
+        const size_t nt = trace.size();
+        if (solver.min_progress > 0.0 && nt >= 2 &&
+            trace[nt - 1] > (1.0 - solver.min_progress) * trace[nt - 2]) {
+          stalled = true;
+          break;
+        }
       }
       src = nr_alt;
     }
@@ -613,7 +621,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     // converged (or capped, or no plain pass): velocities from x* and the
     // freshest density
     Scope sc(this, "velocity");
-    if (converged || iters == 0) {
+    if (converged || stalled || iters == 0) {
       launch_pack_w(P, nullptr, nr, rho, stream);
       launches += 1;
     }
