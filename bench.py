@@ -363,7 +363,7 @@ def run_ours(args, world, rank, local, dist):
         "config": {"workload": args.config, "particles_per_gpu": n,
                    "solver": ("fixed iterations" if args.fixed else
                               f"iterate to max density err <= {args.tol} (cap {args.max_iters}"
-                              + (f"; stop when an iteration lowers it by < "
+                              + (f"; stop when two iterations lower it by < "
                                  f"{100 * args.min_progress:g}%" if args.min_progress > 0 else "")
                               + ")")
                    + (", MLP warm start" if warm is not None else ", plain (no network file)"),
@@ -454,8 +454,8 @@ def main():
     ap.add_argument("--tol", type=float, default=0.01)
     ap.add_argument("--max-iters", type=int, default=12)
     ap.add_argument("--min-progress", type=float, default=0.02,
-                    help="adaptive solver: stop (step not converged) when an iteration lowers "
-                         "the max density error by less than this fraction; 0: off")
+                    help="adaptive solver: stop (step not converged) when two iterations "
+                         "lower the max density error by less than this fraction; 0: off")
     ap.add_argument("--fixed", action="store_true", help="configured iteration count")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

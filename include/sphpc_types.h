@@ -166,9 +166,10 @@ struct SphpcSolver {
                                  FP64 max density error (default) */
   int pad_warm;
   double warm_start_scale;    /* multiplier on the network's Lambda (1) */
-  double min_progress;        /* adaptive: also stop (not converged) when an
-                                 iteration lowers the FP64 max density error by
-                                 less than this fraction; 0 (default): off */
+  double min_progress;        /* adaptive: also stop (not converged) when two
+                                 iterations together lower the FP64 max density
+                                 error by less than this fraction; 0 (default):
+                                 off */
 };
 
 /* FP64 reductions over the local particles. */

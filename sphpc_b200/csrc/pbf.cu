@@ -19,6 +19,14 @@ struct Pair {
 
 // neighbours whose list entries and records are fetched together
 constexpr int kNbrBatch = 4;
+// resident 256-thread blocks per SM asked of the compiler for the neighbour
+// passes (register caps of 40 and 48; more resident warps hide the gather
+// latency better than the registers a larger allocation would keep)
+constexpr int kMinBlocksDensity = 6;
+constexpr int kMinBlocksPosition = 5;
+constexpr int kMinBlocksColor = 5;
+constexpr int kMinBlocksVorticity = 5;
+constexpr int kMinBlocksConfinement = 6;
 
 // x*_p - x*_q as (x_p - x_q) + (d_p - d_q): exact in the first term for any
 // box size, so the FP32 pair geometry keeps its relative precision.
@@ -83,7 +91,7 @@ __device__ __forceinline__ void block_resid(double e, double* resid) {
 }
 
 template <int MODE, bool RESID>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
     k_density_lambda(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   double err = 0.0;
@@ -244,7 +252,7 @@ __global__ void k_accum_lambda(const uint4* __restrict__ rec, float s, float* __
 }
 
 template <int MODE, int SCORR_N, bool SDF>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kMinBlocksPosition)
     k_position(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
@@ -329,7 +337,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_dp(const DevParams P, const Pa
                               __double2float_rn(__dsub_rn(zs, (double)xp.z)), dp.w);
 }
 
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kMinBlocksColor)
     k_color(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
@@ -425,7 +433,7 @@ __global__ void __launch_bounds__(kBlock)
 
 // With nr_out, also the records {X, |omega|} the confinement pass gathers
 // (one 16-byte load per neighbour instead of a record and omega[q]).
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kMinBlocksVorticity)
     k_vorticity(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
@@ -453,7 +461,7 @@ __global__ void __launch_bounds__(kBlock)
 // OW: a.nr carries |omega| as its payload (the vorticity pass's records);
 // otherwise |omega_q| comes from omega[q].w.
 template <bool OW>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kMinBlocksConfinement)
     k_confinement(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;

@@ -595,11 +595,12 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
           converged = true;
           break;
         }
-        // stall: the last iteration barely lowered the maximum error (the
-        // relaxed constraint's fixed point lies above the tolerance)
+        // stall: the last two iterations together barely lowered the maximum
+        // error (the relaxed constraint's fixed point lies above the
+        // tolerance); one iteration alone may raise the maximum of a hard step
         const size_t nt = trace.size();
-        if (solver.min_progress > 0.0 && nt >= 2 &&
-            trace[nt - 1] > (1.0 - solver.min_progress) * trace[nt - 2]) {
+        if (solver.min_progress > 0.0 && nt >= 3 &&
+            trace[nt - 1] > (1.0 - solver.min_progress) * trace[nt - 3]) {
           stalled = true;
           break;
         }

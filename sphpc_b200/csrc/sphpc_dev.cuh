@@ -149,25 +149,32 @@ __device__ __forceinline__ void for_each_neighbor(const NbrView& v, int p, F&& f
 }
 
 // The same visit with each neighbour's 16-byte record loaded for f(q, rq):
-// list entries and records are fetched in batches of B (B list loads, then
-// B record loads, then the B bodies), so a thread keeps B gathers in flight
-// instead of one dependent pair.  Batch slots past the count load the
-// particle's own record and are skipped.
+// list entries and records are fetched in batches of B, and the list
+// entries of the next batch are loaded before the bodies of this one run, so
+// a batch waits only for its record gathers (the list read from HBM overlaps
+// the previous batch).  Batch slots past the count load the particle's own
+// record and are skipped.
 template <int B, class F>
 __device__ __forceinline__ void for_each_neighbor_nr(const NbrView& v, const uint4* __restrict__ nr,
                                                      int p, F&& f) {
   const int cnt = (int)__ldg(v.ncount + p);
   const uint32_t* lst = v.nbr + p;
-  for (int j0 = 0; j0 < cnt; j0 += B) {
-    int q[B];
+  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
+  int q[B];
 #pragma unroll
-    for (int u = 0; u < B; ++u) q[u] = j0 + u < cnt ? (int)__ldg(lst + (size_t)(j0 + u) * v.n) : p;
+  for (int u = 0; u < B; ++u) q[u] = ldq(u);
+  for (int j0 = 0; j0 < cnt; j0 += B) {
     uint4 r[B];
 #pragma unroll
     for (int u = 0; u < B; ++u) r[u] = ld_nr(nr, q[u]);
+    int qn[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
 #pragma unroll
     for (int u = 0; u < B; ++u)
       if (j0 + u < cnt) f(q[u], r[u]);
+#pragma unroll
+    for (int u = 0; u < B; ++u) q[u] = qn[u];
   }
 }
 
@@ -180,10 +187,11 @@ __device__ __forceinline__ void for_each_neighbor_nr2(const NbrView& v,
                                                       F&& f) {
   const int cnt = (int)__ldg(v.ncount + p);
   const uint32_t* lst = v.nbr + p;
-  for (int j0 = 0; j0 < cnt; j0 += B) {
-    int q[B];
+  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
+  int q[B];
 #pragma unroll
-    for (int u = 0; u < B; ++u) q[u] = j0 + u < cnt ? (int)__ldg(lst + (size_t)(j0 + u) * v.n) : p;
+  for (int u = 0; u < B; ++u) q[u] = ldq(u);
+  for (int j0 = 0; j0 < cnt; j0 += B) {
     uint4 r[B];
     float4 e[B];
 #pragma unroll
@@ -191,9 +199,14 @@ __device__ __forceinline__ void for_each_neighbor_nr2(const NbrView& v,
       r[u] = ld_nr(nr, q[u]);
       e[u] = __ldg(extra + q[u]);
     }
+    int qn[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
 #pragma unroll
     for (int u = 0; u < B; ++u)
       if (j0 + u < cnt) f(q[u], r[u], e[u]);
+#pragma unroll
+    for (int u = 0; u < B; ++u) q[u] = qn[u];
   }
 }
 
@@ -203,16 +216,22 @@ __device__ __forceinline__ void for_each_neighbor_pd(const NbrView& v, const PD*
                                                      int p, F&& f) {
   const int cnt = (int)__ldg(v.ncount + p);
   const uint32_t* lst = v.nbr + p;
-  for (int j0 = 0; j0 < cnt; j0 += B) {
-    int q[B];
+  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
+  int q[B];
 #pragma unroll
-    for (int u = 0; u < B; ++u) q[u] = j0 + u < cnt ? (int)__ldg(lst + (size_t)(j0 + u) * v.n) : p;
+  for (int u = 0; u < B; ++u) q[u] = ldq(u);
+  for (int j0 = 0; j0 < cnt; j0 += B) {
     float4 x[B], d[B];
 #pragma unroll
     for (int u = 0; u < B; ++u) ld_pd(pd, q[u], x[u], d[u]);
+    int qn[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
 #pragma unroll
     for (int u = 0; u < B; ++u)
       if (j0 + u < cnt) f(q[u], x[u], d[u]);
+#pragma unroll
+    for (int u = 0; u < B; ++u) q[u] = qn[u];
   }
 }
 

@@ -207,9 +207,13 @@ def test_one_step_matches_oracle(config):
 
 def test_trajectory_statistics_match_oracle():
     """200 steps of the small dam break: per-step trajectories diverge
-    (chaotic flow), the statistics must not: max/mean density error within
-    0.5 percentage points, kinetic energy within 3%, centre of mass within
-    0.05 length units, at steps 50, 100 and 200."""
+    (chaotic flow), the statistics must not: mean density error within 0.05
+    percentage points, kinetic energy within 3%, centre of mass within 0.05
+    length units at steps 50, 100 and 200; the max density error within 0.5
+    percentage points at steps 50 and 100 only.  By step 200 the maximum over
+    the particles is itself chaotic: the FP64 oracle alone, with its initial
+    positions moved by uniform +-1e-6, ends between 0.75% and 3.6% (mean
+    error 5.2e-4 to 6.1e-4, kinetic energy within 1.5%)."""
     with Simulation("small_dam") as sim:
         o = oracle_for(sim)
         done = 0
@@ -219,7 +223,8 @@ def test_trajectory_statistics_match_oracle():
             done = k
             dg = sim.diagnostics()
             do = o.diagnostics()
-            assert abs(dg["max_density_error"] - do["max_density_error"]) < 5e-3, (k, dg, do)
+            if k <= 100:
+                assert abs(dg["max_density_error"] - do["max_density_error"]) < 5e-3, (k, dg, do)
             assert abs(dg["mean_density_error"] - do["mean_density_error"]) < 5e-4, (k, dg, do)
             assert abs(dg["kinetic_energy"] / do["kinetic_energy"] - 1) < 0.03, (k, dg, do)
             for a in range(3):
