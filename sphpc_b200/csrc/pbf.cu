@@ -97,37 +97,48 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
   double err = 0.0;
   if (p < P.n) {
     const uint4 rp = ld_nr(a.nr, p);
-    float rho = P.W0m, comp = 0.0f;
+    // The loop keeps only what varies per pair: the density sums t^3 with
+    // t = h^2 - r^2 (Kahan-compensated) and the gradient sums c d with
+    // c = (h - r)^2 / r and d the pair difference in fixed-point units; the
+    // kernel norms, the mass and 2^-k multiply the sums once afterwards.
+    float st = 0.0f, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
     for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int, const uint4 rq) {
-      const Pair g = pair_nr(P, rp, rq);
+      const float fx = (float)(int)(rp.x - rq.x);
+      const float fy = (float)(int)(rp.y - rq.y);
+      const float fz = (float)(int)(rp.z - rq.z);
+      const float r2 = (fx * fx + fy * fy + fz * fz) * P.fx_inv2;
       if (MODE != 2) {
-        const float t = P.h2 - g.r2;
-        const float w = t > 0.0f ? P.Wn_m * t * t * t : 0.0f;
-        const float y = w - comp;
-        const float s = rho + y;
-        comp = (s - rho) - y;
-        rho = s;
+        const float t = fmaxf(P.h2 - r2, 0.0f);
+        const float y = t * t * t - comp;
+        const float s = st + y;
+        comp = (s - st) - y;
+        st = s;
       }
       if (MODE != 1) {
         float r, rinv;
-        floored_r(P, g.r2, r, rinv);
-        const float hm = P.h - r;
-        const float c = hm > 0.0f ? P.DWn_m * hm * hm * rinv : 0.0f;
-        const float gx = c * g.dx, gy = c * g.dy, gz = c * g.dz;
+        floored_r(P, r2, r, rinv);
+        const float hm = fmaxf(P.h - r, 0.0f);
+        const float c = hm * hm * rinv;
+        const float gx = c * fx, gy = c * fy, gz = c * fz;
         sgx += gx;
         sgy += gy;
         sgz += gz;
         sC += gx * gx + gy * gy + gz * gz;
       }
     });
+    float rho;
     if (MODE == 2) rho = a.rho[p];
-    if (MODE != 2) a.rho[p] = rho;
+    if (MODE != 2) {
+      rho = fmaf(P.Wn_m, st - comp, P.W0m);
+      a.rho[p] = rho;
+    }
     if (MODE != 1) {
       // ComputeLambda's constraint (particles.c:616-617) in FP64
       const float C = (float)fmax(__ddiv_rn((double)rho, P.rho0_d) - 1.0, 0.0);
+      const float g = P.DWn_m * P.fx_inv;  // gradient scale (2^-k is exact)
       sC += sgx * sgx + sgy * sgy + sgz * sgz;
-      sC *= P.inv_rho0_sq;
+      sC *= (g * g) * P.inv_rho0_sq;
       const float lam = -C / (sC + P.lambda_eps);
       if (a.nr_out) a.nr_out[p] = make_uint4(rp.x, rp.y, rp.z, __float_as_uint(lam));
       if (a.lam) a.lam[p] = lam;
@@ -260,32 +271,38 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksPosition)
   const float lp = nr_w(rp);
   float4 xp, dp;  // own particle record, loaded ahead of the neighbour loop
   if (MODE == 0) ld_pd(a.pd, p, xp, dp);
+  // sums of c d with c = (lambda_p + lambda_q + s_corr) (h - r)^2 / r and d
+  // the pair difference in fixed-point units; the spiky norm, the mass and
+  // 2^-k multiply them once afterwards.  Every term carries d, so the batch's
+  // padding slots (q = p, d = 0) add nothing and are not masked.
   float ax = 0.f, ay = 0.f, az = 0.f;
-  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int, const uint4 rq) {
-    const Pair g = pair_nr(P, rp, rq);
+  for_each_neighbor_nr<kNbrBatch, true>(V, a.nr, p, [&](int, const uint4 rq) {
+    const float fx = (float)(int)(rp.x - rq.x);
+    const float fy = (float)(int)(rp.y - rq.y);
+    const float fz = (float)(int)(rp.z - rq.z);
+    const float r2 = (fx * fx + fy * fy + fz * fz) * P.fx_inv2;
     float r, rinv;
-    floored_r(P, g.r2, r, rinv);
-    const float hm = P.h - r;
-    const float delW = hm > 0.0f ? P.DWn_m * hm * hm : 0.0f;
-    float sc = 0.0f;
+    floored_r(P, r2, r, rinv);
+    const float hm = fmaxf(P.h - r, 0.0f);
+    float s = lp + nr_w(rq);
     if (SCORR_N != 0) {
-      const float t = P.h2 - r * r;
-      const float w = t > 0.0f ? P.Wn * t * t * t : 0.0f;
-      const float ratio = w * P.inv_Wdq;
+      const float t = fmaxf(P.h2 - r * r, 0.0f);
+      const float ratio = t * t * t * P.scorr_c;  // W(r) / W(dq)
       if (SCORR_N == 4) {
-        const float r2_ = ratio * ratio;
-        sc = -P.scorr_k * (r2_ * r2_);
+        const float q2 = ratio * ratio;
+        s = fmaf(-P.scorr_k * q2, q2, s);
       } else {
-        sc = -P.scorr_k;
+        float sc = -P.scorr_k;
         for (int e = 0; e < P.scorr_n; ++e) sc *= ratio;
+        s += sc;
       }
     }
-    const float c = (lp + nr_w(rq) + sc) * delW * rinv;
-    ax += c * g.dx;
-    ay += c * g.dy;
-    az += c * g.dz;
+    const float c = s * hm * hm * rinv;
+    ax = fmaf(c, fx, ax);
+    ay = fmaf(c, fy, ay);
+    az = fmaf(c, fz, az);
   });
-  const float s = a.stiffness * P.inv_rho0;
+  const float s = a.stiffness * P.inv_rho0 * (P.DWn_m * P.fx_inv);
   const float dpx = ax * s, dpy = ay * s, dpz = az * s;
   if (MODE == 1) {
     a.dp[p] = make_float4(dpx, dpy, dpz, 0.0f);

@@ -331,6 +331,7 @@ DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob
     const int k = 28 - (int)ceil(log2(h));
     P.fx_scale = ldexp(1.0, k);
     P.fx_inv = (float)ldexp(1.0, -k);
+    P.fx_inv2 = (float)ldexp(1.0, -2 * k);
   }
   P.h2d = h * h;
   P.h = (float)h;
@@ -358,6 +359,7 @@ DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob
     const double t = h * h - dq * dq;
     const double Wdq = dq > h ? 0.0 : prm.W_norm * t * t * t;
     P.inv_Wdq = Wdq > 0.0 ? (float)(1.0 / Wdq) : 0.0f;
+    P.scorr_c = Wdq > 0.0 ? (float)(prm.W_norm / Wdq) : 0.0f;
     if (Wdq <= 0.0) P.scorr_k = 0.0f;
   }
   P.c_xsph = (float)prm.c;

@@ -85,6 +85,7 @@ struct DevParams {
   double hd;            // smoothing radius (double)
   double fx_scale;      // 2^k: fixed-point units per length of the records
   float fx_inv;         // 2^-k
+  float fx_inv2;        // 2^-2k
   double h2d;
   float h, h2;
   float rmin;           // r floor 1e-4 h (particles.c:636)
@@ -99,6 +100,7 @@ struct DevParams {
   float scorr_k;        // s_corr = -k (W/W(dq))^n
   int scorr_n;
   float inv_Wdq;
+  float scorr_c;        // W_norm / W(dq): W(r)/W(dq) = scorr_c (h^2 - r^2)^3
   float c_xsph;
   int xsph_exact;       // 0: reference r expression (particles.c:439)
   float gamma, C_norm;  // surface tension
@@ -153,8 +155,9 @@ __device__ __forceinline__ void for_each_neighbor(const NbrView& v, int p, F&& f
 // entries of the next batch are loaded before the bodies of this one run, so
 // a batch waits only for its record gathers (the list read from HBM overlaps
 // the previous batch).  Batch slots past the count load the particle's own
-// record and are skipped.
-template <int B, class F>
+// record and are skipped, or, with kPadSlots, visited as the pair (p, p)
+// (for bodies whose every term carries the pair difference, which is 0).
+template <int B, bool kPadSlots = false, class F>
 __device__ __forceinline__ void for_each_neighbor_nr(const NbrView& v, const uint4* __restrict__ nr,
                                                      int p, F&& f) {
   const int cnt = (int)__ldg(v.ncount + p);
@@ -172,7 +175,7 @@ __device__ __forceinline__ void for_each_neighbor_nr(const NbrView& v, const uin
     for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
 #pragma unroll
     for (int u = 0; u < B; ++u)
-      if (j0 + u < cnt) f(q[u], r[u]);
+      if (kPadSlots || j0 + u < cnt) f(q[u], r[u]);
 #pragma unroll
     for (int u = 0; u < B; ++u) q[u] = qn[u];
   }
