@@ -222,11 +222,13 @@ def run_reference(args, world, rank):
 
 def timed_arm(sim, args, stream, dist, local, dev):
     """W untimed steps, then K steps timed with CUDA events on the launching
-    stream between barriers (max over ranks), with the clocks sampled."""
+    stream between barriers (max over ranks), with the clocks sampled and the
+    per-stage CUDA-event profile of the same K steps."""
     import torch
     for _ in range(args.warmup):
         sim.step(1)
     torch.cuda.synchronize()
+    sim.profile(True)
     launches0 = sim.launches()
     iters, conv, rejected, used = [], 0, 0, 0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -248,12 +250,15 @@ def timed_arm(sim, args, stream, dist, local, dev):
         if dist:
             dist.barrier()
     ms = max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
+    prof = sim.profile_read()
+    sim.profile(False)
+    prof.pop("kernel_launches", None)
     errs = sim.device_errors()
     if errs:
         raise RuntimeError(f"device error bits 0x{errs:x} during the timed region")
     return {"ms": ms, "iters": iters, "converged": conv, "rejected": rejected,
             "warm_used": used, "launches": sim.launches() - launches0,
-            "clocks": clk.summary(), "diag": sim.diagnostics()}
+            "clocks": clk.summary(), "diag": sim.diagnostics(), "prof": prof}
 
 
 def run_ours(args, world, rank, local, dist):
@@ -300,12 +305,8 @@ def run_ours(args, world, rank, local, dist):
     launches = head["launches"]
     diag = head["diag"]
 
-    # per-stage CUDA-event profile of two more steps (not part of the timed value)
-    sim.profile(True)
-    sim.step(2)
-    prof = sim.profile_read()
-    sim.profile(False)
-    prof.pop("kernel_launches", None)
+    # per-stage CUDA-event profile of the headline arm's timed steps
+    prof = head["prof"]
 
     roof = None
     if prof:
@@ -325,9 +326,14 @@ def run_ours(args, world, rank, local, dist):
                     "traffic": ncu_traffic(name, n), "bytes_per_particle": per,
                     "avg_launch_ms": tot / cnt}
 
-    # end to end through the C ABI with host buffers
+    # end to end through the C ABI with host buffers, over the same steps of
+    # the scene as the headline arm (a fresh particle set, W untimed steps)
     e2e = None
     if not args.no_e2e:
+        sim.close()
+        sim = make_sim(net is not None)
+        for _ in range(args.warmup):
+            sim.step(1)
         e2e = run_e2e(sim, args, dist, world, n)
 
     cpu = None
@@ -380,7 +386,7 @@ def run_ours(args, world, rank, local, dist):
         "gpu_launches": launches,
         "clocks": clocks,
         "roofline": roof,
-        "stage_ms_per_step": {k: v[1] / 2 for k, v in prof.items()},
+        "stage_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()},
         "e2e": e2e,
         "cpu_baseline": cpu,
     }

@@ -359,19 +359,25 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksColor)
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   const uint4 rp = ld_nr(a.nr, p);
+  // sums of (h^2 - r^2)^2 r / (r rho_q) d, d in fixed-point units; the
+  // poly6-gradient norm, m, h and 2^-k multiply them once (every term carries
+  // d, so the padding slots add nothing)
   float cx = 0.f, cy = 0.f, cz = 0.f;
-  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int, const uint4 rq) {
-    const Pair g = pair_nr(P, rp, rq);
+  for_each_neighbor_nr<kNbrBatch, true>(V, a.nr, p, [&](int, const uint4 rq) {
+    const float fx = (float)(int)(rp.x - rq.x);
+    const float fy = (float)(int)(rp.y - rq.y);
+    const float fz = (float)(int)(rp.z - rq.z);
+    const float r2 = (fx * fx + fy * fy + fz * fz) * P.fx_inv2;
     float r, rinv;
-    floored_r(P, g.r2, r, rinv);
-    const float t = P.h2 - r * r;
-    const float grad = t > 0.0f ? P.DWPn * t * t * r : 0.0f;
-    const float c = grad * P.m / nr_w(rq) * rinv;
-    cx += c * g.dx;
-    cy += c * g.dy;
-    cz += c * g.dz;
+    floored_r(P, r2, r, rinv);
+    const float t = fmaxf(P.h2 - r * r, 0.0f);
+    const float c = t * t * r * (rinv * __frcp_rn(nr_w(rq)));
+    cx = fmaf(c, fx, cx);
+    cy = fmaf(c, fy, cy);
+    cz = fmaf(c, fz, cz);
   });
-  a.color[p] = make_float4(P.h * cx, P.h * cy, P.h * cz, 0.0f);
+  const float s = P.h * (P.DWPn * P.m * P.fx_inv);
+  a.color[p] = make_float4(s * cx, s * cy, s * cz, 0.0f);
 }
 
 __device__ __forceinline__ float cohesion(const DevParams& P, float r) {
@@ -397,17 +403,24 @@ __global__ void __launch_bounds__(kBlock)
   const float rp = nr_w(recp);
   const float kcoh = -20.0f * P.gamma * P.m * P.m;
   const float kcur = -P.gamma * P.m;
+  // colour of each neighbour fetched with its record; the self terms of the
+  // padding slots vanish (d = 0, c_p - c_q = 0)
+  const float kcoh_fx = kcoh * P.fx_inv;  // for d in fixed-point units (exact)
+  const float two_rho0 = 2.0f * P.rho0;
   float fx = 0.f, fy = 0.f, fz = 0.f;
-  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int q, const uint4 rq) {
-    const Pair g = pair_nr(P, recp, rq);
+  for_each_neighbor_nr2<kNbrBatch, true>(V, a.nr, a.color, p,
+                                         [&](int, const uint4 rq, const float4 cq) {
+    const float dx = (float)(int)(recp.x - rq.x);
+    const float dy = (float)(int)(recp.y - rq.y);
+    const float dz = (float)(int)(recp.z - rq.z);
+    const float r2 = (dx * dx + dy * dy + dz * dz) * P.fx_inv2;
     float r, rinv;
-    floored_r(P, g.r2, r, rinv);
-    const float4 cq = __ldg(a.color + q);
-    const float coh = kcoh * cohesion(P, r) * rinv;
-    const float K = 2.0f * P.rho0 / (rp + nr_w(rq));
-    fx += K * (coh * g.dx + kcur * (cp.x - cq.x));
-    fy += K * (coh * g.dy + kcur * (cp.y - cq.y));
-    fz += K * (coh * g.dz + kcur * (cp.z - cq.z));
+    floored_r(P, r2, r, rinv);
+    const float coh = kcoh_fx * cohesion(P, r) * rinv;
+    const float K = two_rho0 * __frcp_rn(rp + nr_w(rq));
+    fx += K * (coh * dx + kcur * (cp.x - cq.x));
+    fy += K * (coh * dy + kcur * (cp.y - cq.y));
+    fz += K * (coh * dz + kcur * (cp.z - cq.z));
   });
   float4 v = a.vel[p];
   const float s = P.dt / rp;
@@ -423,20 +436,22 @@ __global__ void __launch_bounds__(kBlock)
   if (p >= P.n) return;
   const uint4 rp = ld_nr(a.nr, p);
   const float4 vp = __ldg(a.vel + p);
+  // sums of (v_q - v_p) t^3 / rho_q; the poly6 norm, m and c multiply them
+  // once (the padding slots' v_q - v_p is 0)
   float sx = 0.f, sy = 0.f, sz = 0.f;
-  for_each_neighbor_nr2<kNbrBatch>(V, a.nr, a.vel, p,
-                                   [&](int, const uint4 rq, const float4 vq) {
+  for_each_neighbor_nr2<kNbrBatch, true>(V, a.nr, a.vel, p,
+                                         [&](int, const uint4 rq, const float4 vq) {
     const Pair g = pair_nr(P, rp, rq);
     // particles.c:439 evaluates x^2 + y^2 * z^2 (kept unless xsph_exact)
     const float rr = P.xsph_exact ? g.r2 : g.dx * g.dx + g.dy * g.dy * g.dz * g.dz;
-    const float t = P.h2 - rr;
-    const float w = t > 0.0f ? P.Wn_m * t * t * t / nr_w(rq) : 0.0f;
-    sx += (vq.x - vp.x) * w;
-    sy += (vq.y - vp.y) * w;
-    sz += (vq.z - vp.z) * w;
+    const float t = fmaxf(P.h2 - rr, 0.0f);
+    const float w = t * t * t * __frcp_rn(nr_w(rq));
+    sx = fmaf(vq.x - vp.x, w, sx);
+    sy = fmaf(vq.y - vp.y, w, sy);
+    sz = fmaf(vq.z - vp.z, w, sz);
   });
-  a.vel_out[p] = make_float4(vp.x + P.c_xsph * sx, vp.y + P.c_xsph * sy,
-                             vp.z + P.c_xsph * sz, 0.0f);
+  const float cw = P.c_xsph * P.Wn_m;
+  a.vel_out[p] = make_float4(fmaf(cw, sx, vp.x), fmaf(cw, sy, vp.y), fmaf(cw, sz, vp.z), 0.0f);
   if (a.write_pos) {
     float4 xp, dp;
     ld_pd(a.pd, p, xp, dp);
@@ -456,20 +471,30 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksVorticity)
   if (p >= P.n) return;
   const uint4 rp = ld_nr(a.nr, p);
   const float4 vp = __ldg(a.vel + p);
+  // sums of (v_q - v_p) x c d with c = (h - r)^2 / r and d in fixed-point
+  // units; the spiky norm and 2^-k multiply them once (the padding slots'
+  // v_q - v_p and d are 0)
   float wx = 0.f, wy = 0.f, wz = 0.f;
-  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int q, const uint4 rq) {
-    const Pair g = pair_nr(P, rp, rq);
+  for_each_neighbor_nr2<kNbrBatch, true>(V, a.nr, a.vel, p,
+                                         [&](int, const uint4 rq, const float4 vq) {
+    const float dx = (float)(int)(rp.x - rq.x);
+    const float dy = (float)(int)(rp.y - rq.y);
+    const float dz = (float)(int)(rp.z - rq.z);
+    const float r2 = (dx * dx + dy * dy + dz * dz) * P.fx_inv2;
     float r, rinv;
-    floored_r(P, g.r2, r, rinv);
-    const float hm = P.h - r;
-    const float c = hm > 0.0f ? P.DWn * hm * hm * rinv : 0.0f;
-    const float gx = c * g.dx, gy = c * g.dy, gz = c * g.dz;
-    const float4 vq = __ldg(a.vel + q);
+    floored_r(P, r2, r, rinv);
+    const float hm = fmaxf(P.h - r, 0.0f);
+    const float c = hm * hm * rinv;
+    const float gx = c * dx, gy = c * dy, gz = c * dz;
     const float ux = vq.x - vp.x, uy = vq.y - vp.y, uz = vq.z - vp.z;
     wx += uy * gz - uz * gy;
     wy += uz * gx - ux * gz;
     wz += ux * gy - uy * gx;
   });
+  const float sw = P.DWn * P.fx_inv;
+  wx *= sw;
+  wy *= sw;
+  wz *= sw;
   const float wm = sqrtf(wx * wx + wy * wy + wz * wz);
   a.omega[p] = make_float4(wx, wy, wz, wm);
   if (a.nr_out) a.nr_out[p] = make_uint4(rp.x, rp.y, rp.z, __float_as_uint(wm));
@@ -483,18 +508,27 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksConfinement)
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   const uint4 rp = ld_nr(a.nr, p);
+  // sums of |omega_q| (h - r)^2 / r d, d in fixed-point units; the spiky
+  // norm and 2^-k multiply them once (the padding slots' d is 0)
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int q, const uint4 rq) {
-    const Pair g = pair_nr(P, rp, rq);
+  for_each_neighbor_nr<kNbrBatch, true>(V, a.nr, p, [&](int q, const uint4 rq) {
+    const float dx = (float)(int)(rp.x - rq.x);
+    const float dy = (float)(int)(rp.y - rq.y);
+    const float dz = (float)(int)(rp.z - rq.z);
+    const float r2 = (dx * dx + dy * dy + dz * dz) * P.fx_inv2;
     float r, rinv;
-    floored_r(P, g.r2, r, rinv);
-    const float hm = P.h - r;
+    floored_r(P, r2, r, rinv);
+    const float hm = fmaxf(P.h - r, 0.0f);
     const float wq = OW ? nr_w(rq) : __ldg(a.omega + q).w;
-    const float c = hm > 0.0f ? P.DWn * hm * hm * rinv * wq : 0.0f;
-    ex += c * g.dx;
-    ey += c * g.dy;
-    ez += c * g.dz;
+    const float c = hm * hm * rinv * wq;
+    ex = fmaf(c, dx, ex);
+    ey = fmaf(c, dy, ey);
+    ez = fmaf(c, dz, ez);
   });
+  const float se = P.DWn * P.fx_inv;
+  ex *= se;
+  ey *= se;
+  ez *= se;
   const float em = fmaxf(sqrtf(ex * ex + ey * ey + ez * ez), P.rmin);
   const float nx = ex / em, ny = ey / em, nz = ez / em;
   const float4 w = __ldg(a.omega + p);

@@ -269,6 +269,29 @@ class DeviceSim {
     cudaEventRecord(e, stream);
     pending.push_back({id, b, e});
   }
+  // Folds the scopes whose end event has completed into the totals without
+  // waiting (scopes complete in order on the one stream), so that a long
+  // profiled run keeps a bounded pool of events.
+  void prof_collect_ready() {
+    const cudaError_t before = cudaPeekAtLastError();
+    size_t k = 0;
+    for (; k < pending.size(); ++k) {
+      const Pending& p = pending[k];
+      if (cudaEventQuery(p.b) != cudaSuccess) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p.a, p.b);
+      prof_ms[p.name] += ms;
+      prof_count[p.name] += 1;
+      ev_pool.push_back(p.a);
+      ev_pool.push_back(p.b);
+    }
+    // a not-ready answer is no error: clear it if the query left it behind,
+    // and nothing else
+    if (before != cudaErrorNotReady && cudaPeekAtLastError() == cudaErrorNotReady)
+      cudaGetLastError();
+    pending.erase(pending.begin(), pending.begin() + (std::ptrdiff_t)k);
+  }
+
   void prof_collect() {
     if (pending.empty()) return;
     cudaStreamSynchronize(stream);
@@ -473,6 +496,7 @@ static float stiffness_of(double k_stiff, int substep) {
 }
 
 int DeviceSim::run_step(const DevParams& P, const Params& prm) {
+  if (prof) prof_collect_ready();
   const bool collect = collect_iters > 0;
   const bool warm = !collect && solver.warm_start && mlp.ready;
   SPHPC_RC(find_neighbors(P, true, false, warm || collect));

@@ -183,7 +183,7 @@ __device__ __forceinline__ void for_each_neighbor_nr(const NbrView& v, const uin
 
 // The same with a second per-neighbour array (velocity, colour) fetched in
 // the same batch: f(q, rq, eq).
-template <int B, class F>
+template <int B, bool kPadSlots = false, class F>
 __device__ __forceinline__ void for_each_neighbor_nr2(const NbrView& v,
                                                       const uint4* __restrict__ nr,
                                                       const float4* __restrict__ extra, int p,
@@ -207,7 +207,7 @@ __device__ __forceinline__ void for_each_neighbor_nr2(const NbrView& v,
     for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
 #pragma unroll
     for (int u = 0; u < B; ++u)
-      if (j0 + u < cnt) f(q[u], r[u], e[u]);
+      if (kPadSlots || j0 + u < cnt) f(q[u], r[u], e[u]);
 #pragma unroll
     for (int u = 0; u < B; ++u) q[u] = qn[u];
   }
