@@ -20,13 +20,18 @@ struct Pair {
 // neighbours whose list entries and records are fetched together
 constexpr int kNbrBatch = 4;
 // resident 256-thread blocks per SM asked of the compiler for the neighbour
-// passes (register caps of 40 and 48; more resident warps hide the gather
-// latency better than the registers a larger allocation would keep)
+// passes (register caps of 40, 48 and 64; more resident warps hide the gather
+// latency better than the registers a larger allocation would keep, as long
+// as the neighbour loop itself does not spill: the position pass spills only
+// in its FP64 epilogue at 40)
 constexpr int kMinBlocksDensity = 6;
-constexpr int kMinBlocksPosition = 5;
+constexpr int kMinBlocksPosition = 6;
 constexpr int kMinBlocksColor = 5;
 constexpr int kMinBlocksVorticity = 5;
 constexpr int kMinBlocksConfinement = 6;
+constexpr int kMinBlocksTension = 4;  // 64 registers: at 48 the loop spills
+constexpr int kMinBlocksXsph = 4;
+constexpr int kMinBlocksFeatures = 4;
 
 // x*_p - x*_q as (x_p - x_q) + (d_p - d_q): exact in the first term for any
 // box size, so the FP32 pair geometry keeps its relative precision.
@@ -162,7 +167,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
 // RAW: FP32 features to feat[p][16]; otherwise the network's input row
 // bf16((f - mean) * inv_std) (norm = mean[16], inv_std[16]) to xbf[p][16].
 template <bool RAW>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kMinBlocksFeatures)
     k_features(const DevParams P, const NbrView V, const PassArgs a, float* __restrict__ feat,
                __nv_bfloat16* __restrict__ xbf, const float* __restrict__ norm, int limit) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -394,7 +399,7 @@ __device__ __forceinline__ float cohesion(const DevParams& P, float r) {
   return P.C_norm * c;
 }
 
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kMinBlocksTension)
     k_tension(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
@@ -430,7 +435,7 @@ __global__ void __launch_bounds__(kBlock)
   a.vel[p] = v;
 }
 
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kMinBlocksXsph)
     k_xsph(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
