@@ -157,7 +157,9 @@ struct SphpcSolver {
   int adaptive;               /* 1: iterate until max density error <=
                                  density_tolerance or max_iterations */
   double density_tolerance;
-  int max_iterations;
+  int max_iterations;         /* cap on the position passes of a step, the
+                                 warm-start pass included (solve_iterations
+                                 likewise without adaptive) */
   int warm_start;             /* 1: MLP warm start of the first iteration */
   int lambda_epsilon_mass_units; /* 1: lambda_epsilon is added before the
                                     1/rho0^2 normalisation (particles.c:661),

@@ -608,8 +608,11 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       }
     }
   }
-  const int first_plain = plain;
-  while (!converged && plain - first_plain < plain_cap) {
+  // The cap counts every position pass of the step, a warm pass (kept or
+  // discarded) included, so that both arms of a comparison get the same work
+  // budget.
+  bool fused_velocity = false;
+  while (!converged && iters < plain_cap) {
     const uint4* src = ready;
     ready = nullptr;
     if (!src) {
@@ -638,12 +641,12 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       launch_accum_lambda(src, stiff, collect_target, (int)collect_rows, stream);
       launches += 1;
     }
-    const bool last = !adaptive && plain - first_plain == plain_cap - 1;
+    const bool last = !adaptive && iters == plain_cap - 1;
     pass_b(src, stiff, last);
+    fused_velocity = last;
     ++plain;
     ++iters;
   }
-  const bool fused_velocity = !adaptive && plain - first_plain == plain_cap && plain_cap > 0;
   if (!fused_velocity) {
     // converged (or capped, or no plain pass): velocities from x* and the
     // freshest density
