@@ -283,7 +283,8 @@ def run_ours(args, world, rank, local, dist):
         if warm:
             sim.mlp_load(net[0], net[1])
             sim.set_solver(warm_start=1,
-                           warm_start_scale=float(net[2].get("warm_start_scale", 1.0)))
+                           warm_start_scale=float(net[2].get("warm_start_scale", 1.0)),
+                           warm_start_min_error=float(net[2].get("warm_start_min_error", 0.0)))
         log(f"[rank {rank}] {args.config}: {sim.n} particles, warm start {warm}, "
             f"init {time.perf_counter()-t_init:.1f}s")
         return sim
@@ -372,7 +373,9 @@ def run_ours(args, world, rank, local, dist):
                               + (f"; stop when two iterations lower it by < "
                                  f"{100 * args.min_progress:g}%" if args.min_progress > 0 else "")
                               + ")")
-                   + (", MLP warm start" if warm is not None else ", plain (no network file)"),
+                   + ((", MLP warm start (network skipped at feature-pass error <= "
+                       f"{float(net[2].get('warm_start_min_error', 0.0)):g})")
+                      if warm is not None else ", plain (no network file)"),
                    "plain": arm_summary(plain),
                    "warm_start": arm_summary(warm),
                    "warm_start_weights": (os.path.relpath(args.weights, ROOT)

@@ -172,6 +172,11 @@ struct SphpcSolver {
                                  iterations together lower the FP64 max density
                                  error by less than this fraction; 0 (default):
                                  off */
+  double warm_start_min_error; /* warm start: run the network only when the
+                                 feature pass's FP64 max density error is
+                                 above this (0, the default: always); below
+                                 it the step is a plain solve from the
+                                 feature pass's lambda_0 */
 };
 
 /* FP64 reductions over the local particles. */

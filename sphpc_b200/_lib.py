@@ -77,7 +77,8 @@ class Solver(C.Structure):
                 ("density_tolerance", C.c_double), ("max_iterations", C.c_int),
                 ("warm_start", C.c_int), ("lambda_epsilon_mass_units", C.c_int),
                 ("warm_start_gate", C.c_int), ("pad_warm", C.c_int),
-                ("warm_start_scale", C.c_double), ("min_progress", C.c_double)]
+                ("warm_start_scale", C.c_double), ("min_progress", C.c_double),
+                ("warm_start_min_error", C.c_double)]
 
 
 class FileIO(C.Structure):

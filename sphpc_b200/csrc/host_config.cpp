@@ -214,6 +214,7 @@ void sphpc_default_solver(struct SphpcSolver* s) {
   s->pad_warm = 0;
   s->warm_start_scale = 1.0;
   s->min_progress = 0.0;
+  s->warm_start_min_error = 0.0;
 }
 
 void sphpc_set_default_solver(const struct SphpcSolver* s) {

@@ -578,6 +578,10 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     SPHPC_RC(read_resid(err0));
     if (err0 <= tol && adaptive) {
       converged = true;
+    } else if (err0 <= solver.warm_start_min_error) {
+      // a mildly compressed step: the plain solve from the feature pass's
+      // lambda_0 converges in a pass or two, which the network cannot beat
+      ready = nr_alt;
     } else {
       {
         Scope sc(this, "mlp_forward");

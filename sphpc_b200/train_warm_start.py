@@ -16,7 +16,10 @@ on a half cosine to 1e-5, batch 65,536, ten passes) by the library's
 tensor-core kernels, and evaluated on a
 collected step of a seed that was not trained on (seed 9); runs of that seed
 also choose the multiplier applied to the network's Lambda (0.5, 0.75 or 1:
-the fewest mean iterations), stored with the network.  The network file
+the fewest mean iterations) and the feature-pass residual below which the
+network is skipped (0, 2, 3 or 5 times the tolerance: the shortest run time),
+both stored with the network (`--reselect` redoes only these two choices for
+an existing network).  The network file
 and a JSON log (loss curve, data sizes, held-out fit) are written.
 """
 from __future__ import annotations
@@ -35,7 +38,7 @@ SCENES = ("dam_break_1m", "obstacle_4m")
 
 
 def collect_scene(config, seed, collect_at, iterations, tol, log):
-    solver = {"adaptive": 1, "density_tolerance": tol, "max_iterations": 12, "seed": seed}
+    solver = solver_for(tol, seed)
     rows = 0
     t0 = time.perf_counter()
     with Simulation(config, solver) as sim:
@@ -80,10 +83,17 @@ def held_out_fit(params, norm, config, seed, collect_at, iterations, tol):
             "baseline_scale": a}
 
 
+# the solver settings of the comparison the network is chosen for: tolerance
+# `tol`, 12 passes at most, the stall stop at 2% over two iterations
+def solver_for(tol, seed):
+    return {"adaptive": 1, "density_tolerance": tol, "max_iterations": 12, "seed": seed,
+            "min_progress": 0.02}
+
+
 def iterations_with(params, norm, config, seed, scale, pre, steps, tol):
     """Mean constraint iterations per step over `steps` steps after `pre`
     plain steps; scale None = the plain solver."""
-    solver = {"adaptive": 1, "density_tolerance": tol, "max_iterations": 12, "seed": seed}
+    solver = solver_for(tol, seed)
     with Simulation(config, solver) as sim:
         sim.step(pre)
         if scale is not None:
@@ -113,6 +123,42 @@ def choose_scale(params, norm, scenes, seed, tol, scales=(0.5, 0.75, 1.0),
     return best, table
 
 
+def seconds_with(params, norm, config, seed, scale, min_error, steps, tol, repeats=2):
+    """Device-synchronised seconds of `steps` warm-started steps after 3
+    warm-up steps (the fastest of `repeats` runs)."""
+    import torch
+    best = float("inf")
+    for _ in range(repeats):
+        with Simulation(config, solver_for(tol, seed)) as sim:
+            sim.mlp_load(params, norm)
+            sim.set_solver(warm_start=1, warm_start_scale=scale, warm_start_min_error=min_error)
+            sim.step(3)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sim.step(steps)
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - t0)
+    return best
+
+
+def choose_min_error(params, norm, scenes, seed, tol, scale, factors=(0.0, 2.0, 3.0, 5.0),
+                     steps=300):
+    """The feature-pass residual below which the network is skipped (a
+    multiple of the tolerance), by the run time of held-out runs: a mildly
+    compressed step converges in a plain pass or two, which the network's
+    cost cannot beat."""
+    table = {}
+    for f in factors:
+        tot = 0.0
+        for config in scenes:
+            sec = seconds_with(params, norm, config, seed, scale, f * tol, steps, tol)
+            table[f"{config} min_error {f:g} tol (s)"] = sec
+            tot += sec
+        table[f"total min_error {f:g} tol (s)"] = tot
+    best = min(factors, key=lambda f: table[f"total min_error {f:g} tol (s)"])
+    return best * tol, table
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--out", default=ws.DEFAULT_WEIGHTS)
@@ -131,6 +177,9 @@ def main(argv=None):
     ap.add_argument("--capacity", type=int, default=230_000_000)
     ap.add_argument("--no-held-out", action="store_true")
     ap.add_argument("--scenes", default=",".join(SCENES))
+    ap.add_argument("--reselect", action="store_true",
+                    help="keep the network in --out and only redo the held-out choices "
+                         "(scale, network threshold)")
     args = ap.parse_args(argv)
     logf = args.log or os.path.splitext(args.out)[0] + "_log.json"
     lines = []
@@ -141,6 +190,28 @@ def main(argv=None):
 
     scenes = args.scenes.split(",")
     collect_at = sorted({int(x) for x in args.collect_at.split(",")})
+    if args.reselect:
+        params, norm, meta = ws.load_network(args.out)
+        scale, table = choose_scale(params, norm, scenes, args.seeds + 1, args.tol)
+        for k, v in table.items():
+            log(f"held-out mean iterations {k}: {v:.2f}")
+        min_error, ttable = choose_min_error(params, norm, scenes, args.seeds + 1, args.tol,
+                                             scale)
+        for k, v in ttable.items():
+            log(f"held-out {k}: {v:.3f}")
+        log(f"warm-start scale {scale}, network skipped at feature-pass error <= {min_error:g}")
+        meta.update({"warm_start_scale": scale, "warm_start_min_error": min_error})
+        ws.save_network(args.out, params, norm, meta)
+        with open(logf) as fh:
+            old = json.load(fh)
+        old["meta"] = meta
+        old["held_out_iterations"] = table
+        old["held_out_seconds"] = ttable
+        old["log"] = old.get("log", []) + lines
+        with open(logf, "w") as fh:
+            json.dump(old, fh, indent=1)
+        log(f"rewrote {args.out} and {logf}")
+        return
     t0 = time.perf_counter()
     ws.dataset_reserve(args.capacity)
     ws.dataset_clear()
@@ -174,9 +245,13 @@ def main(argv=None):
         params, norm, scenes, args.seeds + 1, args.tol)
     for k, v in table.items():
         log(f"held-out mean iterations {k}: {v:.2f}")
-    log(f"warm-start scale {scale}")
+    min_error, ttable = (0.0, {}) if args.no_held_out else choose_min_error(
+        params, norm, scenes, args.seeds + 1, args.tol, scale)
+    for k, v in ttable.items():
+        log(f"held-out {k}: {v:.3f}")
+    log(f"warm-start scale {scale}, network skipped at feature-pass error <= {min_error:g}")
     meta = {"features": list(ws.FEATURES), "rows": int(n), "steps": steps,
-            "warm_start_scale": scale,
+            "warm_start_scale": scale, "warm_start_min_error": min_error,
             "batch": args.batch, "lr": args.lr, "lr_final": args.lr_final,
             "weight_decay": args.weight_decay,
             "scenes": scenes, "seeds": list(range(1, args.seeds + 1)),
@@ -188,7 +263,8 @@ def main(argv=None):
         json.dump({"meta": meta, "collect_seconds": t_collect, "train_seconds": t_train,
                    "rows_per_second": steps * args.batch / t_train,
                    "loss_every": every, "loss": [float(x) for x in loss[::every]],
-                   "held_out": fit, "held_out_iterations": table, "log": lines}, fh,
+                   "held_out": fit, "held_out_iterations": table,
+                   "held_out_seconds": ttable, "log": lines}, fh,
                   indent=1)
     ws.dataset_free()
     log(f"wrote {args.out} and {logf}")
