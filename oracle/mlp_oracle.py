@@ -6,12 +6,12 @@ of the PBF constraint solve whose plain iteration is particles.c:588-746
 kernels in sphpc_b200/csrc/mlp.cu compute, so that tests can check them:
 
   x0 = bf16((f - mean) * inv_std)                          16 features
-  z1 = x0 . bf16(W1)^T + bf16(b1),  h1 = bf16(gelu(z1))    64
-  z2 = h1 . bf16(W2)^T + bf16(b2),  h2 = bf16(gelu(z2))    64
-  z3 = h2 . bf16(W3)^T + bf16(b3),  h3 = gelu(z3)          64 (FP32)
+  z1 = x0 . bf16(W1)^T + bf16(b1),  h1 = bf16(relu(z1))    64
+  z2 = h1 . bf16(W2)^T + bf16(b2),  h2 = bf16(relu(z2))    64
+  z3 = h2 . bf16(W3)^T + bf16(b3),  h3 = relu(z3)          64 (FP32)
   u  = w4 . h3 + b4,           lambda0 = out_scale * u
 
-gelu is the tanh form 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))).
+relu(z) = max(z, 0), with derivative 1 for z > 0 and 0 otherwise.
 With bf16=False every rounding is skipped and the arithmetic is float64:
 that variant is the one the finite-difference gradient check runs on.
 
@@ -37,9 +37,6 @@ OFF_B4 = OFF_W4 + N_HID
 N_PARAMS = OFF_B4 + 1  # 9473
 N_NORM = 2 * N_IN + 1
 
-_GC = np.sqrt(2.0 / np.pi)
-_GA = 0.044715
-
 
 def bf16(a):
     """Round float32 values to the nearest bfloat16 (ties to even), kept as float32."""
@@ -49,13 +46,12 @@ def bf16(a):
     return u.astype(np.uint32).view(np.float32)
 
 
-def gelu(z):
-    return 0.5 * z * (1.0 + np.tanh(_GC * (z + _GA * z ** 3)))
+def relu(z):
+    return np.maximum(z, 0.0)
 
 
-def gelu_grad(z):
-    t = np.tanh(_GC * (z + _GA * z ** 3))
-    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _GC * (1.0 + 3.0 * _GA * z * z)
+def relu_grad(z):
+    return (z > 0.0).astype(np.float64)
 
 
 def unpack(params):
@@ -110,7 +106,7 @@ def forward(params, norm, feat, bf16_emulation=True):
     for l in range(3):
         z = h @ W[l].T + b[l]
         zs.append(z)
-        a = gelu(z)
+        a = relu(z)
         h = rnd(a) if l < 2 else a
         hs.append(h)
     u = h @ q["w4"].astype(np.float64) + float(q["b4"])
@@ -133,14 +129,14 @@ def loss_and_grad(params, norm, feat, target, bf16_emulation=True):
     g[OFF_W4:OFF_B4] = rnd(gu) @ rnd(hs[3])
     g[OFF_B4] = rnd(gu).sum()
     # dz of the last hidden layer; with bf16 emulation the kernels keep dz in bf16
-    dz = rnd(np.outer(gu, c["w4"]) * gelu_grad(zs[2]))
+    dz = rnd(np.outer(gu, c["w4"]) * relu_grad(zs[2]))
     offs = ((OFF_W1, OFF_B1), (OFF_W2, OFF_B2), (OFF_W3, OFF_B3))
     for l in (2, 1, 0):
         ow, ob = offs[l]
         g[ow:ob] = (dz.T @ hs[l]).ravel()
         g[ob:ob + N_HID] = dz.sum(axis=0)
         if l > 0:
-            dz = rnd((dz @ W[l]) * gelu_grad(zs[l - 1]))
+            dz = rnd((dz @ W[l]) * relu_grad(zs[l - 1]))
     return loss, g
 
 

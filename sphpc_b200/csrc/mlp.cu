@@ -7,7 +7,7 @@
 // memory (64 columns), issued by one thread as K/16 tcgen05.mma instructions
 // and completed through tcgen05.commit on an mbarrier.  Thread t then owns
 // particle t of the tile: it reads row t of D (tcgen05.ld 32x32b), adds the
-// bias, applies GELU and writes row t of the next layer's A.
+// bias, applies ReLU and writes row t of the next layer's A.
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -99,23 +99,11 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 
 }  // namespace tc
 
-// GELU, tanh form (Hendrycks & Gimpel 2016):
-// 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), with the tanh argument
-// written x (c + c a x^2) and the result hx + hx t, hx = x / 2.
-constexpr float kGeluC = 0.7978845608028654f;
-constexpr float kGeluCA = 0.7978845608028654f * 0.044715f;
-
-__device__ __forceinline__ float tanh_approx(float u) {
-  float t;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-  return t;
-}
-
-__device__ __forceinline__ float gelu_tanh(float x) {
-  const float t = tanh_approx(x * fmaf(kGeluCA, x * x, kGeluC));
-  const float hx = 0.5f * x;
-  return fmaf(hx, t, hx);
-}
+// The hidden activation, ReLU: one min/max per element on the FMA pipe, so
+// the epilogues between the tensor-core layers cost next to nothing (a
+// smooth activation would spend a multi-function-unit op per element, which
+// bounds a 64-wide layer well below the tensor cores).
+__device__ __forceinline__ float act(float x) { return fmaxf(x, 0.0f); }
 
 namespace {
 
@@ -193,7 +181,7 @@ size_t fwd_smem_bytes() { return sizeof(MlpSmem) + 128; }
 // One CTA of 128 threads per tile of 128 rows, tiles strided over the grid;
 // thread t owns row t.  Per tile: input row to x0, then three layers, each
 // one tcgen05.mma group into tensor memory (64 FP32 columns) followed by the
-// row's GELU epilogue; the last layer's FP32 activations meet w4 on the
+// row's ReLU epilogue; the last layer's FP32 activations meet w4 on the
 // CUDA cores.  BF16_IN: the rows are already the normalised BF16 input (32
 // bytes each); otherwise FP32 features normalised here.
 template <bool BF16_IN>
@@ -305,7 +293,7 @@ __global__ void __launch_bounds__(kMlpTile)
       if (!ok) break;
       tmem_row64(lane_base, 0, h);
 #pragma unroll
-      for (int j = 0; j < kMlpHidden; ++j) h[j] = gelu_tanh(h[j]);
+      for (int j = 0; j < kMlpHidden; ++j) h[j] = act(h[j]);
       if (l < 2) {
 #pragma unroll
         for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.h, kKcH, t, k0, h + k0);
@@ -387,13 +375,8 @@ struct TrainSmem {
 
 size_t train_smem_bytes() { return sizeof(TrainSmem) + 1024; }
 
-// d/dz of gelu_tanh: 0.5 (1 + t) + 0.5 z (1 - t^2) (c + 3 c a z^2).
-__device__ __forceinline__ float gelu_grad(float z) {
-  const float z2 = z * z;
-  const float t = tanh_approx(z * fmaf(kGeluCA, z2, kGeluC));
-  const float hz = 0.5f * z;
-  return fmaf(hz * (1.0f - t * t), fmaf(3.0f * kGeluCA, z2, kGeluC), 0.5f + 0.5f * t);
-}
+// d/dz of act: 1 for z > 0, else 0.
+__device__ __forceinline__ float act_grad(float z) { return z > 0.0f ? 1.0f : 0.0f; }
 
 // Weight gradient over the 128 rows of a tile: D[M=128][N] (+)= A^T B with A
 // = dz [rows x 128] and B = activations [rows x N], both read MN-major.
@@ -518,14 +501,14 @@ __global__ void __launch_bounds__(kMlpTile, 1)
       break;
     tmem_row64(lane_base, kTZ1, v);
 #pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) v[j] = gelu_tanh(v[j]);
+    for (int j = 0; j < kMlpHidden; ++j) v[j] = act(v[j]);
 #pragma unroll
     for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.h1, kKcH, t, k0, v + k0);
     if (!(ok = run([&] { mma_kk(taddr + kTZ2, sh1, kKcH, sw2, kKcH, kKH, tc::kIdescM128N64); })))
       break;
     tmem_row64(lane_base, kTZ2, v);
 #pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) v[j] = gelu_tanh(v[j]);
+    for (int j = 0; j < kMlpHidden; ++j) v[j] = act(v[j]);
 #pragma unroll
     for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.h2, kKcH, t, k0, v + k0);
     if (!(ok = run([&] { mma_kk(taddr + kTZ3, sh2, kKcH, sw3, kKcH, kKH, tc::kIdescM128N64); })))
@@ -534,7 +517,7 @@ __global__ void __launch_bounds__(kMlpTile, 1)
     float u = b4;
 #pragma unroll
     for (int j = 0; j < kMlpHidden; ++j) {
-      v[j] = gelu_tanh(v[j]);
+      v[j] = act(v[j]);
       u = fmaf(s.w4[j], v[j], u);
     }
 #pragma unroll
@@ -550,7 +533,7 @@ __global__ void __launch_bounds__(kMlpTile, 1)
     // layer 3
     tmem_row64(lane_base, kTZ3, v);
 #pragma unroll
-    for (int j = 0; j < kMlpHidden; ++j) v[j] = g * s.w4[j] * gelu_grad(v[j]);
+    for (int j = 0; j < kMlpHidden; ++j) v[j] = g * s.w4[j] * act_grad(v[j]);
 #pragma unroll
     for (int k0 = 0; k0 < kMlpHidden; k0 += 8) put8(s.dz, kKcD, t, k0, v + k0);
     if (!(ok = run([&] {
@@ -558,7 +541,7 @@ __global__ void __launch_bounds__(kMlpTile, 1)
           mma_dh(taddr + kTZ3, sdz, sw3);
         })))
       break;
-    // layer 2: dz2 = dh2 * gelu'(z2)
+    // layer 2: dz2 = dh2 * act'(z2)
 #pragma unroll
     for (int c = 0; c < kMlpHidden; c += 16) {
       float dh[16], z[16];
@@ -566,7 +549,7 @@ __global__ void __launch_bounds__(kMlpTile, 1)
       tc::tmem_ld16(lane_base + kTZ2 + c, z);
       tc::tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) dh[i] *= gelu_grad(z[i]);
+      for (int i = 0; i < 16; ++i) dh[i] *= act_grad(z[i]);
       put8(s.dz, kKcD, t, c, dh);
       put8(s.dz, kKcD, t, c + 8, dh + 8);
     }
@@ -583,7 +566,7 @@ __global__ void __launch_bounds__(kMlpTile, 1)
       tc::tmem_ld16(lane_base + kTZ1 + c, z);
       tc::tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) dh[i] *= gelu_grad(z[i]);
+      for (int i = 0; i < 16; ++i) dh[i] *= act_grad(z[i]);
       put8(s.dz, kKcD, t, c, dh);
       put8(s.dz, kKcD, t, c + 8, dh + 8);
     }

@@ -3,7 +3,7 @@
 // A per-particle MLP maps 16 neighbourhood features to an effective
 // multiplier lambda0 whose single position pass moves x* close to where the
 // plain constraint iterations would take it.  Network: 16 -> 64 -> 64 -> 64
-// (GELU, tanh form) -> 1; BF16 weights and activations on the 5th-generation
+// (ReLU) -> 1; BF16 weights and activations on the 5th-generation
 // tensor cores (tcgen05.mma, FP32 accumulators in tensor memory), FP32 last
 // layer.  Parameter vector (FP32, 9473 values):
 //   W1[64][16] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4
