@@ -176,7 +176,9 @@ struct SphpcSolver {
                                  feature pass's FP64 max density error is
                                  above this (0, the default: always); below
                                  it the step is a plain solve from the
-                                 feature pass's lambda_0 */
+                                 feature pass's lambda_0, and the next step
+                                 (adaptive) is a plain solve without the
+                                 feature pass */
 };
 
 /* FP64 reductions over the local particles. */

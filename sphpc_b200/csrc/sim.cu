@@ -92,6 +92,7 @@ class DeviceSim {
   uint4 *nr = nullptr, *nr_alt = nullptr;  // 16-byte neighbour records (x* fixed point, payload)
   uint4* nr_w = nullptr;         // third record buffer (warm start, feature export)
   int last_warm_rejected = 0;
+  double prev_err0 = -1.0;       // first residual of the previous step (< 0: none)
   std::vector<double> trace;     // max density error at each evaluation of the step
   // training-set collection of the current step (collect_iters > 0)
   int collect_iters = 0;
@@ -498,7 +499,13 @@ static float stiffness_of(double k_stiff, int substep) {
 int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   if (prof) prof_collect_ready();
   const bool collect = collect_iters > 0;
-  const bool warm = !collect && solver.warm_start && mlp.ready;
+  // A step whose predecessor started mildly compressed (first residual at or
+  // below warm_start_min_error) is solved plainly, without the feature pass:
+  // consecutive steps' first residuals are close, and such a step converges
+  // in a pass or two that the network cannot beat.
+  const bool mild = solver.warm_start_min_error > 0.0 && prev_err0 >= 0.0 &&
+                    prev_err0 <= solver.warm_start_min_error;
+  const bool warm = !collect && solver.warm_start && mlp.ready && !mild;
   SPHPC_RC(find_neighbors(P, true, false, warm || collect));
   const NbrView V = view();
   PassArgs a{};
@@ -664,6 +671,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   }
   last_iterations = iters;
   last_converged = converged ? 1 : 0;
+  prev_err0 = (adaptive && !trace.empty()) ? trace[0] : -1.0;
   // post-solve passes (simulation.c:93-106) on the records nr (payload: the
   // density); the last one writes x = x*, d = 0 (UpdatePositions) into pd_alt
   a.pd = pd;

@@ -127,3 +127,36 @@ def test_trained_network_reduces_iterations():
             res[arm] = float(np.mean(its))
     print(res)
     assert res["warm"] <= 0.95 * res["plain"], res
+
+
+def test_network_threshold_skips_mild_steps():
+    """warm_start_min_error: a step whose first density pass finds the max
+    density error at or below it skips the network, and the next step skips
+    the feature pass too (a plain solve); with 0 every step runs the feature
+    pass (and the network where the error is above the tolerance)."""
+    params, norm, meta = ws.load_network()
+    tol = 0.002
+    solver = {"adaptive": 1, "density_tolerance": tol, "max_iterations": 12}
+    # (plain steps before the network is loaded, threshold)
+    for pre, min_error in ((0, 1.0), (5, 1.0), (5, 0.0)):
+        with Simulation("small_dam", solver) as sim:
+            sim.step(pre)
+            sim.mlp_load(params, norm)
+            sim.set_solver(warm_start=1, warm_start_min_error=min_error)
+            sim.profile(True)
+            above, used = 0, 0
+            for _ in range(3):
+                sim.step(1)
+                d = sim.last_step_info()
+                above += d["trace"][0] > tol
+                used += d["warm_start_used"]
+            prof = sim.profile_read()
+            features = prof.get("mlp_features", (0, 0.0))[0]
+            forward = prof.get("mlp_forward", (0, 0.0))[0]
+            if min_error == 0.0:
+                assert (features, forward, used) == (3, above, above), (prof, above)
+            else:
+                # no earlier step: the first step runs the feature pass (and finds
+                # a mild step); after that, and after plain steps, none does
+                assert (features, forward, used) == (1 if pre == 0 else 0, 0, 0), (pre, prof)
+            assert sim.device_errors() == 0
