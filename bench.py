@@ -423,7 +423,8 @@ def run_e2e(sim, args, dist, world, n):
     """Host buffers in, host buffers out, through the public C API: upload the
     state from the host arrays (x, v), K steps each followed by the FP64
     diagnostics read-back, the reference's output frame (x, y, z, density
-    every 1/(30 dt) steps, simulation.c:113-114), and the final state."""
+    every 1/(30 dt) steps, simulation.c:113-114, read back asynchronously),
+    and the final state."""
     import torch
     fields_in = ["x", "y", "z", "v_x", "v_y", "v_z"]
     frame_fields = ["x", "y", "z", "density"]
@@ -440,8 +441,11 @@ def run_e2e(sim, args, dist, world, n):
         sim.step(1)
         sim.diagnostics()
         if k % frame_every == 0:
-            sim.fetch_fields(frame_fields)
+            # the frame crosses the link while the next steps run; the next
+            # frame (or the final read-back) waits for it first
+            sim.fetch_fields_async(frame_fields)
             frames += 1
+    sim.host_wait()
     sim.fetch_fields(out_fields)
     torch.cuda.synchronize()
     dt = max_over_ranks(time.perf_counter() - t0, dist, "cuda")

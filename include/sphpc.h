@@ -90,6 +90,15 @@ int sphpc_update_host(struct Particles *particles);    /* device -> host, all fi
  * e.g. (1<<3)|(1<<4)|(1<<5)|(1<<18) for the output frame of
  * fileio_adios.c:73-76. */
 int sphpc_update_host_fields(struct Particles *particles, unsigned int field_mask);
+/* The same read-back, returning once it is enqueued: the fields are gathered
+ * on the particle set's stream and copied to the host arrays on a copy
+ * stream of the particle set, so the steps that follow run while the frame
+ * crosses the link.  The host arrays hold the frame only after
+ * sphpc_host_wait; every other transfer of the set (and the next
+ * asynchronous read-back) waits for it first.  No counterpart in the
+ * reference, whose acc update host waits for the copy. */
+int sphpc_update_host_fields_async(struct Particles *particles, unsigned int field_mask);
+int sphpc_host_wait(struct Particles *particles);
 /* Host -> device of selected field groups (same bit numbering; a group
  * such as x/y/z is uploaded when all its bits are set; x/y/z are required). */
 int sphpc_update_device_fields(struct Particles *particles, unsigned int field_mask);

@@ -140,6 +140,8 @@ SIGNATURES = {
     "sphpc_update_host": ([PP], C.c_int),
     "sphpc_update_device": ([PP], C.c_int),
     "sphpc_update_host_fields": ([PP, C.c_uint], C.c_int),
+    "sphpc_update_host_fields_async": ([PP, C.c_uint], C.c_int),
+    "sphpc_host_wait": ([PP], C.c_int),
     "sphpc_update_device_fields": ([PP, C.c_uint], C.c_int),
     "sphpc_set_solver": ([PP, C.POINTER(Solver)], C.c_int),
     "sphpc_get_solver": ([PP, C.POINTER(Solver)], C.c_int),

@@ -125,6 +125,15 @@ class DeviceSim {
   uint32_t* err() { return small + 2; }
 
   void release() {
+    // a read-back in flight still writes the host arrays: finish it first
+    if (copy_stream) {
+      cudaStreamSynchronize(copy_stream);
+      cudaStreamDestroy(copy_stream);
+      cudaEventDestroy(gathered);
+      cudaEventDestroy(copied);
+      copy_stream = nullptr;
+      copy_pending = false;
+    }
     dfree(pd); dfree(pd_alt); dfree(vel); dfree(vel_alt);
     dfree(color); dfree(omega); dfree(dp); dfree(rho); dfree(lam);
     dfree(color_alt); dfree(omega_alt); dfree(dp_alt); dfree(rho_alt); dfree(lam_alt);
@@ -189,6 +198,28 @@ class DeviceSim {
 
   int ensure_stage() {
     if (!stage) SPHPC_RC(dalloc(&stage, (size_t)20 * n));
+    return SPHPC_OK;
+  }
+
+  // asynchronous read-back: copy stream and its events, created on first use
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t gathered = nullptr, copied = nullptr;
+  bool copy_pending = false;
+
+  int ensure_copy_stream() {
+    if (copy_stream) return SPHPC_OK;
+    SPHPC_CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    SPHPC_CK(cudaEventCreateWithFlags(&gathered, cudaEventDisableTiming));
+    SPHPC_CK(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+    return SPHPC_OK;
+  }
+
+  // Waits for an asynchronous read-back in flight (the staging buffer and
+  // the host arrays are then free).
+  int wait_copies() {
+    if (!copy_pending) return SPHPC_OK;
+    copy_pending = false;
+    SPHPC_CK(cudaEventSynchronize(copied));
     return SPHPC_OK;
   }
 
@@ -981,9 +1012,15 @@ int sphpc_set_stream(struct Particles* particles, void* cuda_stream) {
 
 int sphpc_update_host(struct Particles* p) { return sphpc_update_host_fields(p, 0xFFFFFFFFu); }
 
-int sphpc_update_host_fields(struct Particles* p, unsigned int field_mask) {
-  SPHPC_SIM(s, p);
+namespace {
+
+// Gathers the fields of field_mask into the staging buffer (original particle
+// order, doubles) and copies them to the host arrays: on the particle set's
+// stream, or, with async, on its copy stream after the gather.
+int download_fields(Particles* p, DeviceSim* s, unsigned int field_mask, bool async) {
+  SPHPC_RC(s->wait_copies());
   SPHPC_RC(s->ensure_stage());
+  if (async) SPHPC_RC(s->ensure_copy_stream());
   const int n = s->n;
   double* fields[20] = {p->x_star, p->y_star, p->z_star, p->x, p->y, p->z, p->v_x, p->v_y,
                         p->v_z, p->dp_x, p->dp_y, p->dp_z, p->w_x, p->w_y, p->w_z,
@@ -995,11 +1032,22 @@ int sphpc_update_host_fields(struct Particles* p, unsigned int field_mask) {
                                                     s->omega, s->color, s->rho, s->lam, mask,
                                                     s->stage);
   SPHPC_CK(cudaGetLastError());
+  cudaStream_t cs = s->stream;
+  if (async) {
+    SPHPC_CK(cudaEventRecord(s->gathered, s->stream));
+    SPHPC_CK(cudaStreamWaitEvent(s->copy_stream, s->gathered, 0));
+    cs = s->copy_stream;
+  }
   for (int k = 0; k < 20; ++k)
-    if (fields[k] && (field_mask & (1u << k)))
+    if (mask & (1u << k))
       SPHPC_CK(cudaMemcpyAsync(fields[k], s->stage + (size_t)k * n, sizeof(double) * n,
-                               cudaMemcpyDeviceToHost, s->stream));
-  SPHPC_CK(cudaStreamSynchronize(s->stream));
+                               cudaMemcpyDeviceToHost, cs));
+  if (async) {
+    SPHPC_CK(cudaEventRecord(s->copied, s->copy_stream));
+    s->copy_pending = true;
+  } else {
+    SPHPC_CK(cudaStreamSynchronize(s->stream));
+  }
   // the host arrays are in original order: ids are the identity (written on
   // full updates; a field subset leaves them as they are)
   if (p->id && field_mask == 0xFFFFFFFFu)
@@ -1007,10 +1055,28 @@ int sphpc_update_host_fields(struct Particles* p, unsigned int field_mask) {
   return SPHPC_OK;
 }
 
+}  // namespace
+
+int sphpc_update_host_fields(struct Particles* p, unsigned int field_mask) {
+  SPHPC_SIM(s, p);
+  return download_fields(p, s, field_mask, false);
+}
+
+int sphpc_update_host_fields_async(struct Particles* p, unsigned int field_mask) {
+  SPHPC_SIM(s, p);
+  return download_fields(p, s, field_mask, true);
+}
+
+int sphpc_host_wait(struct Particles* p) {
+  SPHPC_SIM(s, p);
+  return s->wait_copies();
+}
+
 int sphpc_update_device(struct Particles* p) { return sphpc_update_device_fields(p, 0xFFFFFFFFu); }
 
 int sphpc_update_device_fields(struct Particles* p, unsigned int field_mask) {
   SPHPC_SIM(s, p);
+  SPHPC_RC(s->wait_copies());
   SPHPC_RC(s->ensure_stage());
   const int n = s->n;
   const double* fields[20] = {p->x_star, p->y_star, p->z_star, p->x, p->y, p->z, p->v_x,

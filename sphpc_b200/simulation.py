@@ -94,6 +94,18 @@ class Simulation:
             mask |= 1 << PARTICLE_FIELDS.index(f)
         call("sphpc_update_host_fields", C.byref(self.particles), mask)
 
+    def fetch_fields_async(self, fields):
+        """Device -> host of the named fields, returning once enqueued: the
+        copy overlaps the steps that follow; the host arrays hold the fields
+        after host_wait() (every other transfer waits for it first)."""
+        mask = 0
+        for f in fields:
+            mask |= 1 << PARTICLE_FIELDS.index(f)
+        call("sphpc_update_host_fields_async", C.byref(self.particles), mask)
+
+    def host_wait(self):
+        call("sphpc_host_wait", C.byref(self.particles))
+
     def push_fields(self, fields):
         """Host -> device of the named fields (groups must be complete)."""
         mask = 0
