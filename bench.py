@@ -325,6 +325,9 @@ def run_ours(args, world, rank, local, dist):
             roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak,
                     "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": ncu_traffic(name, n), "bytes_per_particle": per,
+                    # the neighbour passes are bound by instruction issue, not
+                    # by HBM: the share of cycles their schedulers issued
+                    "issue_active_ncu": ncu_stage(name).get("issue_active_pct"),
                     "avg_launch_ms": tot / cnt}
 
     # end to end through the C ABI with host buffers, over the same steps of
@@ -406,17 +409,21 @@ def sim_passes(sim):
     return (bits + 7) // 8
 
 
-def ncu_traffic(stage, n):
-    """DRAM bytes per launch of `stage` from the committed ncu summary, scaled
-    to n particles (profiles/ncu_traffic.json), or None."""
+def ncu_stage(stage):
+    """The committed ncu figures of `stage` (profiles/ncu_traffic.json), or {}."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
-            d = json.load(f)
-        e = d[stage]
-        return e["bytes_per_particle"] * n
+            return json.load(f).get(stage, {})
     except Exception:
-        return None
+        return {}
+
+
+def ncu_traffic(stage, n):
+    """DRAM bytes per launch of `stage` from the committed ncu summary, scaled
+    to n particles, or None."""
+    e = ncu_stage(stage)
+    return e["bytes_per_particle"] * n if "bytes_per_particle" in e else None
 
 
 def run_e2e(sim, args, dist, world, n):
