@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
       const float fx = (float)(int)(rp.x - rq.x);
       const float fy = (float)(int)(rp.y - rq.y);
       const float fz = (float)(int)(rp.z - rq.z);
-      const float r2 = (fx * fx + fy * fy + fz * fz) * P.fx_inv2;
+      const float r2f = fx * fx + fy * fy + fz * fz;
+      const float r2 = r2f * P.fx_inv2;
       if (MODE != 2) {
         const float t = fmaxf(P.h2 - r2, 0.0f);
         const float y = t * t * t - comp;
@@ -125,11 +126,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
         floored_r(P, r2, r, rinv);
         const float hm = fmaxf(P.h - r, 0.0f);
         const float c = hm * hm * rinv;
-        const float gx = c * fx, gy = c * fy, gz = c * fz;
-        sgx += gx;
-        sgy += gy;
-        sgz += gz;
-        sC += gx * gx + gy * gy + gz * gz;
+        // |c d|^2 = c^2 |d|^2: three fused accumulations and one for the norm
+        sgx = fmaf(c, fx, sgx);
+        sgy = fmaf(c, fy, sgy);
+        sgz = fmaf(c, fz, sgz);
+        sC = fmaf(c * c, r2f, sC);
       }
     });
     float rho;
@@ -412,6 +413,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
   // padding slots vanish (d = 0, c_p - c_q = 0)
   const float kcoh_fx = kcoh * P.fx_inv;  // for d in fixed-point units (exact)
   const float two_rho0 = 2.0f * P.rho0;
+  // kcur (c_p - c_q) = kcur c_p - kcur c_q
+  const float kpx = kcur * cp.x, kpy = kcur * cp.y, kpz = kcur * cp.z;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   for_each_neighbor_nr2<kNbrBatch, true>(V, a.nr, a.color, p,
                                          [&](int, const uint4 rq, const float4 cq) {
@@ -423,9 +426,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
     floored_r(P, r2, r, rinv);
     const float coh = kcoh_fx * cohesion(P, r) * rinv;
     const float K = two_rho0 * __frcp_rn(rp + nr_w(rq));
-    fx += K * (coh * dx + kcur * (cp.x - cq.x));
-    fy += K * (coh * dy + kcur * (cp.y - cq.y));
-    fz += K * (coh * dz + kcur * (cp.z - cq.z));
+    fx = fmaf(K, fmaf(coh, dx, fmaf(-kcur, cq.x, kpx)), fx);
+    fy = fmaf(K, fmaf(coh, dy, fmaf(-kcur, cq.y, kpy)), fy);
+    fz = fmaf(K, fmaf(coh, dz, fmaf(-kcur, cq.z, kpz)), fz);
   });
   float4 v = a.vel[p];
   const float s = P.dt / rp;
