@@ -204,7 +204,9 @@ def run_reference(args, world, rank):
     rs.ref.step(args.steps, rs.iterations)
     value = rs.n * args.steps / (time.perf_counter() - t0)
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "devices": "host CPU, one core (the reference's OpenACC path compiled with gcc has no "
+                   "device or multicore target)",
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.config, "sample": rs.desc},
