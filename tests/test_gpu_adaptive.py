@@ -4,6 +4,7 @@ optional stall stop (solver field min_progress)."""
 import numpy as np
 import pytest
 
+from helpers import assert_close, oracle_for, oracle_state
 from sphpc_b200 import Simulation
 
 pytestmark = pytest.mark.gpu
@@ -61,3 +62,31 @@ def test_stall_stop_ends_the_solve_without_converging():
         want = ref.fetch()
     for f in ("x", "y", "z"):
         np.testing.assert_array_equal(got[f], want[f], err_msg=f)
+
+
+def test_adaptive_step_matches_oracle_at_its_iteration_count():
+    """An adaptive step that converges after k position passes ends where the
+    FP64 oracle's step of k fixed iterations ends: the same positions, and
+    the velocities within a looser bound, since the converged step's post
+    passes read the density of its final check (one pass fresher than the
+    fixed-iteration step's); with surface tension, whose pair forces scale
+    with 2 rho0 / (rho_p + rho_q), that moves a few velocities by up to
+    ~1e-4 of the velocity scale."""
+    solver = {"adaptive": 1, "density_tolerance": 0.002, "max_iterations": 12}
+    for config in ("small_dam", "small_obstacle"):
+        with Simulation(config, solver) as sim:
+            sim.step(5)
+            st = sim.fetch()
+            o = oracle_for(sim, st)
+            sim.step(1)
+            d = sim.last_step_info()
+            k = d["iterations"]
+            assert d["converged"] == 1 and 1 <= k < 12, d
+            o.p.solve_iterations = k
+            o.step(1)
+            got, want = sim.fetch(), oracle_state(o)
+            for f in ("x", "y", "z"):
+                assert_close(got[f], want[f], 1e-6, 0.0, atol=1e-6, what=f"{config}:{f}")
+            for f in ("v_x", "v_y", "v_z"):
+                assert_close(got[f], want[f], 1e-4, 3e-4, what=f"{config}:{f}")
+            assert sim.device_errors() == 0
