@@ -292,12 +292,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksPosition)
     const float hm = fmaxf(P.h - r, 0.0f);
     float s = lp + nr_w(rq);
     if (SCORR_N != 0) {
-      const float t = fmaxf(P.h2 - r * r, 0.0f);
-      const float ratio = t * t * t * P.scorr_c;  // W(r) / W(dq)
+      // W(r) / W(dq) = u^3 with u = (h^2 - r^2) / (h^2 - dq^2), u <= 1.05
+      const float u = fmaxf(P.h2 - r * r, 0.0f) * P.scorr_u;
       if (SCORR_N == 4) {
-        const float q2 = ratio * ratio;
-        s = fmaf(-P.scorr_k * q2, q2, s);
+        const float u2 = u * u;
+        const float u4 = u2 * u2;
+        s = fmaf(-P.scorr_k, u4 * u4 * u4, s);
       } else {
+        const float ratio = u * u * u;
         float sc = -P.scorr_k;
         for (int e = 0; e < P.scorr_n; ++e) sc *= ratio;
         s += sc;

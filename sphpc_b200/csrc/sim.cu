@@ -414,7 +414,7 @@ DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob
     const double t = h * h - dq * dq;
     const double Wdq = dq > h ? 0.0 : prm.W_norm * t * t * t;
     P.inv_Wdq = Wdq > 0.0 ? (float)(1.0 / Wdq) : 0.0f;
-    P.scorr_c = Wdq > 0.0 ? (float)(prm.W_norm / Wdq) : 0.0f;
+    P.scorr_u = Wdq > 0.0 ? (float)(1.0 / t) : 0.0f;
     if (Wdq <= 0.0) P.scorr_k = 0.0f;
   }
   P.c_xsph = (float)prm.c;

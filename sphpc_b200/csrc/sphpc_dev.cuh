@@ -100,7 +100,7 @@ struct DevParams {
   float scorr_k;        // s_corr = -k (W/W(dq))^n
   int scorr_n;
   float inv_Wdq;
-  float scorr_c;        // W_norm / W(dq): W(r)/W(dq) = scorr_c (h^2 - r^2)^3
+  float scorr_u;        // 1 / (h^2 - dq^2): W(r)/W(dq) = ((h^2 - r^2) scorr_u)^3
   float c_xsph;
   int xsph_exact;       // 0: reference r expression (particles.c:439)
   float gamma, C_norm;  // surface tension
