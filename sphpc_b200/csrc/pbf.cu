@@ -68,6 +68,15 @@ __device__ __forceinline__ void floored_r(const DevParams& P, float r2, float& r
   r = r2c * rinv;
 }
 
+// The same in fixed-point units (r2f = |d|^2 of the record difference):
+// r_f = r 2^k and rinv_f = 2^-k / r, so the loops need no rescaling of r^2.
+__device__ __forceinline__ void floored_r_fx(const DevParams& P, float r2f, float& r2c,
+                                             float& r, float& rinv) {
+  r2c = fmaxf(r2f, P.rmin2_fx);
+  rinv = rsqrtf(r2c);
+  r = r2c * rinv;
+}
+
 __device__ __forceinline__ void block_resid(double e, double* resid) {
   // max and sum of the per-particle density error over the block (FP64).
   double m = e, s = e;
@@ -104,8 +113,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
     const uint4 rp = ld_nr(a.nr, p);
     // The loop keeps only what varies per pair: the density sums t^3 with
     // t = h^2 - r^2 (Kahan-compensated) and the gradient sums c d with
-    // c = (h - r)^2 / r and d the pair difference in fixed-point units; the
-    // kernel norms, the mass and 2^-k multiply the sums once afterwards.
+    // c = (h - r)^2 / r and d the pair difference, both in fixed-point units;
+    // the kernel norms, the mass and 2^-2k multiply the sums once afterwards.
     float st = 0.0f, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
     for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int, const uint4 rq) {
@@ -113,18 +122,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
       const float fy = (float)(int)(rp.y - rq.y);
       const float fz = (float)(int)(rp.z - rq.z);
       const float r2f = fx * fx + fy * fy + fz * fz;
-      const float r2 = r2f * P.fx_inv2;
       if (MODE != 2) {
-        const float t = fmaxf(P.h2 - r2, 0.0f);
+        const float t = fmaxf(fmaf(-P.fx_inv2, r2f, P.h2), 0.0f);
         const float y = t * t * t - comp;
         const float s = st + y;
         comp = (s - st) - y;
         st = s;
       }
       if (MODE != 1) {
-        float r, rinv;
-        floored_r(P, r2, r, rinv);
-        const float hm = fmaxf(P.h - r, 0.0f);
+        // in fixed-point units: c_f = (h_f - r_f)^2 / r_f = 2^k c
+        float r2c, r, rinv;
+        floored_r_fx(P, r2f, r2c, r, rinv);
+        const float hm = fmaxf(P.h_fx - r, 0.0f);
         const float c = hm * hm * rinv;
         // |c d|^2 = c^2 |d|^2: three fused accumulations and one for the norm
         sgx = fmaf(c, fx, sgx);
@@ -142,7 +151,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
     if (MODE != 1) {
       // ComputeLambda's constraint (particles.c:616-617) in FP64
       const float C = (float)fmax(__ddiv_rn((double)rho, P.rho0_d) - 1.0, 0.0);
-      const float g = P.DWn_m * P.fx_inv;  // gradient scale (2^-k is exact)
+      const float g = P.DWn_m * P.fx_inv2;  // gradient scale (2^-2k is exact)
       sC += sgx * sgx + sgy * sgy + sgz * sgz;
       sC *= (g * g) * P.inv_rho0_sq;
       const float lam = -C / (sC + P.lambda_eps);
@@ -278,22 +287,22 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksPosition)
   float4 xp, dp;  // own particle record, loaded ahead of the neighbour loop
   if (MODE == 0) ld_pd(a.pd, p, xp, dp);
   // sums of c d with c = (lambda_p + lambda_q + s_corr) (h - r)^2 / r and d
-  // the pair difference in fixed-point units; the spiky norm, the mass and
-  // 2^-k multiply them once afterwards.  Every term carries d, so the batch's
+  // the pair difference, both in fixed-point units; the spiky norm, the mass
+  // and 2^-2k multiply them once afterwards.  Every term carries d, so the batch's
   // padding slots (q = p, d = 0) add nothing and are not masked.
   float ax = 0.f, ay = 0.f, az = 0.f;
   for_each_neighbor_nr<kNbrBatch, true>(V, a.nr, p, [&](int, const uint4 rq) {
     const float fx = (float)(int)(rp.x - rq.x);
     const float fy = (float)(int)(rp.y - rq.y);
     const float fz = (float)(int)(rp.z - rq.z);
-    const float r2 = (fx * fx + fy * fy + fz * fz) * P.fx_inv2;
-    float r, rinv;
-    floored_r(P, r2, r, rinv);
-    const float hm = fmaxf(P.h - r, 0.0f);
+    // in fixed-point units: c_f = s (h_f - r_f)^2 / r_f = 2^k c
+    float r2c, r, rinv;
+    floored_r_fx(P, fx * fx + fy * fy + fz * fz, r2c, r, rinv);
+    const float hm = fmaxf(P.h_fx - r, 0.0f);
     float s = lp + nr_w(rq);
     if (SCORR_N != 0) {
       // W(r) / W(dq) = u^3 with u = (h^2 - r^2) / (h^2 - dq^2), u <= 1.05
-      const float u = fmaxf(P.h2 - r * r, 0.0f) * P.scorr_u;
+      const float u = fmaxf(fmaf(-P.scorr_u_fx, r2c, P.scorr_uh2), 0.0f);
       if (SCORR_N == 4) {
         const float u2 = u * u;
         const float u4 = u2 * u2;
@@ -310,7 +319,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksPosition)
     ay = fmaf(c, fy, ay);
     az = fmaf(c, fz, az);
   });
-  const float s = a.stiffness * P.inv_rho0 * (P.DWn_m * P.fx_inv);
+  const float s = a.stiffness * P.inv_rho0 * (P.DWn_m * P.fx_inv2);
   const float dpx = ax * s, dpy = ay * s, dpz = az * s;
   if (MODE == 1) {
     a.dp[p] = make_float4(dpx, dpy, dpz, 0.0f);

@@ -387,6 +387,8 @@ DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob
     P.fx_scale = ldexp(1.0, k);
     P.fx_inv = (float)ldexp(1.0, -k);
     P.fx_inv2 = (float)ldexp(1.0, -2 * k);
+    P.h_fx = (float)ldexp(h, k);
+    P.rmin2_fx = (float)ldexp(h * 0.0001 * h * 0.0001, 2 * k);
   }
   P.h2d = h * h;
   P.h = (float)h;
@@ -415,6 +417,8 @@ DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob
     const double Wdq = dq > h ? 0.0 : prm.W_norm * t * t * t;
     P.inv_Wdq = Wdq > 0.0 ? (float)(1.0 / Wdq) : 0.0f;
     P.scorr_u = Wdq > 0.0 ? (float)(1.0 / t) : 0.0f;
+    P.scorr_u_fx = P.scorr_u * P.fx_inv2;  // a power of two: exact
+    P.scorr_uh2 = P.scorr_u * P.h2;
     if (Wdq <= 0.0) P.scorr_k = 0.0f;
   }
   P.c_xsph = (float)prm.c;

@@ -86,6 +86,8 @@ struct DevParams {
   double fx_scale;      // 2^k: fixed-point units per length of the records
   float fx_inv;         // 2^-k
   float fx_inv2;        // 2^-2k
+  float h_fx;           // h in fixed-point units (h 2^k)
+  float rmin2_fx;       // (1e-4 h)^2 in fixed-point units squared
   double h2d;
   float h, h2;
   float rmin;           // r floor 1e-4 h (particles.c:636)
@@ -101,6 +103,8 @@ struct DevParams {
   int scorr_n;
   float inv_Wdq;
   float scorr_u;        // 1 / (h^2 - dq^2): W(r)/W(dq) = ((h^2 - r^2) scorr_u)^3
+  float scorr_u_fx;     // scorr_u 2^-2k (for r^2 in fixed-point units squared)
+  float scorr_uh2;      // scorr_u h^2
   float c_xsph;
   int xsph_exact;       // 0: reference r expression (particles.c:439)
   float gamma, C_norm;  // surface tension
