@@ -384,10 +384,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksColor)
     const float fx = (float)(int)(rp.x - rq.x);
     const float fy = (float)(int)(rp.y - rq.y);
     const float fz = (float)(int)(rp.z - rq.z);
-    const float r2 = (fx * fx + fy * fy + fz * fz) * P.fx_inv2;
-    float r, rinv;
-    floored_r(P, r2, r, rinv);
-    const float t = fmaxf(P.h2 - r * r, 0.0f);
+    // r and 1/r in fixed-point units (their product is unit-free)
+    float r2c, r, rinv;
+    floored_r_fx(P, fx * fx + fy * fy + fz * fz, r2c, r, rinv);
+    const float t = fmaxf(fmaf(-P.fx_inv2, r2c, P.h2), 0.0f);
     const float c = t * t * r * (rinv * __frcp_rn(nr_w(rq)));
     cx = fmaf(c, fx, cx);
     cy = fmaf(c, fy, cy);
@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksVorticity)
   const uint4 rp = ld_nr(a.nr, p);
   const float4 vp = __ldg(a.vel + p);
   // sums of (v_q - v_p) x c d with c = (h - r)^2 / r and d in fixed-point
-  // units; the spiky norm and 2^-k multiply them once (the padding slots'
+  // units (r too); the spiky norm and 2^-2k multiply them once (the padding slots'
   // v_q - v_p and d are 0)
   float wx = 0.f, wy = 0.f, wz = 0.f;
   for_each_neighbor_nr2<kNbrBatch, true>(V, a.nr, a.vel, p,
@@ -499,10 +499,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksVorticity)
     const float dx = (float)(int)(rp.x - rq.x);
     const float dy = (float)(int)(rp.y - rq.y);
     const float dz = (float)(int)(rp.z - rq.z);
-    const float r2 = (dx * dx + dy * dy + dz * dz) * P.fx_inv2;
-    float r, rinv;
-    floored_r(P, r2, r, rinv);
-    const float hm = fmaxf(P.h - r, 0.0f);
+    float r2c, r, rinv;
+    floored_r_fx(P, dx * dx + dy * dy + dz * dz, r2c, r, rinv);
+    const float hm = fmaxf(P.h_fx - r, 0.0f);
     const float c = hm * hm * rinv;
     const float gx = c * dx, gy = c * dy, gz = c * dz;
     const float ux = vq.x - vp.x, uy = vq.y - vp.y, uz = vq.z - vp.z;
@@ -510,7 +509,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksVorticity)
     wy += uz * gx - ux * gz;
     wz += ux * gy - uy * gx;
   });
-  const float sw = P.DWn * P.fx_inv;
+  const float sw = P.DWn * P.fx_inv2;
   wx *= sw;
   wy *= sw;
   wz *= sw;
@@ -527,24 +526,23 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksConfinement)
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   const uint4 rp = ld_nr(a.nr, p);
-  // sums of |omega_q| (h - r)^2 / r d, d in fixed-point units; the spiky
-  // norm and 2^-k multiply them once (the padding slots' d is 0)
+  // sums of |omega_q| (h - r)^2 / r d, d and r in fixed-point units; the
+  // spiky norm and 2^-2k multiply them once (the padding slots' d is 0)
   float ex = 0.f, ey = 0.f, ez = 0.f;
   for_each_neighbor_nr<kNbrBatch, true>(V, a.nr, p, [&](int q, const uint4 rq) {
     const float dx = (float)(int)(rp.x - rq.x);
     const float dy = (float)(int)(rp.y - rq.y);
     const float dz = (float)(int)(rp.z - rq.z);
-    const float r2 = (dx * dx + dy * dy + dz * dz) * P.fx_inv2;
-    float r, rinv;
-    floored_r(P, r2, r, rinv);
-    const float hm = fmaxf(P.h - r, 0.0f);
+    float r2c, r, rinv;
+    floored_r_fx(P, dx * dx + dy * dy + dz * dz, r2c, r, rinv);
+    const float hm = fmaxf(P.h_fx - r, 0.0f);
     const float wq = OW ? nr_w(rq) : __ldg(a.omega + q).w;
     const float c = hm * hm * rinv * wq;
     ex = fmaf(c, dx, ex);
     ey = fmaf(c, dy, ey);
     ez = fmaf(c, dz, ez);
   });
-  const float se = P.DWn * P.fx_inv;
+  const float se = P.DWn * P.fx_inv2;
   ex *= se;
   ey *= se;
   ez *= se;
