@@ -150,6 +150,15 @@ int sphpc_get_neighbor_buckets(const struct Particles *particles, unsigned int *
 int sphpc_get_cell_data(const struct Particles *particles, unsigned int *hash_values,
                         unsigned int *particle_ids, unsigned int *start_indices);
 
+/* No counterpart in the reference (whose FillNeighbors tests every pair in
+ * FP64, neighbors.c:278-285).  1 if the neighbour build's FP32 candidate
+ * pre-test decides r^2 < h^2 exactly as that FP64 test does for
+ * coordinates of magnitude up to max_coord (it leaves pairs within
+ * +-2^-10 h^2 of h^2 to the FP64 test); 0 otherwise, in which case the
+ * build sends every candidate to the FP64 test.  The build applies it with
+ * max_coord = h * max(hash_size_x, hash_size_y, hash_size_z). */
+int sphpc_neighbor_pretest_fp32_safe(double max_coord, double h);
+
 /* ---------------- obstacle (obstacle.h:32-33) ---------------- */
 
 /* Reads the SDFGen ASCII file named in obstacle->SDF_file_name

@@ -166,6 +166,7 @@ SIGNATURES = {
     "AllocInitObstacle": ([PO], C.c_int),
     "FinalizeObstacle": ([PO], C.c_int),
     "sphpc_read_sdf": ([PO], C.c_int),
+    "sphpc_neighbor_pretest_fp32_safe": ([C.c_double, C.c_double], C.c_int),
     "sphpc_step": ([PP, P, PN, PA, PO, C.c_int], C.c_int),
     "AllocInitFileIO": ([C.POINTER(FileIO), PP, P], C.c_int),
     "WriteParticles": ([PP, P, C.POINTER(FileIO)], C.c_int),

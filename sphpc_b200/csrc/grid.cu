@@ -215,8 +215,10 @@ struct BuildCtx {
 
 // r^2 < h^2 exactly as neighbors.c:278-285 evaluates it on the canonical
 // double positions.  The FP32 absolute positions decide every pair whose r^2
-// lies outside a band of +-2^-10 h^2 (FP32 rounding of coordinates up to
-// 2^15 h moves r^2 by far less); the FP64 test decides the rest.
+// lies outside the band [P.bld_h2lo, P.bld_h2hi] = h^2 (1 -+ 2^-10); the FP64
+// test decides the rest.  The host opens the band to every pair when FP32
+// rounding of the grid's largest coordinate could move r^2 by that much
+// (sphpc_neighbor_pretest_fp32_safe: beyond about 2^12 h).
 __device__ __noinline__ bool exact_neighbor(const BuildCtx& c, const PD* __restrict__ pd,
                                             int j) {
   float4 xq, dq;
@@ -256,8 +258,8 @@ __global__ void __launch_bounds__(kBuildBlock, 10)
   c.xs = xstar_d(c.xp.x, c.dp.x);
   c.ys = xstar_d(c.xp.y, c.dp.y);
   c.zs = xstar_d(c.xp.z, c.dp.z);
-  c.h2lo = P.h2 * (1.0f - 1.0f / 1024.0f);
-  c.h2hi = P.h2 * (1.0f + 1.0f / 1024.0f);
+  c.h2lo = P.bld_h2lo;
+  c.h2hi = P.bld_h2hi;
   c.h2d = P.h2d;
   int cx, cy, cz;
   unpack_cell(V, __ldg(cellp + p), cx, cy, cz);

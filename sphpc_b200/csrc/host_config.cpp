@@ -217,6 +217,27 @@ void sphpc_default_solver(struct SphpcSolver* s) {
   s->warm_start_min_error = 0.0;
 }
 
+// The neighbour build decides r^2 < h^2 from FP32 copies of the absolute
+// predicted positions, and leaves to the exact FP64 test of FillNeighbors
+// (neighbors.c:278-285) only the pairs whose FP32 r^2 lies within
+// +-2^-10 h^2 of h^2.  That is correct while the FP32 error of r^2 stays
+// below the band.  A coordinate of magnitude up to max_coord is rounded to
+// FP32 within u/2, u = 2^(floor(log2 max_coord) - 23); a pair difference
+// (< 2h per axis between adjacent cells) is then off by at most
+// e = u + 2^-24 (2h + u), and r^2 near h^2 by at most
+// e (2 sqrt(3) h + 3e) plus the FP32 rounding of the sum of squares,
+// 3 * 2^-24 h^2.  Safe when that total, with a 10% margin, is below
+// 2^-10 h^2 (for h = 2: coordinates up to 2^13).
+int sphpc_neighbor_pretest_fp32_safe(double max_coord, double h) {
+  if (!(h > 0.0) || !(max_coord >= 0.0) || !std::isfinite(max_coord)) return 0;
+  const double m = max_coord > h ? max_coord : h;
+  const double u = std::ldexp(1.0, (int)std::floor(std::log2(m)) - 23);
+  const double e = u + std::ldexp(2.0 * h + u, -24);
+  const double err = e * (2.0 * std::sqrt(3.0) * h * 1.001 + 3.0 * e) +
+                     3.0 * std::ldexp(1.0, -24) * 1.002 * h * h;
+  return err < 0.9 * std::ldexp(h * h, -10) ? 1 : 0;
+}
+
 void sphpc_set_default_solver(const struct SphpcSolver* s) {
   if (s) set_current_solver(*s);
 }

@@ -4,6 +4,7 @@
 // keeps the same arrays resident with OpenACC `enter data`,
 // particles.c:1056-1078).  Its kernels run on one stream; the reference-named
 // step functions launch one stage each, sphpc_step launches the fused step.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -391,6 +392,17 @@ DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob
     P.rmin2_fx = (float)ldexp(h * 0.0001 * h * 0.0001, 2 * k);
   }
   P.h2d = h * h;
+  {
+    // coordinates that hash inside the grid lie below max(nx, ny, nz) h
+    const int nmax = std::max(nx, std::max(ny, nz));
+    if (sphpc_neighbor_pretest_fp32_safe((double)nmax * h, h)) {
+      P.bld_h2lo = (float)(h * h) * (1.0f - 1.0f / 1024.0f);
+      P.bld_h2hi = (float)(h * h) * (1.0f + 1.0f / 1024.0f);
+    } else {
+      P.bld_h2lo = -1.0f;
+      P.bld_h2hi = INFINITY;
+    }
+  }
   P.h = (float)h;
   P.h2 = (float)(h * h);
   P.rmin = (float)(h * 0.0001);

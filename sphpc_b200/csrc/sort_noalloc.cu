@@ -37,11 +37,52 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-uint32_t* g_scratch_ptr[kMaxDevices] = {};
+
+// The looked-up address of each device, with the unique id of the context it
+// belongs to: a cudaDeviceReset ends the device's primary context, the next
+// runtime call makes a new one and loads the module again, and the array may
+// then sit at another address.
+struct ScratchSlot {
+  uint32_t* ptr = nullptr;
+  unsigned long long ctx_id = 0;
+  bool ctx_known = false;
+};
+ScratchSlot g_scratch[kMaxDevices];
+
+// cuCtxGetCurrent / cuCtxGetId from the driver, fetched through the runtime
+// (the library links only the static runtime).
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+bool g_ctx_fns_tried = false;
+
+// Unique id of the current context; false when the driver cannot say (then
+// the address is looked up again on every call).
+bool current_ctx_id(unsigned long long* id) {
+  if (!g_ctx_fns_tried) {
+    g_ctx_fns_tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+  }
+  if (!g_ctx_get_current || !g_ctx_get_id) return false;
+  void* ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != 0 || !ctx) return false;
+  return g_ctx_get_id(ctx, id) == 0;
+}
 
 // Device address of g_noalloc_scratch on the current device.  In host code
 // the array's name is only a host-side stand-in, so the address comes from
-// cudaGetSymbolAddress, once per device, with that device current.
+// cudaGetSymbolAddress, with the device current: once per device, and again
+// whenever the device's context has changed since (after a cudaDeviceReset).
 int scratch_address(uint32_t** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -49,15 +90,23 @@ int scratch_address(uint32_t** out) {
   if (dev < 0 || dev >= kMaxDevices)
     return set_error(SPHPC_EINVAL, "SortByKeyNoAlloc: device %d out of range", dev);
   std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_ptr[dev]) {
+  ScratchSlot& slot = g_scratch[dev];
+  // no current context yet (before the first runtime call on this thread,
+  // or right after a reset) counts as unknown: cudaGetSymbolAddress below
+  // makes the primary context current, and the next call records its id
+  unsigned long long id = 0;
+  const bool known = current_ctx_id(&id);
+  if (!slot.ptr || !known || !slot.ctx_known || slot.ctx_id != id) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return set_error(SPHPC_ECUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s",
                        cudaGetErrorString(e));
-    g_scratch_ptr[dev] = static_cast<uint32_t*>(p);
+    slot.ptr = static_cast<uint32_t*>(p);
+    slot.ctx_id = id;
+    slot.ctx_known = known;
   }
-  *out = g_scratch_ptr[dev];
+  *out = slot.ptr;
   return SPHPC_OK;
 }
 

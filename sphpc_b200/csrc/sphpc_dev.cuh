@@ -89,6 +89,9 @@ struct DevParams {
   float h_fx;           // h in fixed-point units (h 2^k)
   float rmin2_fx;       // (1e-4 h)^2 in fixed-point units squared
   double h2d;
+  // neighbour-build FP32 pre-test band: pairs with FP32 r^2 in [lo, hi] go
+  // to the exact FP64 test (lo = -1, hi = inf: every pair does)
+  float bld_h2lo, bld_h2hi;
   float h, h2;
   float rmin;           // r floor 1e-4 h (particles.c:636)
   // smoothing-kernel constants; *_m variants carry the particle mass

@@ -41,8 +41,10 @@ def test_no_alloc_sort_matches_sort_by_key_twice():
         torch.cuda.synchronize()
         assert torch.equal(ka, kb)
         assert torch.equal(va, vb)
+        # pinned by an independent stable sort as well, not only by SortByKey
         order = np.argsort(keys, kind="stable")
         np.testing.assert_array_equal(kb.cpu().numpy().view(np.uint32), keys[order])
+        np.testing.assert_array_equal(vb.cpu().numpy().view(np.uint32), vals[order])
 
 
 def test_no_alloc_sort_rejects_counts_above_its_limit():
