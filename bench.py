@@ -273,33 +273,52 @@ def run_ours(args, world, rank, local, dist):
                  "max_iterations": args.max_iters, "min_progress": args.min_progress}
     if args.fixed:
         overrides = {"adaptive": 0}
+    if args.stiffness_k is not None:
+        overrides["stiffness_k"] = args.stiffness_k
+    arms = [a.strip() for a in args.arms.split(",") if a.strip()]
     net = None
     if not args.no_warm and os.path.exists(args.weights):
         net = ws.load_network(args.weights)
     stream = torch.cuda.current_stream(dev)
 
-    def make_sim(warm):
+    def make_sim(kind):
+        """kind: "plain", "warm" (the network's multipliers) or "carry" (the
+        previous step's applied multipliers, no network: the control arm)."""
         t_init = time.perf_counter()
         sim = Simulation(args.config, solver_overrides=overrides)
         sim.set_stream(stream.cuda_stream)
-        if warm:
+        if kind == "warm":
             sim.mlp_load(net[0], net[1])
-            sim.set_solver(warm_start=1,
+            sim.set_solver(warm_start=1, warm_start_source=0,
                            warm_start_scale=float(net[2].get("warm_start_scale", 1.0)),
                            warm_start_min_error=float(net[2].get("warm_start_min_error", 0.0)))
-        log(f"[rank {rank}] {args.config}: {sim.n} particles, warm start {warm}, "
+        elif kind == "carry":
+            sim.set_solver(warm_start=1, warm_start_source=1, warm_start_min_error=0.0)
+        elif kind == "fixed":
+            # the reference arm's own iteration count, fixed: the like-for-like
+            # comparison with its CPU path
+            sim.set_solver(adaptive=0, solve_iterations=args.ref_iterations)
+        log(f"[rank {rank}] {args.config}: {sim.n} particles, arm {kind}, "
             f"init {time.perf_counter()-t_init:.1f}s")
         return sim
 
-    # plain solver first, then (with a trained network) the warm-started one
-    sim = make_sim(False)
-    n = sim.n
-    plain = timed_arm(sim, args, stream, dist, local, dev)
-    warm = None
-    if net is not None:
-        sim.close()
-        sim = make_sim(True)
-        warm = timed_arm(sim, args, stream, dist, local, dev)
+    # plain solver first, then the network-started one (with a trained
+    # network) and the carried-multiplier control, each from the same state
+    results = {}
+    sim = None
+    n = None
+    for kind in ["plain"] + [k for k in arms if k != "plain"]:
+        if kind == "warm" and net is None:
+            continue
+        if sim is not None:
+            sim.close()
+        sim = make_sim(kind)
+        n = sim.n
+        results[kind] = timed_arm(sim, args, stream, dist, local, dev)
+    plain = results["plain"]
+    warm = results.get("warm")
+    carry = results.get("carry")
+    fixed = results.get("fixed")
     head = warm if warm is not None else plain
     ms_max = head["ms"]
     value = job_rate(world, n, args.steps, ms_max / 1e3)
@@ -337,7 +356,7 @@ def run_ours(args, world, rank, local, dist):
     e2e = None
     if not args.no_e2e:
         sim.close()
-        sim = make_sim(net is not None)
+        sim = make_sim("warm" if warm is not None else "plain")
         for _ in range(args.warmup):
             sim.step(1)
         e2e = run_e2e(sim, args, dist, world, n)
@@ -356,6 +375,15 @@ def run_ours(args, world, rank, local, dist):
     if rank != 0:
         return
     clocks = head["clocks"]
+    like = None
+    if fixed is not None:
+        fv = job_rate(world, n, args.steps, fixed["ms"] / 1e3)
+        like = {"iterations": args.ref_iterations, "gpu_value": fv,
+                "gpu_ms_per_step": fixed["ms"] / args.steps,
+                "reference_value": cpu["value"] if cpu else None,
+                "ratio": (fv / cpu["value"]) if cpu and cpu.get("value") else None,
+                "note": "both at the reference arm's fixed iteration count; the reference "
+                        "runs a 32x32x32 block of the scene on one core"}
 
     def arm_summary(a):
         if a is None:
@@ -364,6 +392,7 @@ def run_ours(args, world, rank, local, dist):
                 "ms_per_step": a["ms"] / args.steps,
                 "mean_iterations": float(np.mean(a["iters"])) if a["iters"] else None,
                 "steps_converged": a["converged"] if a["iters"] else None,
+                "steps_unconverged": (len(a["iters"]) - a["converged"]) if a["iters"] else None,
                 "warm_start_steps": a["warm_used"], "gate_rejections": a["rejected"],
                 "final_max_density_error": a["diag"]["max_density_error"],
                 "gpu_launches": a["launches"]}
@@ -383,9 +412,13 @@ def run_ours(args, world, rank, local, dist):
                       if warm is not None else ", plain (no network file)"),
                    "plain": arm_summary(plain),
                    "warm_start": arm_summary(warm),
+                   "carried_multiplier_start": arm_summary(carry),
                    "warm_start_weights": (os.path.relpath(args.weights, ROOT)
                                           if warm is not None else None),
                    "speedup_vs_plain": (plain["ms"] / warm["ms"]) if warm is not None else None,
+                   "speedup_carried_vs_plain": (plain["ms"] / carry["ms"])
+                   if carry is not None else None,
+                   "stiffness_k": args.stiffness_k,
                    "mean_iterations": float(np.mean(iters)) if iters else None,
                    "steps_converged": conv if iters else None,
                    "l2": "state larger than L2 (no flush)",
@@ -395,6 +428,7 @@ def run_ours(args, world, rank, local, dist):
         "clocks": clocks,
         "roofline": roof,
         "stage_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()},
+        "like_for_like": like,
         "e2e": e2e,
         "cpu_baseline": cpu,
     }
@@ -482,6 +516,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-warm", action="store_true", help="plain solver only")
+    ap.add_argument("--arms", default="plain,warm,carry,fixed",
+                    help="solver arms, each from the same initial state: plain, warm (the "
+                         "network's multipliers), carry (the previous step's applied "
+                         "multipliers carried through the sort, no network), fixed (the "
+                         "reference arm's fixed iteration count, --ref-iterations)")
+    ap.add_argument("--stiffness-k", type=float, default=None,
+                    help="UpdateDPs stiffness constant k of s_n = 1 - (1 - k)^(1/n) "
+                         "(the reference's 0.95 by default; 1 gives a constant 1)")
     ap.add_argument("--weights", default=os.path.join(ROOT, "sphpc_b200", "weights",
                                                       "warm_start.npz"))
     ap.add_argument("--ref-iterations", type=int, default=6)

@@ -159,6 +159,55 @@ int sphpc_get_cell_data(const struct Particles *particles, unsigned int *hash_va
  * max_coord = h * max(hash_size_x, hash_size_y, hash_size_z). */
 int sphpc_neighbor_pretest_fp32_safe(double max_coord, double h);
 
+/* ---------------- slab decomposition along x (communication.c) ---------------- */
+
+/* The reference splits the domain into x-slabs, one per MPI rank: it trades
+ * particles that left a slab (ExchangeOOB, communication.c:453-585), copies
+ * a halo of width h (ExchangeHalo, :222-321) and refreshes the halo's
+ * scalars and tuples after every pass (UpdateHaloScalar / UpdateHaloTuple,
+ * :587-753).  Here one exchange per step does all of it: each rank's
+ * working set is its own particles plus copies of its neighbours' particles
+ * within a halo width (sphpc_slab_halo_width) that covers every neighbour
+ * hop of a step, so its own particles' results are those of the undivided
+ * domain (bit for bit: the set is kept in global-id order, so buckets list
+ * each cell's particles in the same order).  Records (32 bytes each:
+ * {x, y, z, gid}, {vx, vy, vz, flags}) are device memory the caller moves
+ * between ranks (NCCL send/recv, or a peer copy).  A slab steps with the
+ * fixed iteration count (adaptive and warm_start off). */
+
+/* Makes the device copy a slab [node_start_x, node_end_x) of a decomposed
+ * domain (has_left / has_right: whether neighbours exist; a side without
+ * one owns everything beyond it): global ids first_gid + host index, and
+ * the particles inside owned.  Every rank may start from the whole scene;
+ * the particles it does not own leave at the first sphpc_slab_pack. */
+int sphpc_slab_init(struct Particles *particles, unsigned int first_gid, double node_start_x,
+                    double node_end_x, int has_left, int has_right);
+/* Halo width one exchange per step needs for these solver settings. */
+int sphpc_slab_halo_width(const struct Params *params, const struct SphpcSolver *solver,
+                          double *width);
+/* Sorts the owned particles by their position at the start of the next
+ * step against [node_start_x, node_end_x): records for the left and right
+ * neighbours (has_left / has_right: whether they exist) into send_left /
+ * send_right (device memory, send_capacity records each), the rest kept.
+ * Returns the record counts. */
+int sphpc_slab_pack(struct Particles *particles, double node_start_x, double node_end_x,
+                    double halo_width, int has_left, int has_right, void *send_left,
+                    void *send_right, int send_capacity, int *count_left, int *count_right);
+/* Rebuilds the working set from the kept records and the neighbours'
+ * (device memory) in global-id order; sets local_count. */
+int sphpc_slab_unpack(struct Particles *particles, const void *recv_left, int count_left,
+                      const void *recv_right, int count_right);
+/* The owned particles' global ids, positions and velocities (host arrays,
+ * in no particular order); *count of them. */
+int sphpc_slab_owned(const struct Particles *particles, unsigned int *gids, double *xyz,
+                     double *vel, int capacity, int *count);
+/* BalanceNodes (geometry.c:102-166) given the neighbours' particle counts
+ * and slab lengths: moves params->node_start_x / node_end_x by h towards an
+ * even share of global_count. */
+int sphpc_balance_nodes(int rank, int proc_count, int num_rank, int num_right,
+                        double length_left, double length_right, int global_count,
+                        struct Params *params);
+
 /* ---------------- obstacle (obstacle.h:32-33) ---------------- */
 
 /* Reads the SDFGen ASCII file named in obstacle->SDF_file_name

@@ -48,6 +48,19 @@ int FindUpperBounds(const unsigned int *const hash_values, const int value_count
                     const int search_count, unsigned int *const end_indices,
                     const void *const cuda_stream);
 
+/* No counterpart in the reference (its Thrust seam has no waits,
+ * thrust_c.cu:86-91).  Failure-detection checks of the library's bounded
+ * device waits: each runs one block that waits, with the given poll limit,
+ * on a flag nothing ever sets -- a radix-sort look-back flag of an earlier
+ * tile (SortByKey's onesweep passes wait up to 2^22 polls), or a
+ * tensor-core completion mbarrier (the warm-start network's kernels wait up
+ * to 2^20 polls).  The wait gives up, the kernel records an error bit and
+ * returns, and the call returns SPHPC_EKERNEL with *error_bits set (2 for
+ * the sort, 16 for the mbarrier); SPHPC_OK would mean the wait ended by
+ * itself.  The device stays usable afterwards. */
+int sphpc_check_sort_wait(int spin_limit, unsigned int *error_bits);
+int sphpc_check_mbarrier_wait(int poll_limit, unsigned int *error_bits);
+
 /* obstacle_cuda.h:23-27 (obstacle_cuda.cu:118-131): pushes every particle
  * whose double position lies inside the obstacle out along the SDF normal.
  * The obstacle must have been uploaded (AllocInitObstacle / _CUDA).  Runs on

@@ -166,7 +166,10 @@ struct SphpcSolver {
                                     i.e. the effective value is eps/rho0^2 */
   int warm_start_gate;        /* 1: discard a warm pass that does not lower the
                                  FP64 max density error (default) */
-  int pad_warm;
+  int warm_start_source;      /* 0: the MLP's multipliers (default); 1: the
+                                 previous step's applied multipliers
+                                 sum_k s_k lambda_k, carried through the
+                                 sort permutation (no network) */
   double warm_start_scale;    /* multiplier on the network's Lambda (1) */
   double min_progress;        /* adaptive: also stop (not converged) when two
                                  iterations together lower the FP64 max density

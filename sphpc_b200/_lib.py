@@ -76,7 +76,7 @@ class Solver(C.Structure):
                 ("rest_density_lattice", C.c_int), ("adaptive", C.c_int),
                 ("density_tolerance", C.c_double), ("max_iterations", C.c_int),
                 ("warm_start", C.c_int), ("lambda_epsilon_mass_units", C.c_int),
-                ("warm_start_gate", C.c_int), ("pad_warm", C.c_int),
+                ("warm_start_gate", C.c_int), ("warm_start_source", C.c_int),
                 ("warm_start_scale", C.c_double), ("min_progress", C.c_double),
                 ("warm_start_min_error", C.c_double)]
 
@@ -203,6 +203,17 @@ SIGNATURES = {
                          C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
     "SortByKey": ([U, U, C.c_int, C.c_void_p], C.c_int),
     "SortByKeyNoAlloc": ([U, U, C.c_int, C.c_void_p], C.c_int),
+    "sphpc_check_sort_wait": ([C.c_int, U], C.c_int),
+    "sphpc_slab_init": ([PP, C.c_uint, C.c_double, C.c_double, C.c_int, C.c_int], C.c_int),
+    "sphpc_slab_halo_width": ([P, C.POINTER(Solver), C.POINTER(C.c_double)], C.c_int),
+    "sphpc_slab_pack": ([PP, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p,
+                         C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "sphpc_slab_unpack": ([PP, C.c_void_p, C.c_int, C.c_void_p, C.c_int], C.c_int),
+    "sphpc_slab_owned": ([PP, U, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int,
+                          C.POINTER(C.c_int)], C.c_int),
+    "sphpc_balance_nodes": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                             C.c_int, P], C.c_int),
+    "sphpc_check_mbarrier_wait": ([C.c_int, U], C.c_int),
     "FindLowerBounds": ([U, C.c_int, C.c_int, U, C.c_void_p], C.c_int),
     "FindUpperBounds": ([U, C.c_int, C.c_int, U, C.c_void_p], C.c_int),
     "CalculateParticleCollisions": ([_DP, _DP, _DP, C.c_int, Obstacle], C.c_int),

@@ -211,7 +211,7 @@ void sphpc_default_solver(struct SphpcSolver* s) {
   s->warm_start = 0;
   s->lambda_epsilon_mass_units = 0;
   s->warm_start_gate = 1;
-  s->pad_warm = 0;
+  s->warm_start_source = 0;
   s->warm_start_scale = 1.0;
   s->min_progress = 0.0;
   s->warm_start_min_error = 0.0;

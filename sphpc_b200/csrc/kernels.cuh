@@ -35,6 +35,9 @@ struct ReorderExtra {
   float4* out4[6];
   const float* in1[4];
   float* out1[4];
+  // carried warm start: records {x*, carry_src[old slot]} into nr_carry
+  const float* carry_src;
+  uint4* nr_carry;
 };
 void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
                     const PD* pd_in, const float4* vel_in, PD* pd_out, float4* vel_out,
@@ -75,6 +78,9 @@ struct PassArgs {
   float stiffness;     // UpdateDPs stiffness for this substep
   int last;            // fused position pass: also UpdateVelocities
   int write_pos;       // post pass: also UpdatePositions
+  float* lam_acc;      // position pass: multiplier applied so far this step,
+                       // sum of stiffness * lambda_p (null: not kept)
+  int acc_add;         // 1: add to lam_acc, 0: start it with this pass
 };
 
 // Density (+lambda) pass: ComputeDensities (particles.c:461-514) and
@@ -127,5 +133,45 @@ void launch_make_nr(const DevParams& P, const PD* pd, const float* src, uint4* n
 // CalculateParticleCollisions seam on device double arrays.
 void launch_collisions_double(const DevParams& P, double* x, double* y, double* z, int n,
                               cudaStream_t st);
+
+// ---- slab decomposition along x (slab.cu) ----
+
+// One particle between ranks: {x, y, z, gid bits}, {vx, vy, vz, flags bits}
+// (flags bit 0: owned by the receiver).
+struct __align__(32) SlabRecord {
+  float4 a, b;
+};
+// Three record arrays read as one concatenation (kept, from the left, from
+// the right).
+struct SlabParts {
+  const SlabRecord* p0;
+  const SlabRecord* p1;
+  const SlabRecord* p2;
+  uint32_t n0, n1, n2;
+};
+// gid[i] = first + i for host index i; owned[i] when the particle's
+// position lies in [lo, hi) (a side without a neighbour owns everything
+// beyond it).
+void launch_slab_init(int n, const uint32_t* ids, const PD* pd, uint32_t first_gid, double lo,
+                      double hi, bool has_left, bool has_right, uint32_t* gid, uint8_t* owned,
+                      cudaStream_t st);
+// Sorts the owned particles of the working set (slot order, host index
+// ids[j]) into kept / to-the-left / to-the-right records by their
+// step-start position (counters[0..2], capacities cap_keep / cap_send:
+// records past a capacity are counted, not written).
+void launch_slab_pack(int n, const uint32_t* ids, const uint32_t* gid, const uint8_t* owned,
+                      const PD* pd, const float4* vel, double lo, double hi, double R,
+                      bool has_left, bool has_right, SlabRecord* keep, SlabRecord* send_l,
+                      SlabRecord* send_r, uint32_t* counters, uint32_t cap_keep,
+                      uint32_t cap_send, cudaStream_t st);
+// keys[k] = gid of record k of the concatenation.
+void launch_slab_keys(const SlabParts& s, uint32_t* keys, cudaStream_t st);
+// Slot k (and host index k) of the new working set <- record perm[k].
+void launch_slab_load(const SlabParts& s, const uint32_t* perm, PD* pd, float4* vel,
+                      uint32_t* gid, uint8_t* owned, uint32_t* ids, cudaStream_t st);
+// Records of the owned particles (unordered; *counter of them).
+void launch_slab_owned(int n, const uint32_t* ids, const uint32_t* gid, const uint8_t* owned,
+                       const PD* pd, const float4* vel, SlabRecord* out, uint32_t* counter,
+                       uint32_t cap, cudaStream_t st);
 
 }  // namespace sphpc

@@ -61,10 +61,13 @@ __device__ __forceinline__ void commit(uint64_t* mbar) {
                : "memory");
 }
 
-// Bounded wait for the mbarrier phase; false after ~1e6 polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+// Bounded wait for the mbarrier phase; false after `limit` polls (~1e6 by
+// default).
+constexpr int kMbarPollLimit = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity,
+                                          int limit = kMbarPollLimit) {
   const uint32_t addr = smem_u32(mbar);
-  for (int i = 0; i < (1 << 20); ++i) {
+  for (int i = 0; i < limit; ++i) {
     uint32_t ok;
     asm volatile(
         "{\n.reg .pred P1;\nmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n"
@@ -873,6 +876,42 @@ int mlp_dataset_claim(long long want, float** feat, float** target, long long* g
   *target = g_ds.target + g_ds.n;
   g_ds.n += *got;
   return SPHPC_OK;
+}
+
+namespace {
+
+// Failure-detection check of the bounded mbarrier wait of the tensor-core
+// kernels: an mbarrier that nothing ever arrives on, waited on through the
+// same helper with a poll limit of `limit`.  The block decides together, as
+// the kernels do, and records kErrMlpWait when the wait gave up.
+__global__ void k_mbar_wait_probe(int limit, uint32_t* err) {
+  __shared__ __align__(8) uint64_t mbar;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  __syncthreads();
+  const bool done = __syncthreads_and(tc::mbar_wait(&mbar, 0, limit) ? 1 : 0) != 0;
+  if (!done && threadIdx.x == 0) atomicOr(err, kErrMlpWait);
+  __syncthreads();
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(tc::smem_u32(&mbar)));
+}
+
+}  // namespace
+
+cudaError_t mbar_wait_probe(int limit, uint32_t* err_bits) {
+  uint32_t* err = nullptr;
+  cudaError_t e = cudaMalloc(&err, sizeof(uint32_t));
+  if (e != cudaSuccess) return e;
+  e = cudaMemset(err, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) {
+    k_mbar_wait_probe<<<1, 128>>>(limit, err);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(err_bits, err, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  cudaFree(err);
+  return e;
 }
 
 }  // namespace sphpc

@@ -74,4 +74,9 @@ void launch_mlp_forward_bf16(const MlpDevice& d, const __nv_bfloat16* xbf, int n
 // nearly full: *got) and returns their feature and target pointers.
 int mlp_dataset_claim(long long want, float** feat, float** target, long long* got);
 
+// Failure-detection check of the bounded mbarrier wait: one block waits,
+// with a poll limit of `limit`, on an mbarrier that nothing arrives on;
+// returns the error bits it raised (kErrMlpWait, 1 << 4, when it gave up).
+cudaError_t mbar_wait_probe(int limit, uint32_t* err_bits);
+
 }  // namespace sphpc

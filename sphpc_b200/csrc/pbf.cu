@@ -340,6 +340,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksPosition)
   st_pd(a.pd_out, p, xp, dn);
   // the record carries the canonical x* = x + d of what was just stored
   a.nr_out[p] = make_nr(P, xstar_d(xp.x, dn.x), xstar_d(xp.y, dn.y), xstar_d(xp.z, dn.z), rho_p);
+  if (a.lam_acc) a.lam_acc[p] = fmaf(a.stiffness, lp, a.acc_add ? a.lam_acc[p] : 0.0f);
   if (a.last) {
     // UpdateVelocities, particles.c:814-837
     float vx = __double2float_rn(__ddiv_rn(ex, P.dt_d));

@@ -1,6 +1,8 @@
 // radix_sort.cu -- onesweep LSD radix sort and the cell-bounds seam kernels.
 #include "radix_sort.cuh"
 
+#include <vector>
+
 namespace sphpc {
 
 namespace {
@@ -62,7 +64,7 @@ __global__ void __launch_bounds__(kSortThreads)
                uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n,
                int shift, const uint32_t* __restrict__ digit_offset,
                uint32_t* __restrict__ lookback, uint32_t* __restrict__ tile_counter,
-               uint32_t* __restrict__ err) {
+               uint32_t* __restrict__ err, int spin_limit) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_whist[kSortWarps][kRadix + 1];
   __shared__ uint32_t s_dstart[kRadix];
@@ -135,7 +137,7 @@ __global__ void __launch_bounds__(kSortThreads)
         uint32_t v = ld_volatile(f);
         int spins = 0;
         while ((v & (kLbAgg | kLbInc)) == 0) {
-          if (++spins > kSpinLimit) {
+          if (++spins > spin_limit) {
             atomicOr(err, 2u);  // kErrSortSpin
             v = kLbInc;
             break;
@@ -256,7 +258,7 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, int n, int passes,
     uint32_t* vout = bv[p & 1];
     k_onesweep<<<tiles, kSortThreads, 0, stream>>>(
         kin, vin, kout, vout, n, p * kRadixBits, s.hist + p * kRadix,
-        s.lookback + (size_t)p * tiles * kRadix, s.counters + p, s.err);
+        s.lookback + (size_t)p * tiles * kRadix, s.counters + p, s.err, kSpinLimit);
     kin = kout;
     vin = vout;
   }
@@ -275,6 +277,54 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, int n, int passes,
   if (keys_res) *keys_res = kres;
   if (vals_res) *vals_res = vres;
   return cudaSuccess;
+}
+
+cudaError_t lookback_wait_probe(int spin_limit, uint32_t* err_bits) {
+  // Two tiles of keys; the tile counter starts at 1, so the one CTA
+  // launched ranks tile 1 and looks back at tile 0, whose flag no CTA ever
+  // writes.  Its wait gives up after spin_limit polls and sets kErrSortSpin;
+  // the digit offsets are those of all 2 tiles, so every scatter the CTA
+  // then makes stays below n.
+  const int n = 2 * kSortTile;
+  std::vector<uint32_t> hk(n);
+  uint32_t hist[kRadix] = {};
+  for (int i = 0; i < n; ++i) {
+    hk[i] = (uint32_t)i * 2654435761u;
+    ++hist[hk[i] & (kRadix - 1)];
+  }
+  uint32_t offs[kRadix];
+  uint32_t acc = 0;
+  for (int d = 0; d < kRadix; ++d) {
+    offs[d] = acc;
+    acc += hist[d];
+  }
+  uint32_t* buf = nullptr;
+  const size_t words = 4 * (size_t)n + kRadix + 2 * kRadix + 2;
+  cudaError_t e = cudaMalloc(&buf, words * sizeof(uint32_t));
+  if (e != cudaSuccess) return e;
+  uint32_t* keys = buf;
+  uint32_t* vals = buf + n;
+  uint32_t* kout = buf + 2 * (size_t)n;
+  uint32_t* vout = buf + 3 * (size_t)n;
+  uint32_t* doff = buf + 4 * (size_t)n;
+  uint32_t* lookback = doff + kRadix;
+  uint32_t* counter = lookback + 2 * kRadix;
+  uint32_t* err = counter + 1;
+  const uint32_t one = 1u;
+  e = cudaMemset(buf, 0, words * sizeof(uint32_t));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(keys, hk.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(doff, offs, sizeof(offs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(counter, &one, sizeof(one), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_onesweep<<<1, kSortThreads>>>(keys, vals, kout, vout, n, 0, doff, lookback, counter, err,
+                                    spin_limit);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(err_bits, err, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  return e;
 }
 
 cudaError_t launch_bounds(const uint32_t* keys, int n, int count, uint32_t* out, bool upper,

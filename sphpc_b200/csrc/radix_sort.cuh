@@ -69,6 +69,11 @@ __device__ __forceinline__ void count_key_digits(uint32_t* s_hist, uint32_t key,
     atomicAdd(&s_hist[p * kRadix + ((key >> (p * kRadixBits)) & (kRadix - 1))], 1u);
 }
 
+// Failure-detection check of the look-back wait: one onesweep CTA waits on a
+// flag that no CTA ever writes, with a poll limit of spin_limit; returns the
+// error bits it raised (kErrSortSpin when the bounded wait gave up).
+cudaError_t lookback_wait_probe(int spin_limit, uint32_t* err_bits);
+
 // lower_bound / upper_bound of every c in [0, count) over sorted keys
 // (FindLowerBounds / FindUpperBounds, thrust_c.cu:93-120).
 cudaError_t launch_bounds(const uint32_t* keys, int n, int count, uint32_t* out, bool upper,

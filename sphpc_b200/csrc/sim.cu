@@ -54,7 +54,9 @@ static int bits_for(uint32_t v) {  // bits needed to hold values 0..v
 
 class DeviceSim {
  public:
-  int n = 0;
+  int n = 0;    // active particles (struct Particles' local_count)
+  int cap = 0;  // capacity of every per-particle array (max_local, as the
+                // reference mirrors particles.c:1056-1078)
   SphpcSolver solver{};
   cudaStream_t stream = nullptr;
   double rho0 = 1000.0, mass = 1.0;
@@ -92,6 +94,19 @@ class DeviceSim {
   MlpState mlp{};
   uint4 *nr = nullptr, *nr_alt = nullptr;  // 16-byte neighbour records (x* fixed point, payload)
   uint4* nr_w = nullptr;         // third record buffer (warm start, feature export)
+  // carried warm start: the multiplier sum_k s_k lambda_k applied to each
+  // particle over the last step (slot order of that step), and whether it
+  // holds one
+  float* lam_acc = nullptr;
+  bool have_carry = false;
+  // slab decomposition: global id and ownership of every particle (host
+  // order), the records a pack keeps, and pack counters
+  bool slab = false;
+  uint32_t* gid = nullptr;
+  uint8_t* owned = nullptr;
+  SlabRecord* slab_keep = nullptr;
+  uint32_t* slab_counters = nullptr;
+  uint32_t slab_nkeep = 0;
   int last_warm_rejected = 0;
   double prev_err0 = -1.0;       // first residual of the previous step (< 0: none)
   std::vector<double> trace;     // max density error at each evaluation of the step
@@ -144,7 +159,8 @@ class DeviceSim {
     mlp_release(mlp);
     for (void* h : pinned) cudaHostUnregister(h);
     pinned.clear();
-    dfree(nr); dfree(nr_alt); dfree(nr_w);
+    dfree(nr); dfree(nr_alt); dfree(nr_w); dfree(lam_acc);
+    dfree(gid); dfree(owned); dfree(slab_keep); dfree(slab_counters);
     for (auto& p : pending) {
       cudaEventDestroy(p.a);
       cudaEventDestroy(p.b);
@@ -154,24 +170,26 @@ class DeviceSim {
     ev_pool.clear();
   }
 
-  int alloc(int n_) {
+  int alloc(int n_, int cap_) {
     n = n_;
-    SPHPC_RC(dalloc(&pd, n)); SPHPC_RC(dalloc(&pd_alt, n));
-    SPHPC_RC(dalloc(&nr, n)); SPHPC_RC(dalloc(&nr_alt, n));
-    SPHPC_RC(dalloc(&vel, n)); SPHPC_RC(dalloc(&vel_alt, n));
-    SPHPC_RC(dalloc(&color, n)); SPHPC_RC(dalloc(&omega, n)); SPHPC_RC(dalloc(&dp, n));
-    SPHPC_RC(dalloc(&rho, n)); SPHPC_RC(dalloc(&lam, n));
-    SPHPC_RC(dalloc(&ids, n)); SPHPC_RC(dalloc(&ids_spare, n));
-    SPHPC_RC(dalloc(&keys_by_id, n)); SPHPC_RC(dalloc(&loc_by_id, n));
-    SPHPC_RC(dalloc(&cellp, n)); SPHPC_RC(dalloc(&ncount, n));
-    SPHPC_RC(dalloc(&nbr, (size_t)kMaxNeighbors * n));
-    SPHPC_RC(dalloc(&xsa, n));
-    SPHPC_CK(cudaMemsetAsync(ncount, 0, n, stream));
+    cap = cap_ > n_ ? cap_ : n_;
+    const int c = cap;
+    SPHPC_RC(dalloc(&pd, c)); SPHPC_RC(dalloc(&pd_alt, c));
+    SPHPC_RC(dalloc(&nr, c)); SPHPC_RC(dalloc(&nr_alt, c));
+    SPHPC_RC(dalloc(&vel, c)); SPHPC_RC(dalloc(&vel_alt, c));
+    SPHPC_RC(dalloc(&color, c)); SPHPC_RC(dalloc(&omega, c)); SPHPC_RC(dalloc(&dp, c));
+    SPHPC_RC(dalloc(&rho, c)); SPHPC_RC(dalloc(&lam, c));
+    SPHPC_RC(dalloc(&ids, c)); SPHPC_RC(dalloc(&ids_spare, c));
+    SPHPC_RC(dalloc(&keys_by_id, c)); SPHPC_RC(dalloc(&loc_by_id, c));
+    SPHPC_RC(dalloc(&cellp, c)); SPHPC_RC(dalloc(&ncount, c));
+    SPHPC_RC(dalloc(&nbr, (size_t)kMaxNeighbors * c));
+    SPHPC_RC(dalloc(&xsa, c));
+    SPHPC_CK(cudaMemsetAsync(ncount, 0, c, stream));
     SPHPC_RC(dalloc(&small, 8));
     SPHPC_RC(dalloc(&resid, 16));
-    SPHPC_RC(dalloc(&sort.keys_alt, n));
-    SPHPC_RC(dalloc(&sort.vals_alt, n));
-    const size_t aux = sort_aux_words(n) + 4;
+    SPHPC_RC(dalloc(&sort.keys_alt, c));
+    SPHPC_RC(dalloc(&sort.vals_alt, c));
+    const size_t aux = sort_aux_words(c) + 4;
     SPHPC_RC(dalloc(&sort_aux, aux));
     sort.hist = sort_aux;
     sort.counters = sort_aux + (size_t)kMaxPasses * kRadix;
@@ -179,26 +197,26 @@ class DeviceSim {
     sort.lookback = sort_aux + (size_t)kMaxPasses * kRadix + kMaxPasses + 4;
     SPHPC_CK(cudaMemsetAsync(small, 0, 8 * sizeof(uint32_t), stream));
     SPHPC_CK(cudaMemsetAsync(sort_aux, 0, aux * sizeof(uint32_t), stream));
-    SPHPC_CK(cudaMemsetAsync(pd, 0, sizeof(PD) * n, stream));
-    SPHPC_CK(cudaMemsetAsync(vel, 0, sizeof(float4) * n, stream));
-    SPHPC_CK(cudaMemsetAsync(color, 0, sizeof(float4) * n, stream));
-    SPHPC_CK(cudaMemsetAsync(omega, 0, sizeof(float4) * n, stream));
-    SPHPC_CK(cudaMemsetAsync(dp, 0, sizeof(float4) * n, stream));
-    SPHPC_CK(cudaMemsetAsync(lam, 0, sizeof(float) * n, stream));
+    SPHPC_CK(cudaMemsetAsync(pd, 0, sizeof(PD) * c, stream));
+    SPHPC_CK(cudaMemsetAsync(vel, 0, sizeof(float4) * c, stream));
+    SPHPC_CK(cudaMemsetAsync(color, 0, sizeof(float4) * c, stream));
+    SPHPC_CK(cudaMemsetAsync(omega, 0, sizeof(float4) * c, stream));
+    SPHPC_CK(cudaMemsetAsync(dp, 0, sizeof(float4) * c, stream));
+    SPHPC_CK(cudaMemsetAsync(lam, 0, sizeof(float) * c, stream));
     return SPHPC_OK;
   }
 
   int ensure_full_alts() {
-    if (!color_alt) SPHPC_RC(dalloc(&color_alt, n));
-    if (!omega_alt) SPHPC_RC(dalloc(&omega_alt, n));
-    if (!dp_alt) SPHPC_RC(dalloc(&dp_alt, n));
-    if (!rho_alt) SPHPC_RC(dalloc(&rho_alt, n));
-    if (!lam_alt) SPHPC_RC(dalloc(&lam_alt, n));
+    if (!color_alt) SPHPC_RC(dalloc(&color_alt, cap));
+    if (!omega_alt) SPHPC_RC(dalloc(&omega_alt, cap));
+    if (!dp_alt) SPHPC_RC(dalloc(&dp_alt, cap));
+    if (!rho_alt) SPHPC_RC(dalloc(&rho_alt, cap));
+    if (!lam_alt) SPHPC_RC(dalloc(&lam_alt, cap));
     return SPHPC_OK;
   }
 
   int ensure_stage() {
-    if (!stage) SPHPC_RC(dalloc(&stage, (size_t)20 * n));
+    if (!stage) SPHPC_RC(dalloc(&stage, (size_t)20 * cap));
     return SPHPC_OK;
   }
 
@@ -247,7 +265,7 @@ class DeviceSim {
     if (passes > kMaxPasses) passes = kMaxPasses;
     SPHPC_RC(dalloc(&cstart, (size_t)C + 1));
     dfree(gaps);
-    SPHPC_RC(dalloc(&gaps, (size_t)n + 4 + C / 4096));
+    SPHPC_RC(dalloc(&gaps, (size_t)cap + 4 + C / 4096));
     SPHPC_CK(cudaMemsetAsync(cstart, 0, sizeof(uint32_t) * ((size_t)C + 1), stream));
     grid_ready = true;
     nbr_valid = false;
@@ -351,17 +369,28 @@ class DeviceSim {
 
   DevParams params(const Params& prm, const AABB* b, const Obstacle* ob) const;
 
-  int find_neighbors(const DevParams& P, bool predict, bool full, bool move_vel);
+  int slab_setup(uint32_t first_gid, double lo, double hi, bool has_left, bool has_right);
+  int find_neighbors(const DevParams& P, bool predict, bool full, bool move_vel,
+                     const float* carry_src = nullptr, uint4* carry_out = nullptr);
   int run_step(const DevParams& P, const Params& prm);
 
+  int ensure_carry_buffers() {
+    if (!nr_w) SPHPC_RC(dalloc(&nr_w, cap));
+    if (!lam_acc) {
+      SPHPC_RC(dalloc(&lam_acc, cap));
+      have_carry = false;
+    }
+    return SPHPC_OK;
+  }
+
   int ensure_warm_buffers() {
-    if (!nr_w) SPHPC_RC(dalloc(&nr_w, n));
-    if (mlp.feat_cap < n) {
+    if (!nr_w) SPHPC_RC(dalloc(&nr_w, cap));
+    if (mlp.feat_cap < cap) {
       if (mlp.feat) cudaFree(mlp.feat);
       mlp.feat = nullptr;
       mlp.feat_cap = 0;
-      SPHPC_RC(dalloc(&mlp.feat, (size_t)n * kMlpIn));
-      mlp.feat_cap = n;
+      SPHPC_RC(dalloc(&mlp.feat, (size_t)cap * kMlpIn));
+      mlp.feat_cap = cap;
     }
     return SPHPC_OK;
   }
@@ -475,7 +504,21 @@ DevParams DeviceSim::params(const Params& prm, const AABB* b, const Obstacle* ob
   return P;
 }
 
-int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool move_vel) {
+int DeviceSim::slab_setup(uint32_t first_gid, double lo, double hi, bool has_left,
+                          bool has_right) {
+  if (!gid) SPHPC_RC(dalloc(&gid, cap));
+  if (!owned) SPHPC_RC(dalloc(&owned, cap));
+  if (!slab_keep) SPHPC_RC(dalloc(&slab_keep, cap));
+  if (!slab_counters) SPHPC_RC(dalloc(&slab_counters, 4));
+  launch_slab_init(n, ids, pd, first_gid, lo, hi, has_left, has_right, gid, owned, stream);
+  SPHPC_CK(cudaGetLastError());
+  slab = true;
+  slab_nkeep = 0;
+  return SPHPC_OK;
+}
+
+int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool move_vel,
+                              const float* carry_src, uint4* carry_out) {
   if (!grid_ready) return set_error(SPHPC_ENOTREADY, "neighbour grid not initialised");
   {
     Scope sc(this, "hash");
@@ -510,6 +553,8 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
       ex.in1[0] = rho; ex.out1[0] = rho_alt;
       ex.in1[1] = lam; ex.out1[1] = lam_alt;
     }
+    ex.carry_src = carry_src;
+    ex.nr_carry = carry_src ? carry_out : nullptr;
     const bool mv = move_vel || full;
     launch_reorder(P, R, loc_by_id, pd, vel, pd_alt, vel_alt, xsa, nr, cellp, predict, mv, &ex,
                    stream);
@@ -523,6 +568,8 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
       std::swap(rho, rho_alt);
       std::swap(lam, lam_alt);
     }
+    // the carried multipliers follow this reorder only when it gathered them
+    if (!carry_src) have_carry = false;
     uint32_t* old = ids;
     ids = R;
     if (R == ids_spare) ids_spare = old;
@@ -552,8 +599,16 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   // in a pass or two that the network cannot beat.
   const bool mild = solver.warm_start_min_error > 0.0 && prev_err0 >= 0.0 &&
                     prev_err0 <= solver.warm_start_min_error;
-  const bool warm = !collect && solver.warm_start && mlp.ready && !mild;
-  SPHPC_RC(find_neighbors(P, true, false, warm || collect));
+  // warm start from the network (source 0) or from the multipliers the last
+  // step applied, carried through this step's sort permutation (source 1)
+  const bool carry_mode = !collect && solver.warm_start && solver.warm_start_source == 1;
+  if (carry_mode) SPHPC_RC(ensure_carry_buffers());
+  const bool warm_net = !collect && solver.warm_start && solver.warm_start_source != 1 &&
+                        mlp.ready && !mild;
+  const bool warm_carry = carry_mode && have_carry && !mild;
+  const bool warm = warm_net || warm_carry;
+  SPHPC_RC(find_neighbors(P, true, false, warm_net || collect,
+                          warm_carry ? lam_acc : nullptr, warm_carry ? nr_w : nullptr));
   const NbrView V = view();
   PassArgs a{};
   a.rho = rho;
@@ -591,7 +646,13 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     if (trace.size() < 16) trace.push_back(max_err);
     return SPHPC_OK;
   };
-  auto pass_b = [&](const uint4* in, float stiffness, bool last) {
+  // carried mode: lam_acc collects the multiplier the network stands for,
+  // Lambda = sum over the first kCarrySubsteps substeps of stiffness *
+  // lambda_p (a kept warm pass is those substeps); the first such pass of
+  // the step (or the first after a discarded warm pass) starts it
+  constexpr int kCarrySubsteps = 2;
+  bool acc_restart = true;
+  auto pass_b = [&](const uint4* in, float stiffness, bool last, bool acc) {
     Scope sc(this, "position");
     a.pd = pd;
     a.pd_out = pd_alt;
@@ -599,12 +660,17 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     a.nr_out = nr;
     a.stiffness = stiffness;
     a.last = last ? 1 : 0;
+    a.lam_acc = (carry_mode && acc) ? lam_acc : nullptr;
+    a.acc_add = acc_restart ? 0 : 1;
+    if (a.lam_acc) acc_restart = false;
     launch_position(P, V, a, 0, stream);
+    a.lam_acc = nullptr;
     launches += 1;
     std::swap(pd, pd_alt);
   };
   int iters = 0, plain = 0;
   bool converged = false, stalled = false;
+  bool carry_done = false;  // lam_acc holds the kept warm pass's Lambda
   const uint4* ready = nullptr;  // records with lambda for the next B (its A already run)
   if (collect) {
     // the first A also writes the features of the (predicted) state; the
@@ -618,9 +684,9 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     launches += 1;
     ready = nr_alt;
   } else if (warm) {
-    SPHPC_RC(ensure_warm_buffers());
     double err0 = 0.0, err1 = 0.0;
-    {
+    if (warm_net) {
+      SPHPC_RC(ensure_warm_buffers());
       Scope sc(this, "mlp_features");
       SPHPC_CK(cudaMemsetAsync(resid, 0, 2 * sizeof(double), stream));
       a.pd = pd;
@@ -628,6 +694,11 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       launch_features_bf16(P, V, a, reinterpret_cast<__nv_bfloat16*>(mlp.feat), mlp.dev.norm,
                            stream);
       launches += 1;
+    } else {
+      // carried: the plain first density pass (lambda_0 into nr_alt for the
+      // gate's fallback) gives the first residual; nr_w already holds the
+      // records with the carried multipliers (written by the reorder)
+      SPHPC_RC(pass_a(nr_alt, true));
     }
     SPHPC_RC(read_resid(err0));
     if (err0 <= tol && adaptive) {
@@ -637,7 +708,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       // lambda_0 converges in a pass or two, which the network cannot beat
       ready = nr_alt;
     } else {
-      {
+      if (warm_net) {
         Scope sc(this, "mlp_forward");
         launch_mlp_forward_bf16(mlp.dev, reinterpret_cast<const __nv_bfloat16*>(mlp.feat), n,
                                 nr_alt, nr_w, err(), stream, (float)solver.warm_start_scale);
@@ -645,7 +716,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       }
       // the network's multipliers, applied at full stiffness in one pass;
       // pd_alt keeps the predicted positions until the gate has decided
-      pass_b(nr_w, 1.0f, false);
+      pass_b(nr_w, 1.0f, false, true);
       ++iters;
       last_warm = 1.0;
       SPHPC_RC(pass_a(nr_w, true));
@@ -660,9 +731,11 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
         last_warm_rejected = 1;
         std::swap(pd, pd_alt);
         ready = nr_alt;
+        acc_restart = true;
       } else {
         ready = nr_w;
         plain = 1;  // the warm pass takes the place of plain substep 0
+        carry_done = true;
       }
     }
   }
@@ -700,7 +773,7 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
       launches += 1;
     }
     const bool last = !adaptive && iters == plain_cap - 1;
-    pass_b(src, stiff, last);
+    pass_b(src, stiff, last, !carry_done && plain < kCarrySubsteps);
     fused_velocity = last;
     ++plain;
     ++iters;
@@ -718,6 +791,11 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   }
   last_iterations = iters;
   last_converged = converged ? 1 : 0;
+  // a step with no position pass applied no multiplier
+  if (carry_mode) {
+    if (acc_restart) SPHPC_CK(cudaMemsetAsync(lam_acc, 0, sizeof(float) * n, stream));
+    have_carry = true;
+  }
   prev_err0 = (adaptive && !trace.empty()) ? trace[0] : -1.0;
   // post-solve passes (simulation.c:93-106) on the records nr (payload: the
   // density); the last one writes x = x*, d = 0 (UpdatePositions) into pd_alt
@@ -907,7 +985,7 @@ static int enter_data(Particles* particles, const Params* params, DeviceSim** ou
   s->solver = current_solver();
   s->rho0 = particles->rest_density;
   s->mass = particles->rest_mass;
-  int rc = s->alloc(particles->local_count);
+  int rc = s->alloc(particles->local_count, particles->max_local);
   if (!rc) {
     // Page-lock the large host arrays in place: the reference's calloc'd
     // arrays stay the caller's, only their transfers get faster.  Arrays
@@ -1442,8 +1520,156 @@ int sphpc_step(struct Particles* particles, const struct Params* params,
   if (!params || !boundary_global) return set_error(SPHPC_EINVAL, "sphpc_step: null argument");
   if (steps < 0) return set_error(SPHPC_EINVAL, "sphpc_step: negative step count");
   if (!s->grid_ready) SPHPC_RC(s->init_grid(*boundary_global, params->smoothing_radius));
+  if (s->slab && (s->solver.adaptive || s->solver.warm_start))
+    return set_error(SPHPC_EINVAL, "sphpc_step: a slab of a decomposed domain steps with the "
+                                   "fixed iteration count (adaptive and warm_start off): its "
+                                   "residual would include the halo");
   const DevParams P = s->params(*params, boundary_global, obstacle);
   for (int k = 0; k < steps; ++k) SPHPC_RC(s->run_step(P, *params));
+  return SPHPC_OK;
+}
+
+// ---- slab decomposition along x ----
+
+int sphpc_slab_init(struct Particles* particles, unsigned int first_gid, double node_start_x,
+                    double node_end_x, int has_left, int has_right) {
+  SPHPC_SIM(s, particles);
+  if (!(node_end_x > node_start_x))
+    return set_error(SPHPC_EINVAL, "sphpc_slab_init: empty slab [%g, %g)", node_start_x, node_end_x);
+  return s->slab_setup(first_gid, node_start_x, node_end_x, has_left != 0, has_right != 0);
+}
+
+int sphpc_slab_halo_width(const struct Params* params, const struct SphpcSolver* solver,
+                          double* width) {
+  if (!params || !solver || !width) return set_error(SPHPC_EINVAL, "sphpc_slab_halo_width: null");
+  const int hops = 2 * solver->solve_iterations + (solver->surface_tension ? 2 : 0) + 1 +
+                   (solver->vorticity ? 2 : 0);
+  // one h per hop, one more for the list built at the predicted positions,
+  // and the motion of the influencing and the influenced particle in a step
+  // (velocities are clamped to velocity_max)
+  *width = (hops + 1) * params->smoothing_radius +
+           2.0 * solver->velocity_max * params->time_step;
+  return SPHPC_OK;
+}
+
+int sphpc_slab_pack(struct Particles* particles, double node_start_x, double node_end_x,
+                    double halo_width, int has_left, int has_right, void* send_left,
+                    void* send_right, int send_capacity, int* count_left, int* count_right) {
+  SPHPC_SIM(s, particles);
+  if (!s->slab) return set_error(SPHPC_ENOTREADY, "sphpc_slab_pack: call sphpc_slab_init first");
+  if (send_capacity < 0 || (send_capacity > 0 && (!send_left || !send_right)) || !count_left ||
+      !count_right || !(node_end_x > node_start_x) || !(halo_width > 0.0))
+    return set_error(SPHPC_EINVAL, "sphpc_slab_pack: bad arguments");
+  SPHPC_CK(cudaMemsetAsync(s->slab_counters, 0, 4 * sizeof(uint32_t), s->stream));
+  launch_slab_pack(s->n, s->ids, s->gid, s->owned, s->pd, s->vel, node_start_x, node_end_x,
+                   halo_width, has_left != 0, has_right != 0, s->slab_keep,
+                   static_cast<SlabRecord*>(send_left), static_cast<SlabRecord*>(send_right),
+                   s->slab_counters, (uint32_t)s->cap, (uint32_t)send_capacity, s->stream);
+  SPHPC_CK(cudaGetLastError());
+  uint32_t h[3];
+  SPHPC_CK(cudaMemcpyAsync(h, s->slab_counters, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  *count_left = (int)h[1];
+  *count_right = (int)h[2];
+  if (h[0] > (uint32_t)s->cap)
+    return set_error(SPHPC_ENOMEM, "sphpc_slab_pack: %u kept particles exceed max_local %d", h[0],
+                     s->cap);
+  if (h[1] > (uint32_t)send_capacity || h[2] > (uint32_t)send_capacity)
+    return set_error(SPHPC_ENOMEM, "sphpc_slab_pack: %u / %u records exceed the send capacity %d",
+                     h[1], h[2], send_capacity);
+  s->slab_nkeep = h[0];
+  return SPHPC_OK;
+}
+
+int sphpc_slab_unpack(struct Particles* particles, const void* recv_left, int count_left,
+                      const void* recv_right, int count_right) {
+  SPHPC_SIM(s, particles);
+  if (!s->slab) return set_error(SPHPC_ENOTREADY, "sphpc_slab_unpack: call sphpc_slab_init first");
+  if (count_left < 0 || count_right < 0 || (count_left > 0 && !recv_left) ||
+      (count_right > 0 && !recv_right))
+    return set_error(SPHPC_EINVAL, "sphpc_slab_unpack: bad arguments");
+  const long long m = (long long)s->slab_nkeep + count_left + count_right;
+  if (m > s->cap)
+    return set_error(SPHPC_ENOMEM, "sphpc_slab_unpack: %lld particles exceed max_local %d", m,
+                     s->cap);
+  if (m == 0) return set_error(SPHPC_EINVAL, "sphpc_slab_unpack: no particles left");
+  SlabParts parts{s->slab_keep, static_cast<const SlabRecord*>(recv_left),
+                  static_cast<const SlabRecord*>(recv_right), s->slab_nkeep,
+                  (uint32_t)count_left, (uint32_t)count_right};
+  // the new working set in gid order: sort (gid, record index)
+  launch_slab_keys(parts, s->keys_by_id, s->stream);
+  const cudaError_t e = radix_sort_pairs(s->keys_by_id, s->loc_by_id, (int)m, kMaxPasses, s->sort,
+                                         s->stream, false, true, true, nullptr, nullptr);
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "sphpc_slab_unpack: %s", cudaGetErrorString(e));
+  launch_slab_load(parts, s->loc_by_id, s->pd, s->vel, s->gid, s->owned, s->ids, s->stream);
+  SPHPC_CK(cudaGetLastError());
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  s->n = (int)m;
+  particles->local_count = (int)m;
+  s->slab_nkeep = 0;
+  s->nbr_valid = false;
+  s->have_carry = false;
+  s->prev_err0 = -1.0;
+  s->keys_sorted = nullptr;
+  uint32_t herr = 0;
+  SPHPC_CK(cudaMemcpy(&herr, s->sort.err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (herr) return set_error(SPHPC_EKERNEL, "sphpc_slab_unpack: sort error bits 0x%x", herr);
+  return SPHPC_OK;
+}
+
+int sphpc_slab_owned(const struct Particles* particles, unsigned int* gids, double* xyz,
+                     double* vel, int capacity, int* count) {
+  SPHPC_SIM(s, particles);
+  if (!s->slab) return set_error(SPHPC_ENOTREADY, "sphpc_slab_owned: call sphpc_slab_init first");
+  if (!count || capacity < 0 || (capacity > 0 && (!gids || !xyz || !vel)))
+    return set_error(SPHPC_EINVAL, "sphpc_slab_owned: bad arguments");
+  SPHPC_CK(cudaMemsetAsync(s->slab_counters + 3, 0, sizeof(uint32_t), s->stream));
+  // the keep buffer is free between an unpack and the next pack
+  launch_slab_owned(s->n, s->ids, s->gid, s->owned, s->pd, s->vel, s->slab_keep,
+                    s->slab_counters + 3, (uint32_t)s->cap, s->stream);
+  SPHPC_CK(cudaGetLastError());
+  uint32_t c = 0;
+  SPHPC_CK(cudaMemcpyAsync(&c, s->slab_counters + 3, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+  SPHPC_CK(cudaStreamSynchronize(s->stream));
+  s->slab_nkeep = 0;
+  *count = (int)c;
+  if ((int)c > capacity)
+    return set_error(SPHPC_EINVAL, "sphpc_slab_owned: %u owned particles exceed capacity %d", c,
+                     capacity);
+  std::vector<SlabRecord> h(c);
+  if (c) SPHPC_CK(cudaMemcpy(h.data(), s->slab_keep, sizeof(SlabRecord) * c, cudaMemcpyDeviceToHost));
+  for (uint32_t k = 0; k < c; ++k) {
+    uint32_t g;
+    memcpy(&g, &h[k].a.w, sizeof(g));
+    gids[k] = g;
+    xyz[3 * k] = h[k].a.x; xyz[3 * k + 1] = h[k].a.y; xyz[3 * k + 2] = h[k].a.z;
+    vel[3 * k] = h[k].b.x; vel[3 * k + 1] = h[k].b.y; vel[3 * k + 2] = h[k].b.z;
+  }
+  return SPHPC_OK;
+}
+
+// BalanceNodes, geometry.c:102-166: with the particle counts and slab
+// lengths of this rank and its neighbours (the reference trades them with
+// MPI_Sendrecv), moves the slab's ends by h towards an even share.
+int sphpc_balance_nodes(int rank, int proc_count, int num_rank, int num_right,
+                        double length_left, double length_right, int global_count,
+                        struct Params* params) {
+  if (!params || proc_count < 1 || rank < 0 || rank >= proc_count)
+    return set_error(SPHPC_EINVAL, "sphpc_balance_nodes: bad arguments");
+  const double h = params->smoothing_radius;
+  const double length = params->node_end_x - params->node_start_x;
+  const int even_particles = (int)(global_count / (double)proc_count);
+  const int max_diff = (int)(even_particles / 10.0f);
+  const int diff_right = num_right - even_particles;
+  const int diff_self = num_rank - even_particles;
+  if (diff_self > max_diff && length > 2 * h && rank != 0)
+    params->node_start_x += h;
+  else if (diff_self < -max_diff && length_left > 2 * h && rank != 0)
+    params->node_start_x -= h;
+  if (diff_right > max_diff && length_right > 2 * h && rank != proc_count - 1)
+    params->node_end_x += h;
+  else if (diff_right < -max_diff && length > 2 * h && rank != proc_count - 1)
+    params->node_end_x -= h;
   return SPHPC_OK;
 }
 
@@ -1721,6 +1947,34 @@ int SortByKey(unsigned int* const keys, unsigned int* const values, const int co
     return set_error(SPHPC_EKERNEL, "SortByKey: look-back wait gave up (error bits 0x%x)", herr);
   }
   return SPHPC_OK;
+}
+
+// ---- failure detection of the bounded device waits ----
+
+static int wait_check(const char* what, cudaError_t e, uint32_t bits, unsigned int* out) {
+  if (out) *out = bits;
+  if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+  if (bits) return set_error(SPHPC_EKERNEL, "%s: the bounded wait gave up (error bits 0x%x)",
+                             what, bits);
+  return SPHPC_OK;
+}
+
+int sphpc_check_sort_wait(int spin_limit, unsigned int* error_bits) {
+  if (spin_limit < 1 || spin_limit > kSpinLimit)
+    return set_error(SPHPC_EINVAL, "sphpc_check_sort_wait: limit %d outside [1, %d]", spin_limit,
+                     kSpinLimit);
+  uint32_t bits = 0;
+  const cudaError_t e = lookback_wait_probe(spin_limit, &bits);
+  return wait_check("sphpc_check_sort_wait", e, bits, error_bits);
+}
+
+int sphpc_check_mbarrier_wait(int poll_limit, unsigned int* error_bits) {
+  if (poll_limit < 1 || poll_limit > (1 << 20))
+    return set_error(SPHPC_EINVAL, "sphpc_check_mbarrier_wait: limit %d outside [1, 2^20]",
+                     poll_limit);
+  uint32_t bits = 0;
+  const cudaError_t e = mbar_wait_probe(poll_limit, &bits);
+  return wait_check("sphpc_check_mbarrier_wait", e, bits, error_bits);
 }
 
 int FindLowerBounds(const unsigned int* const hash_values, const int value_count,

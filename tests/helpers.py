@@ -53,3 +53,60 @@ def rel_err_stats(got, want):
     want = np.asarray(want, np.float64)
     scale = max(np.max(np.abs(want)), 1e-300)
     return float(np.max(np.abs(got - want)) / scale)
+
+
+def oracle_block(sim, state, lo, hi, idx=None):
+    """An OracleSim over the particles of `sim` whose step-start position x
+    lies in the box [lo, hi) (three-vectors), or over the given indices, in
+    their original order, with the scene's parameters and grid (so hash keys,
+    cells and the order within a cell, hence the 60-neighbour cap, are those
+    of the whole set).  Returns (oracle, indices of the particles in the
+    whole set)."""
+    import copy
+
+    x = np.stack([state["x"], state["y"], state["z"]])
+    if idx is None:
+        inside = np.all((x >= np.asarray(lo)[:, None]) & (x < np.asarray(hi)[:, None]), axis=0)
+        idx = np.nonzero(inside)[0]
+    sc = copy.copy(scene_from_ini(sim.path))
+    sc.x0 = np.ascontiguousarray(x[:, idx])
+    o = OracleSim(sc)
+    for f, of in FIELD_MAP.items():
+        if f in state:
+            o.a[of][:] = state[f][idx]
+    return o, idx
+
+
+def interior(state, idx, lo, hi, margin):
+    """Mask over idx of the particles at least `margin` inside the box."""
+    x = np.stack([state["x"][idx], state["y"][idx], state["z"][idx]])
+    lo = np.asarray(lo, np.float64)[:, None] + margin
+    hi = np.asarray(hi, np.float64)[:, None] - margin
+    return np.all((x >= lo) & (x < hi), axis=0)
+
+
+def err_stats(got, want, scale=None):
+    """Max and median of |got - want| / |want| (relative) and the max of
+    |got - want| / max|want| (relative to the field's scale)."""
+    got = np.asarray(got, np.float64)
+    want = np.asarray(want, np.float64)
+    err = np.abs(got - want)
+    s = scale if scale is not None else max(float(np.max(np.abs(want))), 1e-300)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rel = np.where(want != 0, err / np.abs(want), np.where(err == 0, 0.0, np.inf))
+    return {"max_rel": float(np.max(rel)), "median_rel": float(np.median(rel)),
+            "max_of_scale": float(np.max(err) / s), "n": int(err.size)}
+
+
+def parity_record(name, record):
+    """Appends one measured-error record to $SPHPC_PARITY_OUT (JSON lines),
+    when set, and prints it."""
+    import json
+    import os
+
+    line = json.dumps({"test": name, **record})
+    print("PARITY", line)
+    out = os.environ.get("SPHPC_PARITY_OUT")
+    if out:
+        with open(out, "a") as f:
+            f.write(line + "\n")

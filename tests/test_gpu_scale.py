@@ -1,0 +1,202 @@
+"""Parity at the workload sizes: the device path (through the C ABI) against
+the FP64 oracle on the same evolved state, at 1,048,576 particles (the whole
+set) and at 16,777,216 particles (blocks of the scene).
+
+Each test evolves the scene on the device, then from that state compares
+* the first constraint substep's density and lambda (ComputeDensities and
+  ComputeLambda, particles.c:461-514, 588-666, on the predicted positions of
+  the step: ApplyGravity, PredictPositions, FindAllNeighbors first), and
+* one whole fused step (sphpc_step, the loop body simulation.c:56-116) with
+  the configuration's fixed iteration count: final positions, velocities and
+  the last density evaluation.
+Tolerances are those of the small-scene tests (tests/test_gpu_parity.py);
+the measured errors are printed as PARITY records (and appended to
+$SPHPC_PARITY_OUT when set).
+
+Where the step is ill-conditioned -- the 16.7M block where the falling fluid
+meets the sphere, compressed and pushed out of the obstacle through six stiff
+Jacobi iterations -- a change of the input below FP32 resolution moves the
+FP64 result by more than the fixed tolerance.  There the oracle is run a
+second time from the same state with every position moved by one FP32 ulp
+(up or down at random), and each particle's velocity may also differ by four
+times the change that caused: the device is then held to the problem's own
+FP32 noise floor, particle by particle, and the record says how many
+particles needed that allowance.
+
+A block of the 16.7M scene is checked by running the oracle on the particles
+inside a box and comparing only those far enough inside that every
+neighbour hop of the compared quantity stays in the box: a step of I
+iterations reads neighbours 2I times in the solve (density then position
+pass), twice for surface tension, once for XSPH and twice for vorticity
+confinement, each hop reaching at most h (lists are fixed at the step's
+predicted positions) plus the distance a particle moves in the step.
+"""
+import numpy as np
+import pytest
+
+from helpers import (assert_close, err_stats, interior, load_state, oracle_block, oracle_for,
+                     oracle_state, parity_record)
+from sphpc_b200.simulation import Simulation
+
+pytestmark = pytest.mark.gpu
+
+POS = ("x", "y", "z")
+VEL = ("v_x", "v_y", "v_z")
+
+
+def _oracle_step_with_stage(o):
+    """One oracle step stage by stage (oracle_step's order), returning the
+    density and lambda of substep 0 and leaving the state after the step."""
+    p = o.p
+    o.call("apply_gravity")
+    o.call("predict_positions")
+    o.call("find_all_neighbors")
+    stage = None
+    for sub in range(p.solve_iterations):
+        o.call("compute_densities")
+        o.call("compute_lambda")
+        if sub == 0:
+            stage = {"density": o.a["rho"].copy(), "lambda": o.a["lam"].copy()}
+        o.call("update_dps", sub)
+        o.call("update_position_stars")
+    o.call("update_velocities")
+    if p.enable_tension:
+        o.call("surface_tension")
+    o.call("apply_viscosity")
+    if p.enable_vorticity:
+        o.call("compute_vorticity")
+        o.call("vorticity_confinement")
+    o.call("update_positions")
+    return stage
+
+
+def _device_stage(sim, st0):
+    """Density and lambda of substep 0 from state st0, through the
+    reference-named step functions of the C ABI."""
+    sim.push(st0)
+    sim.apply_gravity()
+    sim.predict_positions()
+    sim.find_all_neighbors()
+    sim.compute_densities()
+    sim.compute_lambda()
+    sim.fetch_fields(["density", "lambda"])
+    return {"density": sim.host("density").copy(), "lambda": sim.host("lambda").copy()}
+
+
+def _check_stage(name, got, want, mask=None):
+    m = slice(None) if mask is None else mask
+    assert_close(got["density"][m], want["density"][m], 1e-5, 0.0, what=f"{name}:density")
+    assert_close(got["lambda"][m], want["lambda"][m], 1e-4, 1e-5, what=f"{name}:lambda")
+    return {f: err_stats(got[f][m], want[f][m]) for f in ("density", "lambda")}
+
+
+def _check_step(name, got, want, mask=None, sens=None):
+    """sens: per-field |oracle(state moved by one FP32 ulp) - oracle(state)|,
+    an extra per-particle allowance of four times that change."""
+    m = slice(None) if mask is None else mask
+    rec = {}
+    for f in POS:
+        assert_close(got[f][m], want[f][m], 1e-6, 0.0, atol=1e-6, what=f"{name}:{f}")
+        rec[f] = err_stats(got[f][m], want[f][m])
+    vscale = max(float(np.max(np.abs(want[f][m]))) for f in VEL)
+    for f in VEL:
+        rec[f] = err_stats(got[f][m], want[f][m], scale=vscale)
+        base = 1e-5 * np.abs(want[f][m]) + 2e-5 * vscale
+        err = np.abs(got[f][m] - want[f][m])
+        if sens is not None:
+            extra = 4.0 * sens[f][m]
+            rec[f]["beyond_fixed_tolerance"] = int(np.sum(err > base))
+            rec[f]["ulp_sensitivity_max_of_scale"] = float(np.max(sens[f][m]) / vscale)
+            bad = err > base + extra
+        else:
+            bad = err > base
+        assert not np.any(bad), (name, f, int(bad.sum()), float(np.max(err - base) / vscale))
+    assert_close(got["density"][m], want["density"][m], 1e-5, 0.0, what=f"{name}:density")
+    rec["density"] = err_stats(got["density"][m], want["density"][m])
+    return rec
+
+
+def test_dam_break_1m_whole_set_matches_oracle():
+    """1,048,576 particles (dam_break_1m: 4 iterations, XSPH, vorticity
+    confinement), 60 steps into the collapse, every particle compared."""
+    with Simulation("dam_break_1m") as sim:
+        sim.step(60)
+        st0 = sim.fetch()
+        sim.step(1)
+        sim.fetch_fields(list(POS + VEL) + ["density"])
+        got = {f: sim.host(f).copy() for f in POS + VEL + ("density",)}
+        assert sim.device_errors() == 0
+        o = oracle_for(sim, st0)
+        want_stage = _oracle_step_with_stage(o)
+        want = oracle_state(o)
+        rec = {"step": _check_step("1m:step", got, want)}
+        got_stage = _device_stage(sim, st0)
+        rec["stage"] = _check_stage("1m:stage", got_stage, want_stage)
+        assert sim.device_errors() == 0
+        parity_record("dam_break_1m_whole_set", {"n": sim.n, "steps_before": 60, **rec})
+
+
+def _hops(o):
+    p = o.p
+    return 2 * p.solve_iterations + (2 if p.enable_tension else 0) + 1 + \
+        (2 if p.enable_vorticity else 0)
+
+
+def test_full_16m_blocks_match_oracle():
+    """16,777,216 particles (full_16m: 6 iterations, surface tension,
+    vorticity confinement, the torus+sphere obstacle) 200 steps in, when the
+    falling block meets the sphere: the oracle runs on two boxes of the
+    scene, one around the particle of largest density error and one at the
+    free surface, and the particles deep enough inside each are compared."""
+    with Simulation("full_16m") as sim:
+        h = sim.params.smoothing_radius
+        sim.step(200)
+        st0 = sim.fetch()
+        sim.step(1)
+        sim.fetch_fields(list(POS + VEL) + ["density"])
+        got = {f: sim.host(f).copy() for f in POS + VEL + ("density",)}
+        assert sim.device_errors() == 0
+        got_stage = _device_stage(sim, st0)
+        assert sim.device_errors() == 0
+
+        x = np.stack([st0["x"], st0["y"], st0["z"]])
+        rho0 = sim.particles.rest_density
+        worst = int(np.argmax(st0["density"] / rho0))
+        top = int(np.argmax(st0["y"]))
+        centres = {"max_density_error": x[:, worst], "free_surface": x[:, top]}
+        inner = 24.0
+        records = {}
+        for tag, c in centres.items():
+            # margin: every hop of the step, one h each, plus the motion of a step
+            hops = 2 * sim.solver.solve_iterations + (2 if sim.solver.surface_tension else 0) \
+                + 1 + (2 if sim.solver.vorticity else 0)
+            margin = (hops + 1) * h + 2.0
+            lo = c - inner / 2 - margin
+            hi = c + inner / 2 + margin
+            o, idx = oracle_block(sim, st0, lo, hi)
+            assert _hops(o) == hops   # the oracle runs the same passes
+            want_stage = _oracle_step_with_stage(o)
+            want = oracle_state(o)
+            # the same block from the state moved by one FP32 ulp
+            rng = np.random.default_rng(7)
+            st1 = dict(st0)
+            for f in POS:
+                v32 = st0[f].astype(np.float32)
+                up = rng.random(v32.size) < 0.5
+                st1[f] = np.where(up, np.nextafter(v32, np.float32(np.inf)),
+                                  np.nextafter(v32, np.float32(-np.inf))).astype(np.float64)
+            o1, _ = oracle_block(sim, st1, lo, hi, idx=idx)
+            _oracle_step_with_stage(o1)
+            w1 = oracle_state(o1)
+            sens = {f: np.abs(w1[f] - want[f]) for f in VEL}
+            m_step = interior(st0, idx, lo, hi, margin)
+            m_stage = interior(st0, idx, lo, hi, 3.0 * h)
+            assert m_step.sum() > 1000, (tag, int(m_step.sum()))
+            g = {f: got[f][idx] for f in got}
+            gs = {f: got_stage[f][idx] for f in got_stage}
+            rec = {"box_particles": int(idx.size), "compared_step": int(m_step.sum()),
+                   "compared_stage": int(m_stage.sum()),
+                   "step": _check_step(f"16m:{tag}:step", g, want, m_step, sens),
+                   "stage": _check_stage(f"16m:{tag}:stage", gs, want_stage, m_stage)}
+            records[tag] = rec
+        parity_record("full_16m_blocks", {"n": sim.n, "steps_before": 200, **records})
