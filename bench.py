@@ -35,10 +35,11 @@ UNIT = "particle-steps/s"
 # reference-layout stage: x* and cell in, one count byte and ~30 four-byte
 # list entries out.
 STAGE_BYTES = {
-    "hash": 24,                             # r x*; w key, index
+    "hash": 60,                             # r record {x, d} 32, v 16, id 4; w key, slot 4 + 4
     "radix_sort": None,                     # 16 B per digit pass + 4, set below
     "cell_starts": 4,                       # + 8 per cell, added below
-    "reorder": 104,                         # gather x, x*, v, id: read and write
+    "reorder": 124,                         # r sorted id 4, slot 4, record 32, v 16;
+                                            # w record 32, x* 16, neighbour record 16, cell 4
     "build_neighbors": 16 + 4 + 1 + 4 * 30,
     "density_lambda": 24,
     "position": 36,
@@ -351,6 +352,24 @@ def run_ours(args, world, rank, local, dist):
                     "issue_active_ncu": ncu_stage(name).get("issue_active_pct"),
                     "avg_launch_ms": tot / cnt}
 
+    # the HBM-bound stages (hash, sort, cell starts, reorder), each against
+    # the measured copy bandwidth on its algorithmic bytes
+    hbm_class = {}
+    if prof:
+        peak, kind = peaks()
+        for name in ("hash", "radix_sort", "cell_starts", "reorder"):
+            if name not in prof or not prof[name][0]:
+                continue
+            cnt, tot = prof[name]
+            per = STAGE_BYTES[name]
+            if name == "radix_sort":
+                per = 16 * sim_passes(sim) + 4
+            if name == "cell_starts":
+                per = 4 + 8 * sim_cells(sim) / n
+            gbs = per * n / (tot / cnt / 1e3) / 1e9
+            hbm_class[name] = {"bytes_per_particle": per, "avg_launch_ms": tot / cnt,
+                               "achieved_gbs": gbs, "frac": gbs / peak}
+
     # end to end through the C ABI with host buffers, over the same steps of
     # the scene as the headline arm (a fresh particle set, W untimed steps)
     e2e = None
@@ -427,6 +446,7 @@ def run_ours(args, world, rank, local, dist):
         "gpu_launches": launches,
         "clocks": clocks,
         "roofline": roof,
+        "hbm_class_roofline": hbm_class,
         "stage_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()},
         "like_for_like": like,
         "e2e": e2e,
@@ -440,9 +460,11 @@ def sim_cells(sim):
 
 
 def sim_passes(sim):
+    """Digit passes of the step's sort: the fewest passes of 8- or 9-bit
+    digits over the cell keys' bits (8 bits where that is as few)."""
     C_ = sim_cells(sim)
     bits = max(1, int(C_ - 1).bit_length())
-    return (bits + 7) // 8
+    return min((bits + 7) // 8, (bits + 8) // 9)
 
 
 def ncu_stage(stage):

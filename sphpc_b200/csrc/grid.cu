@@ -60,9 +60,10 @@ __global__ void __launch_bounds__(kBlock)
     k_hash(const DevParams P, const PD* __restrict__ pd, const float4* __restrict__ vel,
            const uint32_t* __restrict__ ids,
            uint32_t* __restrict__ keys_by_id, uint32_t* __restrict__ loc_by_id,
-           uint32_t* __restrict__ hist, int passes, int predict, uint32_t* __restrict__ err) {
-  __shared__ uint32_t s_hist[kMaxPasses * kRadix];
-  for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) s_hist[i] = 0;
+           uint32_t* __restrict__ hist, int passes, int bits, int predict,
+           uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_hist[kMaxPasses * kHistStride];
+  for (int i = threadIdx.x; i < kMaxPasses * kHistStride; i += blockDim.x) s_hist[i] = 0;
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < P.n) {
@@ -82,10 +83,10 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t id = __ldg(ids + i);
     keys_by_id[id] = key;
     loc_by_id[id] = (uint32_t)i;
-    count_key_digits(s_hist, key, passes);
+    count_key_digits(s_hist, key, passes, bits);
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < passes * kRadix; k += blockDim.x)
+  for (int k = threadIdx.x; k < passes * kHistStride; k += blockDim.x)
     if (s_hist[k]) atomicAdd(hist + k, s_hist[k]);
 }
 
@@ -362,18 +363,45 @@ done:
 
 // ---------------------------------------------------------------------------
 // Staged neighbour build (FillNeighbors, neighbors.c:217-298): one thread per
-// particle walks its 9 (dz, dy) slot rows as k_build_neighbors does, but
-// appends every candidate without branches to its own column of a
-// shared-memory staging area (store the slot, advance the count on a hit;
-// the particle itself is skipped by splitting its own row), and the block
-// writes the buckets out at the end as whole columns of nbr[60][n]: for each
-// entry index, a warp's 32 consecutive slots are one 128-byte line.
+// particle walks its 9 (dz, dy) slot rows in the reference's order (rows of
+// cells cx-1..cx+1 are contiguous slot ranges, cells in dx order, particles
+// in ascending original index), appending every candidate without branches
+// to its own column of a shared-memory staging area -- store the entry,
+// advance the count on a hit; the particle itself is skipped by splitting
+// its own row -- and writes its bucket out at the end as column entries of
+// nbr[60][n] (for each entry index, a warp's 32 consecutive slots are one
+// 128-byte line).  A staged entry is 2 bytes, (row << 12) | offset in the
+// row, with the row starts kept in shared memory, so a thread holds 156
+// bytes of shared memory and the candidate loop only the particle's FP32
+// position: enough blocks stay resident to hide the candidate loads.  A
+// particle with a row of more than 4095 candidates takes the verbatim
+// 27-cell walk.
 // ---------------------------------------------------------------------------
 constexpr int kStagedBlock = 128;
+constexpr int kRowBits = 12;
+constexpr int kRowMax = (1 << kRowBits) - 1;
 
-__device__ __forceinline__ void staged_range(const BuildCtx& c, const PD* __restrict__ pd,
-                                             const float4* __restrict__ xsa, int ja, int jb,
-                                             uint32_t* __restrict__ stg, int& cnt) {
+// Exact FP64 test of neighbors.c:278-285 for particle p and candidate j
+// (rare: only pairs whose FP32 r^2 lies in the band); reloads both records.
+__device__ __forceinline__ bool staged_exact(const DevParams& P, const PD* __restrict__ pd, int p,
+                                          int j) {
+  float4 xp, dpp, xq, dq;
+  ld_pd(pd, p, xp, dpp);
+  ld_pd(pd, j, xq, dq);
+  const double ddx = __dsub_rn(xstar_d(xp.x, dpp.x), xstar_d(xq.x, dq.x));
+  const double ddy = __dsub_rn(xstar_d(xp.y, dpp.y), xstar_d(xq.y, dq.y));
+  const double ddz = __dsub_rn(xstar_d(xp.z, dpp.z), xstar_d(xq.z, dq.z));
+  const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)),
+                              __dmul_rn(ddz, ddz));
+  return r2 < P.h2d;
+}
+
+// Appends the candidates of slots [ja, jb) of row r (starting at slot rb).
+__device__ __forceinline__ void staged_range(const DevParams& P, const PD* __restrict__ pd,
+                                             const float4* __restrict__ xsa, float px, float py,
+                                             float pz, int p, int r, int rb, int ja, int jb,
+                                             uint16_t* __restrict__ stg, int& cnt) {
+  const uint32_t tag = (uint32_t)r << kRowBits;
   int j = ja;
   for (; j + 4 <= jb && cnt <= kMaxNeighbors - 4; j += 4) {
     float4 q[4];
@@ -381,294 +409,91 @@ __device__ __forceinline__ void staged_range(const BuildCtx& c, const PD* __rest
     for (int u = 0; u < 4; ++u) q[u] = __ldg(xsa + j + u);
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const float fx = c.xf.x - q[u].x, fy = c.xf.y - q[u].y, fz = c.xf.z - q[u].z;
+      const float fx = px - q[u].x, fy = py - q[u].y, fz = pz - q[u].z;
       const float r2 = fx * fx + fy * fy + fz * fz;
-      bool hit = r2 <= c.h2hi;
-      if (hit && r2 >= c.h2lo) hit = exact_neighbor(c, pd, j + u);
-      stg[cnt * kStagedBlock] = (uint32_t)(j + u);
+      bool hit = r2 <= P.bld_h2hi;
+      if (hit && r2 >= P.bld_h2lo) hit = staged_exact(P, pd, p, j + u);
+      stg[cnt * kStagedBlock] = (uint16_t)(tag | (uint32_t)(j + u - rb));
       cnt += hit ? 1 : 0;
     }
   }
   for (; j < jb && cnt < kMaxNeighbors; ++j) {
     const float4 q = __ldg(xsa + j);
-    const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
+    const float fx = px - q.x, fy = py - q.y, fz = pz - q.z;
     const float r2 = fx * fx + fy * fy + fz * fz;
-    bool hit = r2 <= c.h2hi;
-    if (hit && r2 >= c.h2lo) hit = exact_neighbor(c, pd, j);
-    stg[cnt * kStagedBlock] = (uint32_t)j;
+    bool hit = r2 <= P.bld_h2hi;
+    if (hit && r2 >= P.bld_h2lo) hit = staged_exact(P, pd, p, j);
+    stg[cnt * kStagedBlock] = (uint16_t)(tag | (uint32_t)(j - rb));
     cnt += hit ? 1 : 0;
   }
 }
 
-__global__ void __launch_bounds__(kStagedBlock)
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kStagedBlock, kMinBlocks)
     k_build_staged(const DevParams P, const NbrView V, const PD* __restrict__ pd,
                    const float4* __restrict__ xsa, const uint32_t* __restrict__ cellp,
                    uint32_t* __restrict__ nbr, uint8_t* __restrict__ ncount) {
-  __shared__ uint32_t s_stage[kMaxNeighbors * kStagedBlock];
+  __shared__ uint16_t s_stage[kMaxNeighbors * kStagedBlock];
+  __shared__ int s_rowb[9 * kStagedBlock];
   const int p = blockIdx.x * kStagedBlock + threadIdx.x;
   if (p >= P.n) return;
-  uint32_t* stg = s_stage + threadIdx.x;
+  uint16_t* stg = s_stage + threadIdx.x;
+  int* rowb = s_rowb + threadIdx.x;
   const size_t stride = (size_t)P.n;
   BuildCtx c;
   ld_pd(pd, p, c.xp, c.dp);
-  c.xf = __ldg(xsa + p);
   c.xs = xstar_d(c.xp.x, c.dp.x);
   c.ys = xstar_d(c.xp.y, c.dp.y);
   c.zs = xstar_d(c.xp.z, c.dp.z);
-  c.h2lo = P.bld_h2lo;
-  c.h2hi = P.bld_h2hi;
-  c.h2d = P.h2d;
   int cx, cy, cz;
   unpack_cell(V, __ldg(cellp + p), cx, cy, cz);
-  const bool regular = axis_regular(c.xs, P.hd, cx, P.nx) &&
-                       axis_regular(c.ys, P.hd, cy, P.ny) &&
-                       axis_regular(c.zs, P.hd, cz, P.nz);
+  bool regular = axis_regular(c.xs, P.hd, cx, P.nx) && axis_regular(c.ys, P.hd, cy, P.ny) &&
+                 axis_regular(c.zs, P.hd, cz, P.nz);
+  // the 9 rows' slot ranges (empty outside the grid)
+  const int xlo = cx - (cx > 0);
+  const int xhi = cx + (cx < P.nx - 1);
+  if (regular) {
+    for (int r = 0; r < 9; ++r) {
+      const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+      int b = 0, e = 0;
+      if ((unsigned)z < (unsigned)P.nz && (unsigned)y < (unsigned)P.ny) {
+        const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
+        b = (int)__ldg(V.cstart + rk + xlo);
+        e = (int)__ldg(V.cstart + rk + xhi + 1);
+      }
+      if (e - b > kRowMax) regular = false;  // the row offset would not fit
+      rowb[r * kStagedBlock] = b;
+    }
+  }
   int count = 0;
   if (regular) {
-    const int xlo = cx - (cx > 0);
-    const int xhi = cx + (cx < P.nx - 1);
-    for (int dz = -1; dz <= 1 && count < kMaxNeighbors; ++dz) {
-      const int z = cz + dz;
-      if ((unsigned)z >= (unsigned)P.nz) continue;
-      for (int dy = -1; dy <= 1 && count < kMaxNeighbors; ++dy) {
-        const int y = cy + dy;
-        if ((unsigned)y >= (unsigned)P.ny) continue;
-        const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
-        const int b = (int)__ldg(V.cstart + rk + xlo);
-        const int e = (int)__ldg(V.cstart + rk + xhi + 1);
-        if (dz == 0 && dy == 0) {
-          staged_range(c, pd, xsa, b, p, stg, count);
-          staged_range(c, pd, xsa, p + 1, e, stg, count);
-        } else {
-          staged_range(c, pd, xsa, b, e, stg, count);
-        }
+    const float4 xf = __ldg(xsa + p);
+    for (int r = 0; r < 9 && count < kMaxNeighbors; ++r) {
+      const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+      if ((unsigned)z >= (unsigned)P.nz || (unsigned)y >= (unsigned)P.ny) continue;
+      const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
+      const int b = rowb[r * kStagedBlock];
+      const int e = (int)__ldg(V.cstart + rk + xhi + 1);
+      if (r == 4) {
+        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, b, p, stg, count);
+        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, p + 1, e, stg, count);
+      } else {
+        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, b, e, stg, count);
       }
     }
-    for (int t = 0; t < count; ++t) nbr[(size_t)t * stride + p] = stg[t * kStagedBlock];
+    for (int t = 0; t < count; ++t) {
+      const uint32_t en = stg[t * kStagedBlock];
+      nbr[(size_t)t * stride + p] =
+          (uint32_t)(rowb[(en >> kRowBits) * kStagedBlock] + (int)(en & kRowMax));
+    }
   } else {
+    c.xf = __ldg(xsa + p);
+    c.h2lo = P.bld_h2lo;
+    c.h2hi = P.bld_h2hi;
+    c.h2d = P.h2d;
     count = walk_27_cells(P, V, c, pd, xsa, p, nbr + p, stride);
   }
   ncount[p] = (uint8_t)count;
-}
-
-// ---------------------------------------------------------------------------
-// Cell-cooperative neighbour build (FillNeighbors, neighbors.c:217-298).
-//
-// Regular particles of one cell share their candidate list: the 9 (dz, dy)
-// rows of cells cx-1..cx+1, each a contiguous slot range, concatenated in the
-// reference's order (dz, then dy, then dx and ascending sorted index).  One
-// warp takes a window of 32 slots; for each run of particles of the same cell
-// in the window (m particles), every particle gets L = 32 / m lanes and each
-// lane tests a contiguous part of the list, so all lanes of the warp step
-// through the same candidates in lockstep (one broadcast load serves the m
-// particles) with no divergence between cells.  Hits are appended without
-// branches to the lane's column of a shared-memory staging area; the parts'
-// counts are prefix-summed within each particle, which puts the hits in the
-// reference's order and truncates at 60 exactly as the per-candidate walk
-// does; the buckets are then written as whole columns of nbr[60][n].
-// Particles whose neighbour cells are not cx-1..cx+1 take the verbatim
-// 27-cell walk on their own lane.
-// ---------------------------------------------------------------------------
-constexpr int kCoopWarps = 4;
-constexpr int kRows = 9;
-
-struct CoopRow {
-  int b, e, off;  // slot range [b, e) at offset off of the concatenated list
-};
-
-// Tests slots [ja, jb) against the lane's particle, appending the hits (in
-// slot order) to the lane's staging column stg[t * 32 + lane], t < 60.
-__device__ __forceinline__ void coop_range(const BuildCtx& c, const PD* __restrict__ pd,
-                                           const float4* __restrict__ xsa, int ja, int jb,
-                                           uint32_t* __restrict__ stg, int lane, int& cnt) {
-  int j = ja;
-  // batches of four while four more entries fit below the cap
-  for (; j + 4 <= jb && cnt <= kMaxNeighbors - 4; j += 4) {
-    float4 q[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) q[u] = __ldg(xsa + j + u);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const float fx = c.xf.x - q[u].x, fy = c.xf.y - q[u].y, fz = c.xf.z - q[u].z;
-      const float r2 = fx * fx + fy * fy + fz * fz;
-      bool hit = r2 <= c.h2hi;
-      if (hit && r2 >= c.h2lo) hit = exact_neighbor(c, pd, j + u);
-      stg[cnt * 32 + lane] = (uint32_t)(j + u);
-      cnt += hit ? 1 : 0;
-    }
-  }
-  for (; j < jb && cnt < kMaxNeighbors; ++j) {
-    const float4 q = __ldg(xsa + j);
-    const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
-    const float r2 = fx * fx + fy * fy + fz * fz;
-    bool hit = r2 <= c.h2hi;
-    if (hit && r2 >= c.h2lo) hit = exact_neighbor(c, pd, j);
-    stg[cnt * 32 + lane] = (uint32_t)j;
-    cnt += hit ? 1 : 0;
-  }
-}
-
-// The lane's part [a, b) of the concatenated candidate list of particle p;
-// the particle itself (in row 4, the (0, 0) row) is skipped.
-__device__ __forceinline__ void coop_walk(const BuildCtx& c, const CoopRow* rows, int a, int b,
-                                          int p, const PD* __restrict__ pd,
-                                          const float4* __restrict__ xsa,
-                                          uint32_t* __restrict__ stg, int lane, int& cnt) {
-  int r = 0;
-  while (r < kRows - 1 && rows[r + 1].off <= a) ++r;
-  for (; a < b && r < kRows && cnt < kMaxNeighbors; ++r) {
-    const CoopRow R = rows[r];
-    const int end = min(b, R.off + (R.e - R.b));
-    if (end <= a) continue;
-    const int ja = R.b + (a - R.off), jb = R.b + (end - R.off);
-    if (r == 4) {
-      coop_range(c, pd, xsa, ja, min(jb, p), stg, lane, cnt);
-      coop_range(c, pd, xsa, max(ja, p + 1), jb, stg, lane, cnt);
-    } else {
-      coop_range(c, pd, xsa, ja, jb, stg, lane, cnt);
-    }
-    a = end;
-  }
-}
-
-__global__ void __launch_bounds__(kCoopWarps * 32)
-    k_build_coop(const DevParams P, const NbrView V, const PD* __restrict__ pd,
-                 const float4* __restrict__ xsa, const uint32_t* __restrict__ cellp,
-                 uint32_t* __restrict__ nbr, uint8_t* __restrict__ ncount) {
-  __shared__ uint32_t s_stage[kCoopWarps][kMaxNeighbors * 32];
-  __shared__ CoopRow s_rows[kCoopWarps][kRows];
-  __shared__ int s_off[kCoopWarps][32];
-  constexpr uint32_t kAll = 0xffffffffu;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int win = (blockIdx.x * kCoopWarps + w) * 32;
-  if (win >= P.n) return;  // the whole warp
-  uint32_t* stg = s_stage[w];
-  CoopRow* rows = s_rows[w];
-  int* offs = s_off[w];
-  const size_t stride = (size_t)P.n;
-
-  // the lane's own slot: position, cell, and whether its neighbour cells are
-  // cx-1..cx+1 on every axis
-  const int s = win + lane;
-  const bool valid = s < P.n;
-  BuildCtx c;
-  c.h2lo = P.bld_h2lo;
-  c.h2hi = P.bld_h2hi;
-  c.h2d = P.h2d;
-  uint32_t cp = kAll;
-  bool regular = false;
-  if (valid) {
-    ld_pd(pd, s, c.xp, c.dp);
-    c.xf = __ldg(xsa + s);
-    c.xs = xstar_d(c.xp.x, c.dp.x);
-    c.ys = xstar_d(c.xp.y, c.dp.y);
-    c.zs = xstar_d(c.xp.z, c.dp.z);
-    cp = __ldg(cellp + s);
-    int cx, cy, cz;
-    unpack_cell(V, cp, cx, cy, cz);
-    regular = axis_regular(c.xs, P.hd, cx, P.nx) && axis_regular(c.ys, P.hd, cy, P.ny) &&
-              axis_regular(c.zs, P.hd, cz, P.nz);
-  } else {
-    c.xf = make_float4(0.f, 0.f, 0.f, 0.f);
-    c.xs = c.ys = c.zs = 0.0;
-  }
-  const uint32_t vmask = __ballot_sync(kAll, valid);
-  const int nv = __popc(vmask);  // valid lanes are a prefix of the warp
-  const uint32_t cp_prev = __shfl_up_sync(kAll, cp, 1);
-  uint32_t heads = __ballot_sync(kAll, valid && (lane == 0 || cp != cp_prev));
-
-  while (heads) {
-    const int r0 = __ffs(heads) - 1;
-    heads &= heads - 1;
-    const int r1 = heads ? __ffs(heads) - 1 : nv;
-    const int m = r1 - r0;
-    // the 9 rows of the run's cell and their offsets in the list
-    const uint32_t rcp = __shfl_sync(kAll, cp, r0);
-    int rb = 0, re = 0;
-    if (lane < kRows) {
-      int cx, cy, cz;
-      unpack_cell(V, rcp, cx, cy, cz);
-      const int z = cz + lane / 3 - 1, y = cy + lane % 3 - 1;
-      if ((unsigned)z < (unsigned)P.nz && (unsigned)y < (unsigned)P.ny) {
-        const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
-        const int xlo = cx - (cx > 0);
-        const int xhi = cx + (cx < P.nx - 1);
-        rb = (int)__ldg(V.cstart + rk + xlo);
-        re = (int)__ldg(V.cstart + rk + xhi + 1);
-      }
-    }
-    const int len = re - rb;
-    int incl = len;
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-      const int y = __shfl_up_sync(kAll, incl, o);
-      if (lane >= o) incl += y;
-    }
-    if (lane < kRows) rows[lane] = CoopRow{rb, re, incl - len};
-    const int T = __shfl_sync(kAll, incl, kRows - 1);
-    __syncwarp();
-
-    // L lanes per particle; lane (i, k) tests part k of particle i's list
-    const int L = 32 / m;
-    const int i = lane / L, k = lane - (lane / L) * L;
-    const bool act = i < m;
-    const int src = r0 + (act ? i : 0);
-    BuildCtx pc;
-    pc.h2lo = c.h2lo;
-    pc.h2hi = c.h2hi;
-    pc.h2d = c.h2d;
-    pc.xf.x = __shfl_sync(kAll, c.xf.x, src);
-    pc.xf.y = __shfl_sync(kAll, c.xf.y, src);
-    pc.xf.z = __shfl_sync(kAll, c.xf.z, src);
-    pc.xs = __shfl_sync(kAll, c.xs, src);
-    pc.ys = __shfl_sync(kAll, c.ys, src);
-    pc.zs = __shfl_sync(kAll, c.zs, src);
-    const bool preg = __shfl_sync(kAll, regular ? 1 : 0, src) != 0;
-    const int pp = win + src;
-    int cnt = 0;
-    if (act && preg) {
-      const int a = (int)((long long)T * k / L);
-      const int b = (int)((long long)T * (k + 1) / L);
-      coop_walk(pc, rows, a, b, pp, pd, xsa, stg, lane, cnt);
-    }
-    // where each part's hits start in its particle's bucket
-    int incl2 = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(kAll, incl2, o);
-      if (lane >= o) incl2 += y;
-    }
-    const int before = __shfl_sync(kAll, incl2, act && i > 0 ? i * L - 1 : 0);
-    const int base = act && i > 0 ? before : 0;
-    const int last = __shfl_sync(kAll, incl2, act ? i * L + L - 1 : 0);
-    offs[lane] = incl2 - cnt - base;
-    const int pcount = act ? min(last - base, kMaxNeighbors) : 0;
-    __syncwarp();
-    // write-out: lane -> particle i2 = lane % m, entry e0 + lane / m
-    const int maxc = __reduce_max_sync(kAll, (unsigned)pcount);
-    const int i2 = lane % m;
-    const int cnt2 = __shfl_sync(kAll, pcount, i2 * L);
-    const bool wl = lane < m * L;
-    for (int e0 = 0; e0 < maxc; e0 += L) {
-      const int e = e0 + lane / m;
-      if (wl && e < cnt2) {
-        int lo = 0, hi = L - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (offs[i2 * L + mid] <= e) lo = mid;
-          else hi = mid - 1;
-        }
-        const int kl = i2 * L + lo;
-        nbr[(size_t)e * stride + (size_t)(win + r0 + i2)] = stg[(e - offs[kl]) * 32 + kl];
-      }
-    }
-    if (act && k == 0 && preg) ncount[pp] = (uint8_t)pcount;
-    __syncwarp();  // the staging area and rows belong to the next run
-  }
-  if (valid && !regular) {
-    const int cnt = walk_27_cells(P, V, c, pd, xsa, s, nbr + s, stride);
-    ncount[s] = (uint8_t)cnt;
-  }
 }
 
 __global__ void __launch_bounds__(kBlock)
@@ -691,9 +516,9 @@ __global__ void __launch_bounds__(kBlock)
 
 void launch_hash(const DevParams& P, const PD* pd, const float4* vel, const uint32_t* ids,
                  uint32_t* keys_by_id, uint32_t* loc_by_id, uint32_t* hist, int passes,
-                 bool predict, uint32_t* err, cudaStream_t st) {
+                 int bits, bool predict, uint32_t* err, cudaStream_t st) {
   k_hash<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, vel, ids, keys_by_id, loc_by_id, hist,
-                                           passes, predict ? 1 : 0, err);
+                                           passes, bits, predict ? 1 : 0, err);
 }
 
 void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
@@ -725,22 +550,21 @@ void launch_build_neighbors(const DevParams& P, const NbrView& V, const PD* pd,
   static const int build_kind = [] {
     const char* e = getenv("SPHPC_NEIGHBOR_BUILD");
     if (e && strcmp(e, "lane") == 0) return 1;
-    if (e && strcmp(e, "staged") == 0) return 2;
+    if (e && strcmp(e, "staged10") == 0) return 2;
     return 0;
   }();
-  if (build_kind == 2) {
-    k_build_staged<<<grid_for(P.n, kStagedBlock), kStagedBlock, 0, st>>>(P, V, pd, xsa, cellp,
-                                                                          nbr, ncount);
-    return;
-  }
   if (build_kind == 1) {
     k_build_neighbors<<<grid_for(P.n, kBuildBlock), kBuildBlock, 0, st>>>(P, V, pd, xsa, cellp,
                                                                            nbr, ncount);
     return;
   }
-  const int warps = (P.n + 31) / 32;
-  k_build_coop<<<(warps + kCoopWarps - 1) / kCoopWarps, kCoopWarps * 32, 0, st>>>(
-      P, V, pd, xsa, cellp, nbr, ncount);
+  if (build_kind == 2) {
+    k_build_staged<10><<<grid_for(P.n, kStagedBlock), kStagedBlock, 0, st>>>(P, V, pd, xsa, cellp,
+                                                                              nbr, ncount);
+    return;
+  }
+  k_build_staged<9><<<grid_for(P.n, kStagedBlock), kStagedBlock, 0, st>>>(P, V, pd, xsa, cellp,
+                                                                           nbr, ncount);
 }
 
 void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr, int32_t* count,

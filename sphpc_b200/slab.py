@@ -160,26 +160,32 @@ class DistExchange:
         return self._recv[0], nfl, self._recv[1], nfr
 
 
-def step_local(domains, steps: int = 1):
-    """Steps slabs that one process holds (in slab order along x), handing
-    each neighbour's records over by device copies."""
+def exchange_local(domains):
+    """One exchange among slabs that one process holds (in slab order along
+    x), the records handed over by device copies: afterwards every slab
+    owns the particles whose positions lie in it, and holds its halo."""
     import torch
+    counts = [d.pack() for d in domains]
+    recv = []
+    for i, d in enumerate(domains):
+        nfl = counts[i - 1][1] if i > 0 else 0
+        nfr = counts[i + 1][0] if i + 1 < len(domains) else 0
+        if nfl:
+            d.recv[0][:nfl * RECORD_BYTES].copy_(domains[i - 1].send[1][:nfl * RECORD_BYTES])
+        if nfr:
+            d.recv[1][:nfr * RECORD_BYTES].copy_(domains[i + 1].send[0][:nfr * RECORD_BYTES])
+        recv.append((d.recv[0], nfl, d.recv[1], nfr))
+    torch.cuda.synchronize()
+    for d, r in zip(domains, recv):
+        d.unpack(*r)
+
+
+def step_local(domains, steps: int = 1):
+    """Steps slabs that one process holds (in slab order along x): each step
+    one exchange (exchange_local), then the fused step of every slab."""
     for _ in range(steps):
-        counts = [d.pack() for d in domains]
-        recv = []
-        for i, d in enumerate(domains):
-            nfl = counts[i - 1][1] if i > 0 else 0
-            nfr = counts[i + 1][0] if i + 1 < len(domains) else 0
-            rl = d.recv[0]
-            rr = d.recv[1]
-            if nfl:
-                rl[:nfl * RECORD_BYTES].copy_(domains[i - 1].send[1][:nfl * RECORD_BYTES])
-            if nfr:
-                rr[:nfr * RECORD_BYTES].copy_(domains[i + 1].send[0][:nfr * RECORD_BYTES])
-            recv.append((rl, nfl, rr, nfr))
-        torch.cuda.synchronize()
-        for d, r in zip(domains, recv):
-            d.unpack(*r)
+        exchange_local(domains)
+        for d in domains:
             d.sim.step(1)
 
 

@@ -110,7 +110,13 @@ def _check_step(name, got, want, mask=None, sens=None):
             bad = err > base + extra
         else:
             bad = err > base
-        assert not np.any(bad), (name, f, int(bad.sum()), float(np.max(err - base) / vscale))
+        rec[f]["failed"] = int(bad.sum())
+        if np.any(bad):
+            k = int(np.argmax(err - base - (extra if sens is not None else 0.0)))
+            rec[f]["worst"] = {"err_of_scale": float(err[k] / vscale),
+                               "allowed_of_scale": float((base[k] + (extra[k] if sens is not None
+                                                                     else 0.0)) / vscale),
+                               "want": float(want[f][m][k])}
     assert_close(got["density"][m], want["density"][m], 1e-5, 0.0, what=f"{name}:density")
     rec["density"] = err_stats(got["density"][m], want["density"][m])
     return rec
@@ -130,6 +136,7 @@ def test_dam_break_1m_whole_set_matches_oracle():
         want_stage = _oracle_step_with_stage(o)
         want = oracle_state(o)
         rec = {"step": _check_step("1m:step", got, want)}
+        assert not any(rec["step"][f]["failed"] for f in VEL), rec["step"]
         got_stage = _device_stage(sim, st0)
         rec["stage"] = _check_stage("1m:stage", got_stage, want_stage)
         assert sim.device_errors() == 0
@@ -177,18 +184,22 @@ def test_full_16m_blocks_match_oracle():
             assert _hops(o) == hops   # the oracle runs the same passes
             want_stage = _oracle_step_with_stage(o)
             want = oracle_state(o)
-            # the same block from the state moved by one FP32 ulp
-            rng = np.random.default_rng(7)
-            st1 = dict(st0)
-            for f in POS:
-                v32 = st0[f].astype(np.float32)
-                up = rng.random(v32.size) < 0.5
-                st1[f] = np.where(up, np.nextafter(v32, np.float32(np.inf)),
-                                  np.nextafter(v32, np.float32(-np.inf))).astype(np.float64)
-            o1, _ = oracle_block(sim, st1, lo, hi, idx=idx)
-            _oracle_step_with_stage(o1)
-            w1 = oracle_state(o1)
-            sens = {f: np.abs(w1[f] - want[f]) for f in VEL}
+            # the same block from the state moved by one FP32 ulp, three
+            # draws: the largest change per particle
+            sens = {f: np.zeros(idx.size) for f in VEL}
+            for seed in (7, 8, 9):
+                rng = np.random.default_rng(seed)
+                st1 = dict(st0)
+                for f in POS:
+                    v32 = st0[f].astype(np.float32)
+                    up = rng.random(v32.size) < 0.5
+                    st1[f] = np.where(up, np.nextafter(v32, np.float32(np.inf)),
+                                      np.nextafter(v32, np.float32(-np.inf))).astype(np.float64)
+                o1, _ = oracle_block(sim, st1, lo, hi, idx=idx)
+                _oracle_step_with_stage(o1)
+                w1 = oracle_state(o1)
+                for f in VEL:
+                    sens[f] = np.maximum(sens[f], np.abs(w1[f] - want[f]))
             m_step = interior(st0, idx, lo, hi, margin)
             m_stage = interior(st0, idx, lo, hi, 3.0 * h)
             assert m_step.sum() > 1000, (tag, int(m_step.sum()))
@@ -200,3 +211,38 @@ def test_full_16m_blocks_match_oracle():
                    "stage": _check_stage(f"16m:{tag}:stage", gs, want_stage, m_stage)}
             records[tag] = rec
         parity_record("full_16m_blocks", {"n": sim.n, "steps_before": 200, **records})
+        failed = {(t, f): r["step"][f]["failed"] for t, r in records.items() for f in VEL
+                  if r["step"][f]["failed"]}
+        assert not failed, failed
+
+
+def test_full_16m_cell_sort_is_a_stable_sort_of_the_hash():
+    """At 16,777,216 particles the cell keys have 26 bits and the step's
+    radix sort runs 3 passes of 9-bit digits (smaller scenes use 8-bit
+    digits): SortHash's result (neighbors.c:128-155) must be the stable sort
+    of (key, original index) of HashVal's keys (neighbors.c:79-98,
+    restated here in FP64), and the cell starts its lower bounds."""
+    with Simulation("full_16m") as sim:
+        sim.step(3)
+        sim.apply_gravity()
+        sim.predict_positions()
+        sim.find_all_neighbors()
+        keys, ids, start = sim.cell_data()
+        st = sim.fetch(["x_star", "y_star", "z_star"])
+        nb = sim.neighbors
+        nx, ny, nz = nb.hash_size_x, nb.hash_size_y, nb.hash_size_z
+        assert int(nx * ny * nz - 1).bit_length() == 26
+        h = sim.params.smoothing_radius
+        cx = np.floor(st["x_star"] / h).astype(np.int64)
+        cy = np.floor(st["y_star"] / h).astype(np.int64)
+        cz = np.floor(st["z_star"] / h).astype(np.int64)
+        key_of = (nx * ny * cz + cy * nx + cx).astype(np.uint32)
+        ids = ids.astype(np.int64)
+        assert np.array_equal(np.sort(ids), np.arange(sim.n))
+        np.testing.assert_array_equal(keys, key_of[ids])
+        assert np.all(np.diff(keys.astype(np.int64)) >= 0)
+        same = np.diff(keys.astype(np.int64)) == 0
+        assert np.all(np.diff(ids)[same] > 0)
+        C_ = nx * ny * nz
+        np.testing.assert_array_equal(start[:C_], np.searchsorted(keys, np.arange(C_), "left"))
+        assert sim.device_errors() == 0

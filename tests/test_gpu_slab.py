@@ -28,6 +28,16 @@ def _owned_union(domains):
     return g[o], np.concatenate(xs)[o], np.concatenate(vs)[o], [len(a) for a in gs]
 
 
+def _owners(domains, n):
+    owner = np.full(n, -1)
+    for r, d in enumerate(domains):
+        g, _, _ = d.owned()
+        assert np.all(owner[g] == -1)
+        owner[g] = r
+    assert np.all(owner >= 0)
+    return owner
+
+
 def test_three_slabs_equal_the_undivided_run():
     steps_per_check = (1, 9, 30)
     with Simulation("dam_break_32k") as whole:
@@ -48,13 +58,18 @@ def test_three_slabs_equal_the_undivided_run():
                 want_v = np.stack([st["v_x"], st["v_y"], st["v_z"]], 1)
                 np.testing.assert_array_equal(x, want_x)
                 np.testing.assert_array_equal(v, want_v)
-                owner = np.concatenate([np.full(c, r) for r, c in enumerate(counts)])
                 if first_owner is None:
-                    first_owner = owner
-            # the fluid crossed slab ends: some particles changed owner, and
+                    first_owner = _owners(domains, n)
             # every slab's working set held fewer particles than the scene
-            assert np.any(owner != first_owner)
             assert all(s.particles.local_count < n for s in sims)
+            # one more exchange hands every particle to the slab its position
+            # lies in; the fluid crossed slab ends, so some changed owner
+            slab.exchange_local(domains)
+            owner = _owners(domains, n)
+            st = whole.fetch(["x"])
+            edges = np.array([b[0] for b in BOUNDS[1:]])
+            np.testing.assert_array_equal(owner, np.searchsorted(edges, st["x"], side="right"))
+            assert np.sum(owner != first_owner) > 100
             for s in sims:
                 assert s.device_errors() == 0
         finally:
