@@ -460,11 +460,10 @@ def sim_cells(sim):
 
 
 def sim_passes(sim):
-    """Digit passes of the step's sort: the fewest passes of 8- or 9-bit
-    digits over the cell keys' bits (8 bits where that is as few)."""
+    """Digit passes of the step's sort: 8-bit digits over the cell keys' bits."""
     C_ = sim_cells(sim)
     bits = max(1, int(C_ - 1).bit_length())
-    return min((bits + 7) // 8, (bits + 8) // 9)
+    return (bits + 7) // 8
 
 
 def ncu_stage(stage):

@@ -1,8 +1,5 @@
 // grid.cu -- uniform-grid hashing, particle reorder, cell-start table and the
 // neighbour build of the PBF pipeline.
-#include <cstdlib>
-#include <cstring>
-
 #include "kernels.cuh"
 
 namespace sphpc {
@@ -60,10 +57,9 @@ __global__ void __launch_bounds__(kBlock)
     k_hash(const DevParams P, const PD* __restrict__ pd, const float4* __restrict__ vel,
            const uint32_t* __restrict__ ids,
            uint32_t* __restrict__ keys_by_id, uint32_t* __restrict__ loc_by_id,
-           uint32_t* __restrict__ hist, int passes, int bits, int predict,
-           uint32_t* __restrict__ err) {
-  __shared__ uint32_t s_hist[kMaxPasses * kHistStride];
-  for (int i = threadIdx.x; i < kMaxPasses * kHistStride; i += blockDim.x) s_hist[i] = 0;
+           uint32_t* __restrict__ hist, int passes, int predict, uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_hist[kMaxPasses * kRadix];
+  for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) s_hist[i] = 0;
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < P.n) {
@@ -83,10 +79,10 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t id = __ldg(ids + i);
     keys_by_id[id] = key;
     loc_by_id[id] = (uint32_t)i;
-    count_key_digits(s_hist, key, passes, bits);
+    count_key_digits(s_hist, key, passes);
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < passes * kHistStride; k += blockDim.x)
+  for (int k = threadIdx.x; k < passes * kRadix; k += blockDim.x)
     if (s_hist[k]) atomicAdd(hist + k, s_hist[k]);
 }
 
@@ -273,94 +269,6 @@ __device__ __forceinline__ int walk_27_cells(const DevParams& P, const NbrView& 
   return count;
 }
 
-constexpr int kBuildBlock = 128;
-
-// FillNeighbors, neighbors.c:217-298: one thread per particle, bucket entries
-// written as they are found into column nbr[count][p] (L2 merges the partial
-// lines of a warp's columns).
-__global__ void __launch_bounds__(kBuildBlock, 10)
-    k_build_neighbors(const DevParams P, const NbrView V, const PD* __restrict__ pd,
-                      const float4* __restrict__ xsa, const uint32_t* __restrict__ cellp,
-                      uint32_t* __restrict__ nbr, uint8_t* __restrict__ ncount) {
-  const int p = blockIdx.x * kBuildBlock + threadIdx.x;
-  if (p >= P.n) return;
-  BuildCtx c;
-  ld_pd(pd, p, c.xp, c.dp);
-  c.xf = __ldg(xsa + p);
-  c.xs = xstar_d(c.xp.x, c.dp.x);
-  c.ys = xstar_d(c.xp.y, c.dp.y);
-  c.zs = xstar_d(c.xp.z, c.dp.z);
-  c.h2lo = P.bld_h2lo;
-  c.h2hi = P.bld_h2hi;
-  c.h2d = P.h2d;
-  int cx, cy, cz;
-  unpack_cell(V, __ldg(cellp + p), cx, cy, cz);
-  const bool regular = axis_regular(c.xs, P.hd, cx, P.nx) &&
-                       axis_regular(c.ys, P.hd, cy, P.ny) &&
-                       axis_regular(c.zs, P.hd, cz, P.nz);
-  uint32_t* out = nbr + p;
-  const size_t stride = (size_t)P.n;
-  int count = 0;
-  if (regular) {
-    // rows (dz, dy) of cells cx-1..cx+1 are contiguous slot ranges
-    const int xlo = cx - (cx > 0);
-    const int xhi = cx + (cx < P.nx - 1);
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int z = cz + dz;
-      if ((unsigned)z >= (unsigned)P.nz) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int y = cy + dy;
-        if ((unsigned)y >= (unsigned)P.ny) continue;
-        const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
-        const int b = (int)__ldg(V.cstart + rk + xlo);
-        const int e = (int)__ldg(V.cstart + rk + xhi + 1);
-        // self can only appear in the particle's own row
-        const bool self_row = dz == 0 && dy == 0;
-        int j = b;
-        for (; j + 4 <= e; j += 4) {
-          // hit and band masks of four candidates without branches; the exact
-          // test only for the rare in-band bits, then the hits in order
-          uint32_t hit = 0u, band = 0u;
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const float4 q = __ldg(xsa + j + u);
-            const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
-            const float r2 = fx * fx + fy * fy + fz * fz;
-            hit |= (uint32_t)(r2 <= c.h2hi) << u;
-            band |= (uint32_t)(r2 >= c.h2lo) << u;
-          }
-          if (self_row && (unsigned)(p - j) < 4u) hit &= ~(1u << (p - j));
-          band &= hit;
-          if (band) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-              if (((band >> u) & 1u) && !exact_neighbor(c, pd, j + u)) hit &= ~(1u << u);
-          }
-          while (hit) {
-            const int u = __ffs(hit) - 1;
-            hit &= hit - 1u;
-            out[(size_t)count * stride] = (uint32_t)(j + u);
-            if (++count == kMaxNeighbors) goto done;
-          }
-        }
-        for (; j < e; ++j) {
-          const float4 q = __ldg(xsa + j);
-          const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
-          const float r2 = fx * fx + fy * fy + fz * fz;
-          if (r2 > c.h2hi || (self_row && j == p)) continue;
-          if (r2 >= c.h2lo && !exact_neighbor(c, pd, j)) continue;
-          out[(size_t)count * stride] = (uint32_t)j;
-          if (++count == kMaxNeighbors) goto done;
-        }
-      }
-    }
-  } else {
-    count = walk_27_cells(P, V, c, pd, xsa, p, out, stride);
-  }
-done:
-  ncount[p] = (uint8_t)count;
-}
-
 // ---------------------------------------------------------------------------
 // Staged neighbour build (FillNeighbors, neighbors.c:217-298): one thread per
 // particle walks its 9 (dz, dy) slot rows in the reference's order (rows of
@@ -428,8 +336,9 @@ __device__ __forceinline__ void staged_range(const DevParams& P, const PD* __res
   }
 }
 
-template <int kMinBlocks>
-__global__ void __launch_bounds__(kStagedBlock, kMinBlocks)
+// 9 blocks of 128 threads per SM: 56 registers, no spills (a tighter cap
+// spills and gains nothing).
+__global__ void __launch_bounds__(kStagedBlock, 9)
     k_build_staged(const DevParams P, const NbrView V, const PD* __restrict__ pd,
                    const float4* __restrict__ xsa, const uint32_t* __restrict__ cellp,
                    uint32_t* __restrict__ nbr, uint8_t* __restrict__ ncount) {
@@ -516,9 +425,9 @@ __global__ void __launch_bounds__(kBlock)
 
 void launch_hash(const DevParams& P, const PD* pd, const float4* vel, const uint32_t* ids,
                  uint32_t* keys_by_id, uint32_t* loc_by_id, uint32_t* hist, int passes,
-                 int bits, bool predict, uint32_t* err, cudaStream_t st) {
+                 bool predict, uint32_t* err, cudaStream_t st) {
   k_hash<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, vel, ids, keys_by_id, loc_by_id, hist,
-                                           passes, bits, predict ? 1 : 0, err);
+                                           passes, predict ? 1 : 0, err);
 }
 
 void launch_reorder(const DevParams& P, const uint32_t* sorted_ids, const uint32_t* loc_by_id,
@@ -547,24 +456,8 @@ void launch_cell_starts(const uint32_t* keys_sorted, int n, uint32_t ncells, uin
 void launch_build_neighbors(const DevParams& P, const NbrView& V, const PD* pd,
                             const float4* xsa, const uint32_t* cellp, uint32_t* nbr,
                             uint8_t* ncount, cudaStream_t st) {
-  static const int build_kind = [] {
-    const char* e = getenv("SPHPC_NEIGHBOR_BUILD");
-    if (e && strcmp(e, "lane") == 0) return 1;
-    if (e && strcmp(e, "staged10") == 0) return 2;
-    return 0;
-  }();
-  if (build_kind == 1) {
-    k_build_neighbors<<<grid_for(P.n, kBuildBlock), kBuildBlock, 0, st>>>(P, V, pd, xsa, cellp,
-                                                                           nbr, ncount);
-    return;
-  }
-  if (build_kind == 2) {
-    k_build_staged<10><<<grid_for(P.n, kStagedBlock), kStagedBlock, 0, st>>>(P, V, pd, xsa, cellp,
-                                                                              nbr, ncount);
-    return;
-  }
-  k_build_staged<9><<<grid_for(P.n, kStagedBlock), kStagedBlock, 0, st>>>(P, V, pd, xsa, cellp,
-                                                                           nbr, ncount);
+  k_build_staged<<<grid_for(P.n, kStagedBlock), kStagedBlock, 0, st>>>(P, V, pd, xsa, cellp, nbr,
+                                                                        ncount);
 }
 
 void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr, int32_t* count,

@@ -20,10 +20,10 @@ inline int grid_for(int n, int block = kBlock) { return n > 0 ? (n + block - 1) 
 // slot order, computes the canonical x*, its cell key, and scatters the key
 // and the slot into original-index order.  When `predict` is false the
 // current x* (pos + disp) is hashed instead.  Accumulates the radix digit
-// histograms of all `passes` (digits of `bits` bits) into hist.
+// histograms of all `passes` into hist.
 void launch_hash(const DevParams& P, const PD* pd, const float4* vel, const uint32_t* ids,
                  uint32_t* keys_by_id, uint32_t* loc_by_id, uint32_t* hist, int passes,
-                 int bits, bool predict, uint32_t* err, cudaStream_t st);
+                 bool predict, uint32_t* err, cudaStream_t st);
 
 // Reorder gather: new slot j takes particle sorted_ids[j] from its old slot.
 // predict: recompute x* from x and v (+gravity) as launch_hash did, else

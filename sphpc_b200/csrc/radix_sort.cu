@@ -24,29 +24,24 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 }
 
 __global__ void __launch_bounds__(256) k_digit_histogram(const uint32_t* __restrict__ keys,
-                                                         int n, int passes, int bits,
+                                                         int n, int passes,
                                                          uint32_t* __restrict__ hist) {
-  __shared__ uint32_t s_hist[kMaxPasses * kHistStride];
-  for (int i = threadIdx.x; i < kMaxPasses * kHistStride; i += blockDim.x) s_hist[i] = 0;
+  __shared__ uint32_t s_hist[kMaxPasses * kRadix];
+  for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) s_hist[i] = 0;
   __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    count_key_digits(s_hist, __ldg(keys + i), passes, bits);
+    count_key_digits(s_hist, __ldg(keys + i), passes);
   __syncthreads();
-  for (int i = threadIdx.x; i < passes * kHistStride; i += blockDim.x)
+  for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x)
     if (s_hist[i]) atomicAdd(hist + i, s_hist[i]);
 }
 
-// Exclusive scan of each pass's 2^bits digit counts (one block, 256
-// threads, each owning 2^bits / 256 consecutive digits).
-__global__ void __launch_bounds__(256) k_scan_digits(uint32_t* __restrict__ hist, int passes,
-                                                     int bits) {
-  __shared__ uint32_t s_warp[8];
+// Exclusive scan of each pass's 256 digit counts (one block, 256 threads).
+__global__ void __launch_bounds__(256) k_scan_digits(uint32_t* __restrict__ hist, int passes) {
+  __shared__ uint32_t s_warp[kRadix / 32];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int per = (1 << bits) / 256;  // 1 or 2
   for (int p = 0; p < passes; ++p) {
-    uint32_t* h = hist + p * kHistStride + t * per;
-    uint32_t v0 = h[0], v1 = per > 1 ? h[1] : 0u;
-    const uint32_t v = v0 + v1;
+    const uint32_t v = hist[p * kRadix + t];
     uint32_t x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -57,37 +52,33 @@ __global__ void __launch_bounds__(256) k_scan_digits(uint32_t* __restrict__ hist
     __syncthreads();
     uint32_t wsum = 0;
     for (int w = 0; w < warp; ++w) wsum += s_warp[w];
-    const uint32_t excl = wsum + x - v;
-    h[0] = excl;
-    if (per > 1) h[1] = excl + v0;
+    hist[p * kRadix + t] = wsum + x - v;
     __syncthreads();
   }
 }
 
-// One digit pass of BITS bits.  vals_in == nullptr means the values are the
-// input indices (iota), which is how SortHash calls SortByKey
-// (neighbors.c:123).  The per-warp digit counters are 16-bit (a warp ranks
-// at most 512 pairs of a tile).
-template <int BITS>
-__global__ void __launch_bounds__(kSortThreads)
+// One digit pass.  vals_in == nullptr means the values are the input
+// indices (iota), which is how SortHash calls SortByKey (neighbors.c:123).
+// Three blocks per SM (80 registers, no spills) rather than the two that
+// the compiler's own choice of 128 registers leaves room for: the passes
+// wait on loads and on the look-back, so resident warps are what hides it.
+__global__ void __launch_bounds__(kSortThreads, 3)
     k_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n,
                int shift, const uint32_t* __restrict__ digit_offset,
                uint32_t* __restrict__ lookback, uint32_t* __restrict__ tile_counter,
                uint32_t* __restrict__ err, int spin_limit) {
-  constexpr int kR = 1 << BITS;          // digits
-  constexpr int kPer = kR / kSortThreads;  // digits per thread in the digit phase
   __shared__ uint32_t s_tile;
-  __shared__ uint16_t s_whist[kSortWarps][kR + 2];
-  __shared__ uint32_t s_dstart[kR];
-  __shared__ uint32_t s_gbase[kR];
-  __shared__ uint32_t s_wsum[kSortThreads / 32];
+  __shared__ uint32_t s_whist[kSortWarps][kRadix + 1];
+  __shared__ uint32_t s_dstart[kRadix];
+  __shared__ uint32_t s_gbase[kRadix];
+  __shared__ uint32_t s_wsum[kRadix / 32];
   __shared__ uint32_t s_keys[kSortTile];
   __shared__ uint32_t s_vals[kSortTile];
 
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   if (t == 0) s_tile = atomicAdd(tile_counter, 1u);
-  for (int i = t; i < kSortWarps * (kR + 2); i += kSortThreads)
+  for (int i = t; i < kSortWarps * (kRadix + 1); i += kSortThreads)
     (&s_whist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
@@ -110,13 +101,13 @@ __global__ void __launch_bounds__(kSortThreads)
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
     const int64_t idx = wbase + i * 32 + lane;
-    const uint32_t d = idx < n ? ((key[i] >> shift) & (kR - 1)) : (uint32_t)kR;
+    const uint32_t d = idx < n ? ((key[i] >> shift) & (kRadix - 1)) : (uint32_t)kRadix;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const int leader = __ffs(peers) - 1;
     uint32_t prev = 0;
     if (lane == leader) {
       prev = s_whist[warp][d];
-      s_whist[warp][d] = (uint16_t)(prev + __popc(peers));
+      s_whist[warp][d] = prev + __popc(peers);
     }
     prev = __shfl_sync(0xffffffffu, prev, leader);
     rank[i] = prev + __popc(peers & lt);
@@ -125,58 +116,47 @@ __global__ void __launch_bounds__(kSortThreads)
   __syncthreads();
 
   // Per digit: exclusive prefix over warps, the tile count, look-back.
-  // Thread t owns digits t * kPer .. t * kPer + kPer - 1.
   {
-    uint32_t cnt[kPer];
-    uint32_t tsum = 0;
+    const int d = t;  // kSortThreads == kRadix
+    uint32_t sum = 0;
 #pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-      const int d = t * kPer + k;
-      uint32_t sum = 0;
-#pragma unroll
-      for (int w = 0; w < kSortWarps; ++w) {
-        const uint32_t c = s_whist[w][d];
-        s_whist[w][d] = (uint16_t)sum;
-        sum += c;
-      }
-      cnt[k] = sum;
-      tsum += sum;
-      uint32_t* my = lookback + (size_t)tile * kR + d;
-      if (tile == 0) {
-        st_volatile(my, kLbInc | sum);
-      } else {
-        st_volatile(my, kLbAgg | sum);
-      }
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = s_whist[w][d];
+      s_whist[w][d] = sum;
+      sum += c;
     }
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-      const int d = t * kPer + k;
-      uint32_t excl = 0;
-      if (tile > 0) {
-        int64_t pt = (int64_t)tile - 1;
-        while (pt >= 0) {
-          const uint32_t* f = lookback + (size_t)pt * kR + d;
-          uint32_t v = ld_volatile(f);
-          int spins = 0;
-          while ((v & (kLbAgg | kLbInc)) == 0) {
-            if (++spins > spin_limit) {
-              atomicOr(err, 2u);  // kErrSortSpin
-              v = kLbInc;
-              break;
-            }
-            __nanosleep(32);
-            v = ld_volatile(f);
+    const uint32_t cnt = sum;
+    uint32_t* my = lookback + (size_t)tile * kRadix + d;
+    if (tile == 0) {
+      st_volatile(my, kLbInc | cnt);
+    } else {
+      st_volatile(my, kLbAgg | cnt);
+    }
+    uint32_t excl = 0;
+    if (tile > 0) {
+      int64_t pt = (int64_t)tile - 1;
+      while (pt >= 0) {
+        const uint32_t* f = lookback + (size_t)pt * kRadix + d;
+        uint32_t v = ld_volatile(f);
+        int spins = 0;
+        while ((v & (kLbAgg | kLbInc)) == 0) {
+          if (++spins > spin_limit) {
+            atomicOr(err, 2u);  // kErrSortSpin
+            v = kLbInc;
+            break;
           }
-          excl += v & kLbValue;
-          if (v & kLbInc) break;
-          --pt;
+          __nanosleep(32);
+          v = ld_volatile(f);
         }
-        st_volatile(lookback + (size_t)tile * kR + d, kLbInc | (excl + cnt[k]));
+        excl += v & kLbValue;
+        if (v & kLbInc) break;
+        --pt;
       }
-      s_gbase[d] = __ldg(digit_offset + d) + excl;
+      st_volatile(my, kLbInc | (excl + cnt));
     }
-    // tile-local exclusive scan of the counts over digits
-    uint32_t x = tsum;
+    s_gbase[d] = __ldg(digit_offset + d) + excl;
+    // tile-local exclusive scan of cnt over digits
+    uint32_t x = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -186,12 +166,7 @@ __global__ void __launch_bounds__(kSortThreads)
     __syncthreads();
     uint32_t wsum = 0;
     for (int w = 0; w < warp; ++w) wsum += s_wsum[w];
-    uint32_t run = wsum + x - tsum;
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-      s_dstart[t * kPer + k] = run;
-      run += cnt[k];
-    }
+    s_dstart[d] = wsum + x - cnt;
   }
   __syncthreads();
 
@@ -200,7 +175,7 @@ __global__ void __launch_bounds__(kSortThreads)
   for (int i = 0; i < kSortItems; ++i) {
     const int64_t idx = wbase + i * 32 + lane;
     if (idx < n) {
-      const uint32_t d = (key[i] >> shift) & (kR - 1);
+      const uint32_t d = (key[i] >> shift) & (kRadix - 1);
       const uint32_t lp = s_dstart[d] + s_whist[warp][d] + rank[i];
       s_keys[lp] = key[i];
       s_vals[lp] = val[i];
@@ -210,7 +185,7 @@ __global__ void __launch_bounds__(kSortThreads)
   const int valid = (int)min((int64_t)kSortTile, (int64_t)n - tile_base);
   for (int k = t; k < valid; k += kSortThreads) {
     const uint32_t kk = s_keys[k];
-    const uint32_t d = (kk >> shift) & (kR - 1);
+    const uint32_t d = (kk >> shift) & (kRadix - 1);
     const uint32_t g = s_gbase[d] + (uint32_t)k - s_dstart[d];
     if (g < (uint32_t)n) {
       keys_out[g] = kk;
@@ -239,20 +214,19 @@ __global__ void k_bounds(const uint32_t* __restrict__ keys, int n, int count,
 
 }  // namespace
 
-void launch_digit_histogram(const uint32_t* keys, int n, int passes, int bits, uint32_t* hist,
+void launch_digit_histogram(const uint32_t* keys, int n, int passes, uint32_t* hist,
                             cudaStream_t stream) {
   if (n <= 0) return;
   int blocks = (n + 255) / 256;
   if (blocks > 148 * 8) blocks = 148 * 8;
-  k_digit_histogram<<<blocks, 256, 0, stream>>>(keys, n, passes, bits, hist);
+  k_digit_histogram<<<blocks, 256, 0, stream>>>(keys, n, passes, hist);
 }
 
-cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, int n, int passes, int bits,
+cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, int n, int passes,
                              const SortScratch& s, cudaStream_t stream, bool hist_ready,
                              bool vals_iota, bool copy_back, uint32_t** keys_res,
                              uint32_t** vals_res) {
   if (passes < 1 || passes > kMaxPasses) return cudaErrorInvalidValue;
-  if (bits != 8 && bits != 9) return cudaErrorInvalidValue;
   if (n < 0 || (uint64_t)n > kLbValue || vals == nullptr) return cudaErrorInvalidValue;
   cudaError_t e;
   if (n <= 1) {
@@ -266,16 +240,16 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, int n, int passes, 
   }
   const int tiles = sort_tiles(n);
   if (!hist_ready) {
-    e = cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * kMaxPasses * kHistStride, stream);
+    e = cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * kMaxPasses * kRadix, stream);
     if (e != cudaSuccess) return e;
-    launch_digit_histogram(keys, n, passes, bits, s.hist, stream);
+    launch_digit_histogram(keys, n, passes, s.hist, stream);
   }
-  const size_t radix = (size_t)1 << bits;
-  e = cudaMemsetAsync(s.lookback, 0, sizeof(uint32_t) * (size_t)passes * tiles * radix, stream);
+  e = cudaMemsetAsync(s.lookback, 0, sizeof(uint32_t) * (size_t)passes * tiles * kRadix,
+                      stream);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(s.counters, 0, sizeof(uint32_t) * kMaxPasses, stream);
   if (e != cudaSuccess) return e;
-  k_scan_digits<<<1, 256, 0, stream>>>(s.hist, passes, bits);
+  k_scan_digits<<<1, kRadix, 0, stream>>>(s.hist, passes);
   // Pass p reads the previous output and writes buffer set (p & 1):
   // set 0 = scratch alternates, set 1 = the caller's arrays.
   uint32_t* const bk[2] = {s.keys_alt, keys};
@@ -285,15 +259,9 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, int n, int passes, 
   for (int p = 0; p < passes; ++p) {
     uint32_t* kout = bk[p & 1];
     uint32_t* vout = bv[p & 1];
-    uint32_t* lb = s.lookback + (size_t)p * tiles * radix;
-    if (bits == 9)
-      k_onesweep<9><<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, p * bits,
-                                                         s.hist + p * kHistStride, lb,
-                                                         s.counters + p, s.err, kSpinLimit);
-    else
-      k_onesweep<8><<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, p * bits,
-                                                         s.hist + p * kHistStride, lb,
-                                                         s.counters + p, s.err, kSpinLimit);
+    k_onesweep<<<tiles, kSortThreads, 0, stream>>>(
+        kin, vin, kout, vout, n, p * kRadixBits, s.hist + p * kRadix,
+        s.lookback + (size_t)p * tiles * kRadix, s.counters + p, s.err, kSpinLimit);
     kin = kout;
     vin = vout;
   }
@@ -352,8 +320,8 @@ cudaError_t lookback_wait_probe(int spin_limit, uint32_t* err_bits) {
   if (e == cudaSuccess) e = cudaMemcpy(doff, offs, sizeof(offs), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(counter, &one, sizeof(one), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    k_onesweep<8><<<1, kSortThreads>>>(keys, vals, kout, vout, n, 0, doff, lookback, counter,
-                                       err, spin_limit);
+    k_onesweep<<<1, kSortThreads>>>(keys, vals, kout, vout, n, 0, doff, lookback, counter, err,
+                                    spin_limit);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaDeviceSynchronize();

@@ -1,9 +1,7 @@
 // radix_sort.cuh -- stable LSD radix sort of u32 keys with u32 values.
 //
 // Replaces thrust::sort_by_key (thrust_c.cu:86-91).  One "onesweep" kernel
-// per digit of 8 or 9 bits (the step's cell keys take the width that needs
-// the fewest passes: 26-bit keys sort in 3 passes of 9 bits, not 4 of 8;
-// SortByKey's 32-bit keys in 4 of 8): every tile of 4096 pairs ranks its keys stably inside the
+// per 8-bit digit: every tile of 4096 pairs ranks its keys stably inside the
 // tile (warp match + per-warp digit counters, in input order), publishes its
 // per-digit counts, resolves the per-digit prefix of all earlier tiles with a
 // decoupled look-back, stages the tile in shared memory in digit order and
@@ -17,10 +15,8 @@
 
 namespace sphpc {
 
-constexpr int kRadixBits = 8;             // digit width of SortByKey (32-bit keys)
+constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
-constexpr int kDigitBitsMax = 9;          // widest digit of the step's sort
-constexpr int kHistStride = 1 << kDigitBitsMax;  // per-pass histogram stride (512)
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;
@@ -36,69 +32,41 @@ constexpr int kSpinLimit = 1 << 22;     // bounded waits: ~0.1-1 s, then error
 struct SortScratch {
   uint32_t* keys_alt;     // n
   uint32_t* vals_alt;     // n
-  uint32_t* hist;         // kMaxPasses * kHistStride (counts, then exclusive offsets)
-  uint32_t* lookback;     // passes * tiles * 2^bits
+  uint32_t* hist;         // kMaxPasses * kRadix  (counts, then exclusive offsets)
+  uint32_t* lookback;     // kMaxPasses * tiles * kRadix
   uint32_t* counters;     // kMaxPasses tile counters
   uint32_t* err;          // error bits
 };
 
 inline int sort_tiles(int n) { return (n + kSortTile - 1) / kSortTile; }
 
-// Words of scratch excluding the two alternate buffers, for digits of up to
-// `bits` bits: histograms, tile counters, error word, look-back flags.
-inline size_t sort_aux_words(int n, int bits = kDigitBitsMax) {
-  return (size_t)kMaxPasses * kHistStride + kMaxPasses + 4 +
-         (size_t)kMaxPasses * sort_tiles(n) * ((size_t)1 << bits);
-}
-
-// Layout of that scratch: hist, counters, err, look-back flags.
-inline void sort_scratch_layout(uint32_t* aux, SortScratch* s) {
-  s->hist = aux;
-  s->counters = aux + (size_t)kMaxPasses * kHistStride;
-  s->err = s->counters + kMaxPasses;
-  s->lookback = s->counters + kMaxPasses + 4;
-}
-
-// Digit width and pass count for keys below 2^key_bits: the fewest passes,
-// 8-bit digits where that is as few.
-inline void sort_digits_for(int key_bits, int* passes, int* bits) {
-  int p8 = (key_bits + 7) / 8;
-  int p9 = (key_bits + 8) / 9;
-  if (p8 < 1) p8 = 1;
-  if (p9 < 1) p9 = 1;
-  if (p9 < p8) {
-    *passes = p9;
-    *bits = 9;
-  } else {
-    *passes = p8 > kMaxPasses ? kMaxPasses : p8;
-    *bits = 8;
-  }
+// Bytes of scratch excluding the two alternate buffers.
+inline size_t sort_aux_words(int n) {
+  return (size_t)kMaxPasses * kRadix + (size_t)kMaxPasses * sort_tiles(n) * kRadix +
+         kMaxPasses;
 }
 
 // Host: enqueue the whole sort on `stream`.  Sorts (keys, vals) by the low
-// bits*passes bits of the keys (bits 8 or 9).  With vals_iota the input values are taken to be
+// 8*passes bits of the keys.  With vals_iota the input values are taken to be
 // 0..n-1 and vals is only an output buffer.  If hist_ready is true,
 // scratch.hist already holds the digit counts of all passes (from a fused
 // producer).  An odd pass count leaves the result in the scratch alternates:
 // copy_back copies it into keys/vals, otherwise keys_res/vals_res say where
 // it is.
-cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, int n, int passes, int bits,
+cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, int n, int passes,
                              const SortScratch& s, cudaStream_t stream, bool hist_ready,
                              bool vals_iota, bool copy_back, uint32_t** keys_res,
                              uint32_t** vals_res);
 
-// Histogram of all `passes` digits of `bits` bits, accumulated into hist
-// (hist[p * kHistStride + digit], must be zeroed).
-void launch_digit_histogram(const uint32_t* keys, int n, int passes, int bits, uint32_t* hist,
+// Histogram of all `passes` digits, accumulated into hist (must be zeroed).
+void launch_digit_histogram(const uint32_t* keys, int n, int passes, uint32_t* hist,
                             cudaStream_t stream);
 
 // Device helper for fused producers: count the digits of one key into
-// shared-memory histograms s_hist[passes][kHistStride].
-__device__ __forceinline__ void count_key_digits(uint32_t* s_hist, uint32_t key, int passes,
-                                                 int bits) {
-  const uint32_t mask = (1u << bits) - 1u;
+// shared-memory histograms s_hist[passes][kRadix].
+__device__ __forceinline__ void count_key_digits(uint32_t* s_hist, uint32_t key, int passes) {
   for (int p = 0; p < passes; ++p)
-    atomicAdd(&s_hist[p * kHistStride + ((key >> (p * bits)) & mask)], 1u);
+    atomicAdd(&s_hist[p * kRadix + ((key >> (p * kRadixBits)) & (kRadix - 1))], 1u);
 }
 
 // Failure-detection check of the look-back wait: one onesweep CTA waits on a

@@ -66,7 +66,7 @@ class DeviceSim {
   bool grid_ready = false;
   int nx = 0, ny = 0, nz = 0;
   uint32_t C = 0;
-  int bx = 0, by = 0, passes = 1, digit_bits = 8;
+  int bx = 0, by = 0, passes = 1;
 
   // per-particle arrays, slot order
   PD *pd = nullptr, *pd_alt = nullptr;
@@ -189,9 +189,12 @@ class DeviceSim {
     SPHPC_RC(dalloc(&resid, 16));
     SPHPC_RC(dalloc(&sort.keys_alt, c));
     SPHPC_RC(dalloc(&sort.vals_alt, c));
-    const size_t aux = sort_aux_words(c);
+    const size_t aux = sort_aux_words(c) + 4;
     SPHPC_RC(dalloc(&sort_aux, aux));
-    sort_scratch_layout(sort_aux, &sort);
+    sort.hist = sort_aux;
+    sort.counters = sort_aux + (size_t)kMaxPasses * kRadix;
+    sort.err = sort_aux + (size_t)kMaxPasses * kRadix + kMaxPasses;
+    sort.lookback = sort_aux + (size_t)kMaxPasses * kRadix + kMaxPasses + 4;
     SPHPC_CK(cudaMemsetAsync(small, 0, 8 * sizeof(uint32_t), stream));
     SPHPC_CK(cudaMemsetAsync(sort_aux, 0, aux * sizeof(uint32_t), stream));
     SPHPC_CK(cudaMemsetAsync(pd, 0, sizeof(PD) * c, stream));
@@ -258,7 +261,8 @@ class DeviceSim {
     if (grid_ready && CC == C && nnx == nx && nny == ny && nnz == nz) return SPHPC_OK;
     dfree(cstart);
     nx = nnx; ny = nny; nz = nnz; C = CC; bx = bxx; by = byy;
-    sort_digits_for(bits_for(C - 1), &passes, &digit_bits);
+    passes = (bits_for(C - 1) + kRadixBits - 1) / kRadixBits;
+    if (passes > kMaxPasses) passes = kMaxPasses;
     SPHPC_RC(dalloc(&cstart, (size_t)C + 1));
     dfree(gaps);
     SPHPC_RC(dalloc(&gaps, (size_t)cap + 4 + C / 4096));
@@ -518,16 +522,16 @@ int DeviceSim::find_neighbors(const DevParams& P, bool predict, bool full, bool 
   if (!grid_ready) return set_error(SPHPC_ENOTREADY, "neighbour grid not initialised");
   {
     Scope sc(this, "hash");
-    SPHPC_CK(cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * kMaxPasses * kHistStride, stream));
-    launch_hash(P, pd, vel, ids, keys_by_id, loc_by_id, sort.hist, passes, digit_bits, predict,
-                err(), stream);
+    SPHPC_CK(cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * kMaxPasses * kRadix, stream));
+    launch_hash(P, pd, vel, ids, keys_by_id, loc_by_id, sort.hist, passes, predict, err(),
+                stream);
     launches += 1;
   }
   uint32_t *K = nullptr, *R = nullptr;
   {
     Scope sc(this, "radix_sort");
-    const cudaError_t e = radix_sort_pairs(keys_by_id, ids_spare, n, passes, digit_bits, sort,
-                                           stream, true, true, false, &K, &R);
+    const cudaError_t e = radix_sort_pairs(keys_by_id, ids_spare, n, passes, sort, stream, true,
+                                           true, false, &K, &R);
     if (e != cudaSuccess)
       return set_error(SPHPC_ECUDA, "radix sort: %s", cudaGetErrorString(e));
     launches += 1 + (unsigned)passes;
@@ -1594,9 +1598,8 @@ int sphpc_slab_unpack(struct Particles* particles, const void* recv_left, int co
                   (uint32_t)count_left, (uint32_t)count_right};
   // the new working set in gid order: sort (gid, record index)
   launch_slab_keys(parts, s->keys_by_id, s->stream);
-  const cudaError_t e = radix_sort_pairs(s->keys_by_id, s->loc_by_id, (int)m, kMaxPasses,
-                                         kRadixBits, s->sort, s->stream, false, true, true,
-                                         nullptr, nullptr);
+  const cudaError_t e = radix_sort_pairs(s->keys_by_id, s->loc_by_id, (int)m, kMaxPasses, s->sort,
+                                         s->stream, false, true, true, nullptr, nullptr);
   if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "sphpc_slab_unpack: %s", cudaGetErrorString(e));
   launch_slab_load(parts, s->loc_by_id, s->pd, s->vel, s->gid, s->owned, s->ids, s->stream);
   SPHPC_CK(cudaGetLastError());
@@ -1910,10 +1913,13 @@ static int seam_scratch(int count, SortScratch* out) {
     sc.cap = 0;
     SPHPC_RC(dalloc(&sc.s.keys_alt, (size_t)count));
     SPHPC_RC(dalloc(&sc.s.vals_alt, (size_t)count));
-    const size_t aux = sort_aux_words(count, kRadixBits);
+    const size_t aux = sort_aux_words(count) + 4;
     SPHPC_RC(dalloc(&sc.aux, aux));
     SPHPC_CK(cudaMemset(sc.aux, 0, aux * sizeof(uint32_t)));
-    sort_scratch_layout(sc.aux, &sc.s);
+    sc.s.hist = sc.aux;
+    sc.s.counters = sc.aux + (size_t)kMaxPasses * kRadix;
+    sc.s.err = sc.aux + (size_t)kMaxPasses * kRadix + kMaxPasses;
+    sc.s.lookback = sc.aux + (size_t)kMaxPasses * kRadix + kMaxPasses + 4;
     sc.cap = count;
   }
   *out = sc.s;
@@ -1929,8 +1935,8 @@ int SortByKey(unsigned int* const keys, unsigned int* const values, const int co
   SortScratch sc;
   SPHPC_RC(seam_scratch(count, &sc));
   cudaStream_t st = (cudaStream_t)cuda_stream;
-  const cudaError_t e = radix_sort_pairs(keys, values, count, kMaxPasses, kRadixBits, sc, st,
-                                         false, false, true, nullptr, nullptr);
+  const cudaError_t e = radix_sort_pairs(keys, values, count, kMaxPasses, sc, st, false, false,
+                                         true, nullptr, nullptr);
   if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "SortByKey: %s", cudaGetErrorString(e));
   // the scratch is shared by every caller: finish before releasing it
   SPHPC_CK(cudaStreamSynchronize(st));

@@ -26,8 +26,10 @@ constexpr int kNoAllocMaxPairs = 1 << 18;
 // radix_sort_pairs (about 2.4 MB).  Every GPU that loads the library holds
 // this array until the process exits.
 constexpr size_t kNoAllocWords =
-    2 * (size_t)kNoAllocMaxPairs + (size_t)kMaxPasses * kHistStride + kMaxPasses + 4 +
-    (size_t)kMaxPasses * ((kNoAllocMaxPairs + kSortTile - 1) / kSortTile) * kRadix;
+    2 * (size_t)kNoAllocMaxPairs + ((size_t)kMaxPasses * kRadix +
+                                    (size_t)kMaxPasses * ((kNoAllocMaxPairs + kSortTile - 1) /
+                                                          kSortTile) * kRadix +
+                                    kMaxPasses) + 8;
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
 
@@ -129,7 +131,11 @@ extern "C" int SortByKeyNoAlloc(unsigned int* const keys, unsigned int* const va
   SortScratch s;
   s.keys_alt = base;
   s.vals_alt = base + kNoAllocMaxPairs;
-  sort_scratch_layout(base + 2 * (size_t)kNoAllocMaxPairs, &s);
+  uint32_t* aux = base + 2 * (size_t)kNoAllocMaxPairs;
+  s.hist = aux;
+  s.counters = aux + (size_t)kMaxPasses * kRadix;
+  s.err = aux + (size_t)kMaxPasses * kRadix + kMaxPasses;
+  s.lookback = aux + (size_t)kMaxPasses * kRadix + kMaxPasses + 4;
   cudaStream_t st = (cudaStream_t)cuda_stream;
   // The array keeps the previous call's contents: the error word must start
   // at zero (histograms, look-back flags and tile counters are cleared by
@@ -137,8 +143,8 @@ extern "C" int SortByKeyNoAlloc(unsigned int* const keys, unsigned int* const va
   cudaError_t e = cudaMemsetAsync(s.err, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess)
     return set_error(SPHPC_ECUDA, "SortByKeyNoAlloc: %s", cudaGetErrorString(e));
-  e = radix_sort_pairs(keys, values, count, kMaxPasses, kRadixBits, s, st, false, false, true,
-                       nullptr, nullptr);
+  e = radix_sort_pairs(keys, values, count, kMaxPasses, s, st, false, false, true, nullptr,
+                       nullptr);
   if (e != cudaSuccess)
     return set_error(SPHPC_ECUDA, "SortByKeyNoAlloc: %s", cudaGetErrorString(e));
   uint32_t herr = 0;

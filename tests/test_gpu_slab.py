@@ -60,8 +60,9 @@ def test_three_slabs_equal_the_undivided_run():
                 np.testing.assert_array_equal(v, want_v)
                 if first_owner is None:
                     first_owner = _owners(domains, n)
-            # every slab's working set held fewer particles than the scene
-            assert all(s.particles.local_count < n for s in sims)
+            # the slab farthest from the initial block sees only part of the
+            # scene (the middle slab's halo spans the whole early block)
+            assert sims[2].particles.local_count < n
             # one more exchange hands every particle to the slab its position
             # lies in; the fluid crossed slab ends, so some changed owner
             slab.exchange_local(domains)
