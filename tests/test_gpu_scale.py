@@ -83,11 +83,28 @@ def _device_stage(sim, st0):
     return {"density": sim.host("density").copy(), "lambda": sim.host("lambda").copy()}
 
 
-def _check_stage(name, got, want, mask=None):
+def _check_stage(name, got, want, rho0, mask=None):
+    """Density within 1e-5 relative.  Lambda within 1e-4 relative plus 1e-5 of
+    its scale plus what one FP32 ulp of the density moves it by: lambda =
+    -C / D with C = max(rho / rho0 - 1, 0), so an FP32 density resolves C
+    only to e = 2^-23 rho / rho0, and lambda to 4 e / D = 4 e |lambda| / C
+    (at most 4 |lambda| where C is below e): a barely compressed particle
+    at the free surface has a small C and a small D."""
     m = slice(None) if mask is None else mask
     assert_close(got["density"][m], want["density"][m], 1e-5, 0.0, what=f"{name}:density")
-    assert_close(got["lambda"][m], want["lambda"][m], 1e-4, 1e-5, what=f"{name}:lambda")
-    return {f: err_stats(got[f][m], want[f][m]) for f in ("density", "lambda")}
+    lam_w = want["lambda"][m]
+    rho_w = want["density"][m]
+    C = np.maximum(rho_w / rho0 - 1.0, 0.0)
+    e = 2.0 ** -23 * rho_w / rho0
+    resolution = 4.0 * e * np.abs(lam_w) / np.maximum(C, e)
+    err = np.abs(got["lambda"][m] - lam_w)
+    tol = 1e-4 * np.abs(lam_w) + 1e-5 * np.max(np.abs(lam_w)) + resolution
+    rec = {f: err_stats(got[f][m], want[f][m]) for f in ("density", "lambda")}
+    rec["lambda"]["beyond_fixed_tolerance"] = int(np.sum(err > tol - resolution))
+    bad = err > tol
+    assert not np.any(bad), (name, "lambda", int(bad.sum()),
+                             float(np.max((err - tol)[bad]) / np.max(np.abs(lam_w))))
+    return rec
 
 
 def _check_step(name, got, want, mask=None, sens=None):
@@ -128,11 +145,13 @@ def _check_step(name, got, want, mask=None, sens=None):
     return rec
 
 
-def test_dam_break_1m_whole_set_matches_oracle():
+@pytest.mark.parametrize("steps_before", [60, 250])
+def test_dam_break_1m_whole_set_matches_oracle(steps_before):
     """1,048,576 particles (dam_break_1m: 4 iterations, XSPH, vorticity
-    confinement), 60 steps into the collapse, every particle compared."""
+    confinement), 60 and 250 steps into the collapse, every particle
+    compared."""
     with Simulation("dam_break_1m") as sim:
-        sim.step(60)
+        sim.step(steps_before)
         st0 = sim.fetch()
         sim.step(1)
         sim.fetch_fields(list(POS + VEL) + ["density"])
@@ -144,9 +163,9 @@ def test_dam_break_1m_whole_set_matches_oracle():
         rec = {"step": _check_step("1m:step", got, want)}
         assert not any(rec["step"][f]["failed"] for f in VEL + ("density",)), rec["step"]
         got_stage = _device_stage(sim, st0)
-        rec["stage"] = _check_stage("1m:stage", got_stage, want_stage)
+        rec["stage"] = _check_stage("1m:stage", got_stage, want_stage, sim.particles.rest_density)
         assert sim.device_errors() == 0
-        parity_record("dam_break_1m_whole_set", {"n": sim.n, "steps_before": 60, **rec})
+        parity_record("dam_break_1m_whole_set", {"n": sim.n, "steps_before": steps_before, **rec})
 
 
 def _hops(o):
@@ -214,7 +233,7 @@ def test_full_16m_blocks_match_oracle():
             rec = {"box_particles": int(idx.size), "compared_step": int(m_step.sum()),
                    "compared_stage": int(m_stage.sum()),
                    "step": _check_step(f"16m:{tag}:step", g, want, m_step, sens),
-                   "stage": _check_stage(f"16m:{tag}:stage", gs, want_stage, m_stage)}
+                   "stage": _check_stage(f"16m:{tag}:stage", gs, want_stage, rho0, m_stage)}
             records[tag] = rec
         parity_record("full_16m_blocks", {"n": sim.n, "steps_before": 200, **records})
         failed = {(t, f): r["step"][f]["failed"] for t, r in records.items()
