@@ -55,6 +55,12 @@ class SlabDomain:
         if solver.adaptive or solver.warm_start:
             sim.set_solver(adaptive=0, warm_start=0)
         self.width = halo_width(sim)
+        # halo copies come from the two neighbours only: a slab between two
+        # neighbours must hold every particle its neighbours' halos need
+        if self.has_left and self.has_right and self.node_end - self.node_start < self.width:
+            raise ValueError(f"slab [{self.node_start}, {self.node_end}) is narrower than the "
+                             f"halo width {self.width:.3g} (its neighbours would need particles "
+                             f"two slabs away)")
         call("sphpc_slab_init", C.byref(sim.particles), 0, self.node_start, self.node_end,
              int(self.has_left), int(self.has_right))
         cap = send_capacity or max(1024, sim.particles.max_local // 2)

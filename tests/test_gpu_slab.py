@@ -4,7 +4,8 @@ records handed over by device copies, against the undivided run.  Each slab
 works on its own particles plus its neighbours' within the halo width, so
 its own particles' positions and velocities must equal the undivided run's
 bit for bit while the fluid flows across the slab ends (particles change
-owner); every particle is owned by exactly one slab."""
+owner, over 200 steps); every particle is owned by exactly one slab.  A slab
+narrower than the halo between two neighbours is refused."""
 import numpy as np
 import pytest
 
@@ -13,7 +14,8 @@ from sphpc_b200.simulation import Simulation
 
 pytestmark = pytest.mark.gpu
 
-BOUNDS = [(0.0, 16.0), (16.0, 40.0), (40.0, 96.0)]
+# the middle slab (both neighbours) is wider than the halo (21.6 here)
+BOUNDS = [(0.0, 16.0), (16.0, 38.0), (38.0, 96.0)]
 
 
 def _owned_union(domains):
@@ -39,7 +41,7 @@ def _owners(domains, n):
 
 
 def test_three_slabs_equal_the_undivided_run():
-    steps_per_check = (1, 9, 30)
+    steps_per_check = (1, 9, 190)
     with Simulation("dam_break_32k") as whole:
         n = whole.n
         sims = [Simulation("dam_break_32k") for _ in BOUNDS]
@@ -76,3 +78,9 @@ def test_three_slabs_equal_the_undivided_run():
         finally:
             for s in sims:
                 s.close()
+
+
+def test_slab_narrower_than_the_halo_is_refused():
+    with Simulation("dam_break_32k") as sim:
+        with pytest.raises(ValueError):
+            slab.SlabDomain(sim, 16.0, 30.0, True, True)
