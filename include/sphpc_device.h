@@ -28,12 +28,11 @@ int SortByKey(unsigned int *const keys, unsigned int *const values, const int co
  * so count is limited to 262,144 pairs (larger counts return SPHPC_EINVAL).
  * It calls no cudaMalloc or cudaFree.  The first call on a device, and the
  * first after the device's context has been replaced (cudaDeviceReset),
- * looks up the array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls on a device share the one
- * array: calls that overlap on the GPU (from several host threads or
- * streams) race and must be serialised by the caller.  Each call waits on
- * the host until its sort has finished on cuda_stream (it reads back the
- * sort's error word). */
+ * looks up the array's device address (cudaGetSymbolAddress).  All calls on
+ * a device share the one array: calls that overlap on the GPU (from several
+ * host threads or streams) race and must be serialised by the caller.  Each
+ * call waits on the host until its sort has finished on cuda_stream (it
+ * reads back the sort's error word). */
 int SortByKeyNoAlloc(unsigned int *const keys, unsigned int *const values, const int count,
                      const void *const cuda_stream);
 

@@ -304,27 +304,14 @@ __device__ __forceinline__ bool staged_exact(const DevParams& P, const PD* __res
   return r2 < P.h2d;
 }
 
-// Appends the candidates of slots [ja, jb) of row r (starting at slot rb):
-// the entry of slot j is (r << kRowBits) | (j - rb), carried incrementally;
-// `sa` is the shared-memory address of the thread's next staging slot
-// (entry t at stg[t * kStagedBlock], kRowStep bytes apart) and moves on by
-// one row of the staging area on a hit, so the count is (sa - base) /
-// kRowStep; `full` is the address of entry 60 (the cap), never written.
-constexpr uint32_t kRowStep = kStagedBlock * sizeof(uint16_t);
-
-__device__ __forceinline__ void st_shared_u16(uint32_t addr, uint32_t v) {
-  asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"((unsigned short)v) : "memory");
-}
-
+// Appends the candidates of slots [ja, jb) of row r (starting at slot rb).
 __device__ __forceinline__ void staged_range(const DevParams& P, const PD* __restrict__ pd,
                                              const float4* __restrict__ xsa, float px, float py,
                                              float pz, int p, int r, int rb, int ja, int jb,
-                                             uint32_t& sa, uint32_t full) {
-  uint32_t e = ((uint32_t)r << kRowBits) | (uint32_t)(ja - rb);
+                                             uint16_t* __restrict__ stg, int& cnt) {
+  const uint32_t tag = (uint32_t)r << kRowBits;
   int j = ja;
-  // batches of four while four more entries fit below the cap
-  const uint32_t batch_end = full - 3 * kRowStep;
-  for (; j + 4 <= jb && sa < batch_end; j += 4, e += 4) {
+  for (; j + 4 <= jb && cnt <= kMaxNeighbors - 4; j += 4) {
     float4 q[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) q[u] = __ldg(xsa + j + u);
@@ -334,18 +321,18 @@ __device__ __forceinline__ void staged_range(const DevParams& P, const PD* __res
       const float r2 = fx * fx + fy * fy + fz * fz;
       bool hit = r2 <= P.bld_h2hi;
       if (hit && r2 >= P.bld_h2lo) hit = staged_exact(P, pd, p, j + u);
-      st_shared_u16(sa, e + u);
-      sa += hit ? kRowStep : 0u;
+      stg[cnt * kStagedBlock] = (uint16_t)(tag | (uint32_t)(j + u - rb));
+      cnt += hit ? 1 : 0;
     }
   }
-  for (; j < jb && sa < full; ++j, ++e) {
+  for (; j < jb && cnt < kMaxNeighbors; ++j) {
     const float4 q = __ldg(xsa + j);
     const float fx = px - q.x, fy = py - q.y, fz = pz - q.z;
     const float r2 = fx * fx + fy * fy + fz * fz;
     bool hit = r2 <= P.bld_h2hi;
     if (hit && r2 >= P.bld_h2lo) hit = staged_exact(P, pd, p, j);
-    st_shared_u16(sa, e);
-    sa += hit ? kRowStep : 0u;
+    stg[cnt * kStagedBlock] = (uint16_t)(tag | (uint32_t)(j - rb));
+    cnt += hit ? 1 : 0;
   }
 }
 
@@ -390,23 +377,19 @@ __global__ void __launch_bounds__(kStagedBlock, 9)
   int count = 0;
   if (regular) {
     const float4 xf = __ldg(xsa + p);
-    const uint32_t base = (uint32_t)__cvta_generic_to_shared(stg);
-    const uint32_t full = base + kMaxNeighbors * kRowStep;
-    uint32_t sa = base;
-    for (int r = 0; r < 9 && sa < full; ++r) {
+    for (int r = 0; r < 9 && count < kMaxNeighbors; ++r) {
       const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
       if ((unsigned)z >= (unsigned)P.nz || (unsigned)y >= (unsigned)P.ny) continue;
       const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
       const int b = rowb[r * kStagedBlock];
       const int e = (int)__ldg(V.cstart + rk + xhi + 1);
       if (r == 4) {
-        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, b, p, sa, full);
-        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, p + 1, e, sa, full);
+        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, b, p, stg, count);
+        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, p + 1, e, stg, count);
       } else {
-        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, b, e, sa, full);
+        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, b, e, stg, count);
       }
     }
-    count = (int)((sa - base) / kRowStep);
     for (int t = 0; t < count; ++t) {
       const uint32_t en = stg[t * kStagedBlock];
       nbr[(size_t)t * stride + p] =

@@ -59,10 +59,12 @@ __global__ void __launch_bounds__(256) k_scan_digits(uint32_t* __restrict__ hist
 
 // One digit pass.  vals_in == nullptr means the values are the input
 // indices (iota), which is how SortHash calls SortByKey (neighbors.c:123).
-// Three blocks per SM (80 registers, no spills) rather than the two that
-// the compiler's own choice of 128 registers leaves room for: the passes
-// wait on loads and on the look-back, so resident warps are what hides it.
-__global__ void __launch_bounds__(kSortThreads, 3)
+// Five blocks per SM (48 registers, no spills; 43 KB of shared memory
+// each) rather than the two that the compiler's own choice of 128
+// registers leaves room for: the passes wait on loads and on the
+// look-back, so resident warps are what hides it.  The values are loaded
+// only when the tile is staged, which is what lets the ranking fit.
+__global__ void __launch_bounds__(kSortThreads, 5)
     k_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n,
                int shift, const uint32_t* __restrict__ digit_offset,
@@ -85,17 +87,13 @@ __global__ void __launch_bounds__(kSortThreads, 3)
   const int64_t tile_base = (int64_t)tile * kSortTile;
   const int64_t wbase = tile_base + (int64_t)warp * 32 * kSortItems;
 
-  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+  // the values are loaded only when the tile is staged, so that the ranking
+  // holds two arrays of registers, not three
+  uint32_t key[kSortItems], rank[kSortItems];
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
     const int64_t idx = wbase + i * 32 + lane;
-    if (idx < n) {
-      key[i] = __ldg(keys_in + idx);
-      val[i] = vals_in ? __ldg(vals_in + idx) : (uint32_t)idx;
-    } else {
-      key[i] = 0xffffffffu;
-      val[i] = 0;
-    }
+    key[i] = idx < n ? __ldg(keys_in + idx) : 0xffffffffu;
   }
   const uint32_t lt = lanemask_lt();
 #pragma unroll
@@ -134,23 +132,36 @@ __global__ void __launch_bounds__(kSortThreads, 3)
     }
     uint32_t excl = 0;
     if (tile > 0) {
+      // kLookBack predecessors' flags per poll, consumed in order down to the
+      // first inclusive one; a poll that finds the nearest one not yet
+      // published waits and polls again from there
       int64_t pt = (int64_t)tile - 1;
-      while (pt >= 0) {
-        const uint32_t* f = lookback + (size_t)pt * kRadix + d;
-        uint32_t v = ld_volatile(f);
-        int spins = 0;
-        while ((v & (kLbAgg | kLbInc)) == 0) {
+      int spins = 0;
+      for (;;) {
+        uint32_t v[kLookBack];
+#pragma unroll
+        for (int k = 0; k < kLookBack; ++k)
+          v[k] = pt - k >= 0 ? ld_volatile(lookback + (size_t)(pt - k) * kRadix + d) : 0u;
+        int k = 0;
+        bool done = false;
+#pragma unroll
+        for (; k < kLookBack; ++k) {
+          if ((v[k] & (kLbAgg | kLbInc)) == 0) break;
+          excl += v[k] & kLbValue;
+          if (v[k] & kLbInc) {
+            done = true;
+            break;
+          }
+        }
+        if (done) break;
+        pt -= k;
+        if (k == 0) {
           if (++spins > spin_limit) {
             atomicOr(err, 2u);  // kErrSortSpin
-            v = kLbInc;
             break;
           }
           __nanosleep(32);
-          v = ld_volatile(f);
         }
-        excl += v & kLbValue;
-        if (v & kLbInc) break;
-        --pt;
       }
       st_volatile(my, kLbInc | (excl + cnt));
     }
@@ -178,7 +189,7 @@ __global__ void __launch_bounds__(kSortThreads, 3)
       const uint32_t d = (key[i] >> shift) & (kRadix - 1);
       const uint32_t lp = s_dstart[d] + s_whist[warp][d] + rank[i];
       s_keys[lp] = key[i];
-      s_vals[lp] = val[i];
+      s_vals[lp] = vals_in ? __ldg(vals_in + idx) : (uint32_t)idx;
     }
   }
   __syncthreads();

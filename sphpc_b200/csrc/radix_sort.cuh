@@ -27,6 +27,7 @@ constexpr uint32_t kLbAgg = 1u << 30;   // look-back: tile aggregate available
 constexpr uint32_t kLbInc = 2u << 30;   // look-back: inclusive prefix available
 constexpr uint32_t kLbValue = (1u << 30) - 1u;
 constexpr int kSpinLimit = 1 << 22;     // bounded waits: ~0.1-1 s, then error
+constexpr int kLookBack = 4;            // look-back flags read per poll
 
 // Scratch needed by one sort of n pairs with `passes` digit passes.
 struct SortScratch {
