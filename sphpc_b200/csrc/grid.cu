@@ -6,6 +6,48 @@ namespace sphpc {
 
 namespace {
 
+// x* as absolute FP32 for the neighbour build's candidate test, in pair
+// blocks: slots 2b and 2b+1 share the 32 bytes {x0, x1, y0, y1, z0, z1, 0,
+// 0} at float4 index 2b, so that the coordinates of a slot pair load as the
+// 64-bit operands of the packed FP32x2 arithmetic of sm_100.
+__device__ __forceinline__ void xsa_store(float4* xsa, int j, float x, float y, float z) {
+  float* f = reinterpret_cast<float*>(xsa + (j & ~1)) + (j & 1);
+  f[0] = x;
+  f[2] = y;
+  f[4] = z;
+  f[6] = 0.0f;
+}
+
+__device__ __forceinline__ float4 xsa_load(const float4* __restrict__ xsa, int j) {
+  const float* f = reinterpret_cast<const float*>(xsa + (j & ~1)) + (j & 1);
+  return make_float4(__ldg(f), __ldg(f + 2), __ldg(f + 4), 0.0f);
+}
+
+// Packed FP32x2 (sm_100): two independent IEEE single-precision operations
+// per instruction, each rounded to nearest as its scalar form.
+__device__ __forceinline__ uint64_t f2_dup(float a) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ float f2_lo(uint64_t a) { return __uint_as_float((uint32_t)a); }
+__device__ __forceinline__ float f2_hi(uint64_t a) { return __uint_as_float((uint32_t)(a >> 32)); }
+
 // Canonical predicted position of one particle.  predict: ApplyGravity then
 // PredictPositions (particles.c:516-527, 766-782) evaluated in FP64 exactly
 // as the reference does, then the box clamp (particles.c:842-867); the
@@ -109,7 +151,7 @@ __global__ void __launch_bounds__(kBlock)
   cz = min(cz, P.nz - 1);
   d.w = predict ? 0.0f : dg.w;
   st_pd(pd_out, j, x, d);
-  xsa[j] = make_float4((float)xs, (float)ys, (float)zs, 0.0f);
+  xsa_store(xsa, j, (float)xs, (float)ys, (float)zs);
   nr_out[j] = make_nr(P, xs, ys, zs, d.w);
   cellp[j] = pack_cell(P, cx, cy, cz);
   if (move_vel) {
@@ -234,7 +276,7 @@ __device__ __forceinline__ bool exact_neighbor(const BuildCtx& c, const PD* __re
 
 __device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const PD* __restrict__ pd,
                                             const float4* __restrict__ xsa, int j) {
-  const float4 q = __ldg(xsa + j);
+  const float4 q = xsa_load(xsa, j);
   const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
   const float r2f = fx * fx + fy * fy + fz * fz;
   if (r2f < c.h2lo) return true;
@@ -304,36 +346,80 @@ __device__ __forceinline__ bool staged_exact(const DevParams& P, const PD* __res
   return r2 < P.h2d;
 }
 
-// Appends the candidates of slots [ja, jb) of row r (starting at slot rb).
+// Test and append of one candidate slot j with FP32 r^2 = r2 (the exact
+// FP64 test decides inside the band): the entry is stored at the thread's
+// next staging slot and the count advances on a hit.
+__device__ __forceinline__ void staged_one(const DevParams& P, const PD* __restrict__ pd, int p,
+                                           int j, float r2, uint32_t entry,
+                                           uint16_t* __restrict__ stg, int& cnt) {
+  bool hit = r2 <= P.bld_h2hi;
+  if (hit && r2 >= P.bld_h2lo) hit = staged_exact(P, pd, p, j);
+  stg[cnt * kStagedBlock] = (uint16_t)entry;
+  cnt += hit ? 1 : 0;
+}
+
+// r^2 of one slot from the FP32 positions (the ragged ends of a range).
+__device__ __forceinline__ float staged_r2(const float4* __restrict__ xsa, int j, float px,
+                                           float py, float pz) {
+  const float4 q = xsa_load(xsa, j);
+  const float fx = px - q.x, fy = py - q.y, fz = pz - q.z;
+  return fx * fx + fy * fy + fz * fz;
+}
+
+// Appends the candidates of slots [ja, jb) of row r (starting at slot rb),
+// entries (r << kRowBits) | (j - rb).  The slots of an even-aligned pair are
+// tested together with packed FP32x2 arithmetic (each lane rounds as the
+// scalar form would: x_p - x_q, then (dx^2 + dy^2) + dz^2 by fused
+// multiply-adds), two pairs per batch while four more entries fit below the
+// cap; an odd first or last slot is tested alone.
 __device__ __forceinline__ void staged_range(const DevParams& P, const PD* __restrict__ pd,
-                                             const float4* __restrict__ xsa, float px, float py,
+                                             const float4* __restrict__ xsa, uint64_t pxx,
+                                             uint64_t pyy, uint64_t pzz, float px, float py,
                                              float pz, int p, int r, int rb, int ja, int jb,
                                              uint16_t* __restrict__ stg, int& cnt) {
   const uint32_t tag = (uint32_t)r << kRowBits;
   int j = ja;
+  if ((j & 1) && j < jb && cnt < kMaxNeighbors) {
+    staged_one(P, pd, p, j, staged_r2(xsa, j, px, py, pz), tag | (uint32_t)(j - rb), stg, cnt);
+    ++j;
+  }
+  const ulonglong2* blk = reinterpret_cast<const ulonglong2*>(xsa);
   for (; j + 4 <= jb && cnt <= kMaxNeighbors - 4; j += 4) {
-    float4 q[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) q[u] = __ldg(xsa + j + u);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const float fx = px - q[u].x, fy = py - q[u].y, fz = pz - q[u].z;
-      const float r2 = fx * fx + fy * fy + fz * fz;
-      bool hit = r2 <= P.bld_h2hi;
-      if (hit && r2 >= P.bld_h2lo) hit = staged_exact(P, pd, p, j + u);
-      stg[cnt * kStagedBlock] = (uint16_t)(tag | (uint32_t)(j + u - rb));
-      cnt += hit ? 1 : 0;
-    }
+    // pair blocks of slots j, j+1 and j+2, j+3: {xx, yy} and {zz, -}
+    const ulonglong2 a0 = __ldg(blk + j), b0 = __ldg(blk + j + 1);
+    const ulonglong2 a1 = __ldg(blk + j + 2), b1 = __ldg(blk + j + 3);
+    uint64_t d = f2_sub(pxx, a0.x);
+    uint64_t s0 = f2_mul(d, d);
+    d = f2_sub(pyy, a0.y);
+    s0 = f2_fma(d, d, s0);
+    d = f2_sub(pzz, b0.x);
+    s0 = f2_fma(d, d, s0);
+    d = f2_sub(pxx, a1.x);
+    uint64_t s1 = f2_mul(d, d);
+    d = f2_sub(pyy, a1.y);
+    s1 = f2_fma(d, d, s1);
+    d = f2_sub(pzz, b1.x);
+    s1 = f2_fma(d, d, s1);
+    const uint32_t e = tag | (uint32_t)(j - rb);
+    staged_one(P, pd, p, j, f2_lo(s0), e, stg, cnt);
+    staged_one(P, pd, p, j + 1, f2_hi(s0), e + 1, stg, cnt);
+    staged_one(P, pd, p, j + 2, f2_lo(s1), e + 2, stg, cnt);
+    staged_one(P, pd, p, j + 3, f2_hi(s1), e + 3, stg, cnt);
   }
-  for (; j < jb && cnt < kMaxNeighbors; ++j) {
-    const float4 q = __ldg(xsa + j);
-    const float fx = px - q.x, fy = py - q.y, fz = pz - q.z;
-    const float r2 = fx * fx + fy * fy + fz * fz;
-    bool hit = r2 <= P.bld_h2hi;
-    if (hit && r2 >= P.bld_h2lo) hit = staged_exact(P, pd, p, j);
-    stg[cnt * kStagedBlock] = (uint16_t)(tag | (uint32_t)(j - rb));
-    cnt += hit ? 1 : 0;
+  for (; j + 2 <= jb && cnt <= kMaxNeighbors - 2; j += 2) {
+    const ulonglong2 a0 = __ldg(blk + j), b0 = __ldg(blk + j + 1);
+    uint64_t d = f2_sub(pxx, a0.x);
+    uint64_t s0 = f2_mul(d, d);
+    d = f2_sub(pyy, a0.y);
+    s0 = f2_fma(d, d, s0);
+    d = f2_sub(pzz, b0.x);
+    s0 = f2_fma(d, d, s0);
+    const uint32_t e = tag | (uint32_t)(j - rb);
+    staged_one(P, pd, p, j, f2_lo(s0), e, stg, cnt);
+    staged_one(P, pd, p, j + 1, f2_hi(s0), e + 1, stg, cnt);
   }
+  for (; j < jb && cnt < kMaxNeighbors; ++j)
+    staged_one(P, pd, p, j, staged_r2(xsa, j, px, py, pz), tag | (uint32_t)(j - rb), stg, cnt);
 }
 
 // 9 blocks of 128 threads per SM: 56 registers, no spills (a tighter cap
@@ -376,7 +462,8 @@ __global__ void __launch_bounds__(kStagedBlock, 9)
   }
   int count = 0;
   if (regular) {
-    const float4 xf = __ldg(xsa + p);
+    const float4 xf = xsa_load(xsa, p);
+    const uint64_t pxx = f2_dup(xf.x), pyy = f2_dup(xf.y), pzz = f2_dup(xf.z);
     for (int r = 0; r < 9 && count < kMaxNeighbors; ++r) {
       const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
       if ((unsigned)z >= (unsigned)P.nz || (unsigned)y >= (unsigned)P.ny) continue;
@@ -384,10 +471,10 @@ __global__ void __launch_bounds__(kStagedBlock, 9)
       const int b = rowb[r * kStagedBlock];
       const int e = (int)__ldg(V.cstart + rk + xhi + 1);
       if (r == 4) {
-        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, b, p, stg, count);
-        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, p + 1, e, stg, count);
+        staged_range(P, pd, xsa, pxx, pyy, pzz, xf.x, xf.y, xf.z, p, r, b, b, p, stg, count);
+        staged_range(P, pd, xsa, pxx, pyy, pzz, xf.x, xf.y, xf.z, p, r, b, p + 1, e, stg, count);
       } else {
-        staged_range(P, pd, xsa, xf.x, xf.y, xf.z, p, r, b, b, e, stg, count);
+        staged_range(P, pd, xsa, pxx, pyy, pzz, xf.x, xf.y, xf.z, p, r, b, b, e, stg, count);
       }
     }
     for (int t = 0; t < count; ++t) {
@@ -396,7 +483,7 @@ __global__ void __launch_bounds__(kStagedBlock, 9)
           (uint32_t)(rowb[(en >> kRowBits) * kStagedBlock] + (int)(en & kRowMax));
     }
   } else {
-    c.xf = __ldg(xsa + p);
+    c.xf = xsa_load(xsa, p);
     c.h2lo = P.bld_h2lo;
     c.h2hi = P.bld_h2hi;
     c.h2d = P.h2d;

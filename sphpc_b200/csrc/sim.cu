@@ -183,7 +183,7 @@ class DeviceSim {
     SPHPC_RC(dalloc(&keys_by_id, c)); SPHPC_RC(dalloc(&loc_by_id, c));
     SPHPC_RC(dalloc(&cellp, c)); SPHPC_RC(dalloc(&ncount, c));
     SPHPC_RC(dalloc(&nbr, (size_t)kMaxNeighbors * c));
-    SPHPC_RC(dalloc(&xsa, c));
+    SPHPC_RC(dalloc(&xsa, (size_t)c + 2));  // pair blocks: 32 bytes per slot pair
     SPHPC_CK(cudaMemsetAsync(ncount, 0, c, stream));
     SPHPC_RC(dalloc(&small, 8));
     SPHPC_RC(dalloc(&resid, 16));

@@ -13,7 +13,9 @@
 //                    of two records is exact for any box) and a payload (w:
 //                    lambda after a density/lambda pass, the density after
 //                    a position pass).  Neighbour sums gather only these.
-//   xsa[n]   float4  x* as absolute FP32 (neighbour-build candidate test)
+//   xsa[n]   float4  x* as absolute FP32 (neighbour-build candidate test),
+//                    in pair blocks: slots 2b, 2b+1 share {x0, x1, y0, y1},
+//                    {z0, z1, 0, 0} at float4 index 2b
 //   vel[n]   float4  v
 //   ids[n]   u32     original particle index of each slot
 //   cellp[n] u32     packed grid cell (cx | cy<<bx | cz<<(bx+by)) of x* at
