@@ -23,30 +23,15 @@ __device__ __forceinline__ float4 xsa_load(const float4* __restrict__ xsa, int j
   return make_float4(__ldg(f), __ldg(f + 2), __ldg(f + 4), 0.0f);
 }
 
-// Packed FP32x2 (sm_100): two independent IEEE single-precision operations
-// per instruction, each rounded to nearest as its scalar form.
-__device__ __forceinline__ uint64_t f2_dup(float a) {
-  uint64_t r;
-  asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
-  return r;
+// The pair block of even slot j as three 64-bit pairs {x_j, x_j+1}, {y..},
+// {z..}: one 256-bit read-only load (sm_100).
+__device__ __forceinline__ void ld_pair(const float4* __restrict__ xsa, int j, uint64_t& xx,
+                                        uint64_t& yy, uint64_t& zz) {
+  asm("{\n\t.reg .b64 pad;\n\t"
+      "ld.global.nc.v4.u64 {%0,%1,%2,pad}, [%3];\n\t}"
+      : "=l"(xx), "=l"(yy), "=l"(zz)
+      : "l"(xsa + j));
 }
-__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
-  uint64_t r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
-  uint64_t r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
-  uint64_t r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-  return r;
-}
-__device__ __forceinline__ float f2_lo(uint64_t a) { return __uint_as_float((uint32_t)a); }
-__device__ __forceinline__ float f2_hi(uint64_t a) { return __uint_as_float((uint32_t)(a >> 32)); }
 
 // Canonical predicted position of one particle.  predict: ApplyGravity then
 // PredictPositions (particles.c:516-527, 766-782) evaluated in FP64 exactly
@@ -383,22 +368,22 @@ __device__ __forceinline__ void staged_range(const DevParams& P, const PD* __res
     staged_one(P, pd, p, j, staged_r2(xsa, j, px, py, pz), tag | (uint32_t)(j - rb), stg, cnt);
     ++j;
   }
-  const ulonglong2* blk = reinterpret_cast<const ulonglong2*>(xsa);
   for (; j + 4 <= jb && cnt <= kMaxNeighbors - 4; j += 4) {
-    // pair blocks of slots j, j+1 and j+2, j+3: {xx, yy} and {zz, -}
-    const ulonglong2 a0 = __ldg(blk + j), b0 = __ldg(blk + j + 1);
-    const ulonglong2 a1 = __ldg(blk + j + 2), b1 = __ldg(blk + j + 3);
-    uint64_t d = f2_sub(pxx, a0.x);
+    // pair blocks of slots j, j+1 and j+2, j+3
+    uint64_t x0, y0, z0, x1, y1, z1;
+    ld_pair(xsa, j, x0, y0, z0);
+    ld_pair(xsa, j + 2, x1, y1, z1);
+    uint64_t d = f2_sub(pxx, x0);
     uint64_t s0 = f2_mul(d, d);
-    d = f2_sub(pyy, a0.y);
+    d = f2_sub(pyy, y0);
     s0 = f2_fma(d, d, s0);
-    d = f2_sub(pzz, b0.x);
+    d = f2_sub(pzz, z0);
     s0 = f2_fma(d, d, s0);
-    d = f2_sub(pxx, a1.x);
+    d = f2_sub(pxx, x1);
     uint64_t s1 = f2_mul(d, d);
-    d = f2_sub(pyy, a1.y);
+    d = f2_sub(pyy, y1);
     s1 = f2_fma(d, d, s1);
-    d = f2_sub(pzz, b1.x);
+    d = f2_sub(pzz, z1);
     s1 = f2_fma(d, d, s1);
     const uint32_t e = tag | (uint32_t)(j - rb);
     staged_one(P, pd, p, j, f2_lo(s0), e, stg, cnt);
@@ -407,12 +392,13 @@ __device__ __forceinline__ void staged_range(const DevParams& P, const PD* __res
     staged_one(P, pd, p, j + 3, f2_hi(s1), e + 3, stg, cnt);
   }
   for (; j + 2 <= jb && cnt <= kMaxNeighbors - 2; j += 2) {
-    const ulonglong2 a0 = __ldg(blk + j), b0 = __ldg(blk + j + 1);
-    uint64_t d = f2_sub(pxx, a0.x);
+    uint64_t x0, y0, z0;
+    ld_pair(xsa, j, x0, y0, z0);
+    uint64_t d = f2_sub(pxx, x0);
     uint64_t s0 = f2_mul(d, d);
-    d = f2_sub(pyy, a0.y);
+    d = f2_sub(pyy, y0);
     s0 = f2_fma(d, d, s0);
-    d = f2_sub(pzz, b0.x);
+    d = f2_sub(pzz, z0);
     s0 = f2_fma(d, d, s0);
     const uint32_t e = tag | (uint32_t)(j - rb);
     staged_one(P, pd, p, j, f2_lo(s0), e, stg, cnt);

@@ -46,6 +46,30 @@ struct __align__(32) PD {
   float4 d;
 };
 
+// Packed FP32x2 (sm_100): two independent IEEE single-precision operations
+// per instruction, each rounded to nearest as its scalar form.
+__device__ __forceinline__ uint64_t f2_dup(float a) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ float f2_lo(uint64_t a) { return __uint_as_float((uint32_t)a); }
+__device__ __forceinline__ float f2_hi(uint64_t a) { return __uint_as_float((uint32_t)(a >> 32)); }
 // One 256-bit read-only load of a record (ld.global.nc.v8.f32, sm_100).
 __device__ __forceinline__ void ld_pd(const PD* __restrict__ base, int i, float4& x, float4& d) {
   asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
