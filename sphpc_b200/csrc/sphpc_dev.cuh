@@ -70,6 +70,7 @@ __device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
 }
 __device__ __forceinline__ float f2_lo(uint64_t a) { return __uint_as_float((uint32_t)a); }
 __device__ __forceinline__ float f2_hi(uint64_t a) { return __uint_as_float((uint32_t)(a >> 32)); }
+
 // One 256-bit read-only load of a record (ld.global.nc.v8.f32, sm_100).
 __device__ __forceinline__ void ld_pd(const PD* __restrict__ base, int i, float4& x, float4& d) {
   asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
