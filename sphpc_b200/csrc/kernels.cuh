@@ -81,6 +81,8 @@ struct PassArgs {
   float* lam_acc;      // position pass: multiplier applied so far this step,
                        // sum of stiffness * lambda_p (null: not kept)
   int acc_add;         // 1: add to lam_acc, 0: start it with this pass
+  const NV* nv;        // post passes: {record, colour or velocity} gathered
+  NV* nv_out;          // post passes: {record, colour or velocity} for the next pass
 };
 
 // Density (+lambda) pass: ComputeDensities (particles.c:461-514) and
@@ -106,15 +108,21 @@ void launch_position(const DevParams& P, const NbrView& V, const PassArgs& a, in
                      cudaStream_t st);
 // UpdatePositionStars alone, in place on pd_out: d += dp, clamp, SDF.
 void launch_apply_dp(const DevParams& P, const PassArgs& a, cudaStream_t st);
+// nv[p] = {nr[p], e[p]}: the combined records of a post pass whose
+// producer did not write them.
+void launch_pack_nv(int n, const uint4* nr, const float4* e, NV* nv, cudaStream_t st);
 // ComputeSurfaceTension colour pass (:94-140) and force pass (:142-204).
-// Density of neighbours is read from d.w.
+// The colour pass gathers nr (neighbour densities in w) and writes color[]
+// and nv_out = {nr, colour}; the force pass gathers nv, updates vel in place
+// and, if nv_out is set, writes {nr, new velocity} there.
 void launch_color(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st);
 void launch_tension(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st);
-// ApplyViscosity (:383-459) as a Jacobi update vel -> vel_out; with
-// write_pos also UpdatePositions into pd_out.
+// ApplyViscosity (:383-459) as a Jacobi update of the velocities in nv into
+// vel_out (and, if set, nv_out = {nr, new velocity}); with write_pos also
+// UpdatePositions into pd_out.
 void launch_xsph(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st);
-// ComputeVorticity (:207-283) from vel; ApplyVorticityConfinement (:285-381)
-// updates vel in place.
+// ComputeVorticity (:207-283) from the velocities in nv;
+// ApplyVorticityConfinement (:285-381) updates vel in place.
 void launch_vorticity(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st);
 void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a, bool omega_in_nr,
                         cudaStream_t st);

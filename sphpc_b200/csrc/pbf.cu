@@ -372,6 +372,13 @@ __global__ void __launch_bounds__(kBlock) k_apply_dp(const DevParams P, const Pa
                               __double2float_rn(__dsub_rn(zs, (double)xp.z)), dp.w);
 }
 
+__global__ void __launch_bounds__(kBlock) k_pack_nv(int n, const uint4* __restrict__ nr,
+                                                    const float4* __restrict__ e,
+                                                    NV* __restrict__ nv) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) st_nv(nv, p, ld_nr(nr, p), __ldg(e + p));
+}
+
 __global__ void __launch_bounds__(kBlock, kMinBlocksColor)
     k_color(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -395,7 +402,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksColor)
     cz = fmaf(c, fz, cz);
   });
   const float s = P.h * (P.DWPn * P.m * P.fx_inv);
-  a.color[p] = make_float4(s * cx, s * cy, s * cz, 0.0f);
+  const float4 col = make_float4(s * cx, s * cy, s * cz, 0.0f);
+  a.color[p] = col;
+  if (a.nv_out) st_nv(a.nv_out, p, rp, col);
 }
 
 __device__ __forceinline__ float cohesion(const DevParams& P, float r) {
@@ -416,8 +425,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
     k_tension(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const uint4 recp = ld_nr(a.nr, p);
-  const float4 cp = __ldg(a.color + p);
+  uint4 recp;
+  float4 cp;
+  ld_nv(a.nv, p, recp, cp);
   const float rp = nr_w(recp);
   const float kcoh = -20.0f * P.gamma * P.m * P.m;
   const float kcur = -P.gamma * P.m;
@@ -428,8 +438,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
   // kcur (c_p - c_q) = kcur c_p - kcur c_q
   const float kpx = kcur * cp.x, kpy = kcur * cp.y, kpz = kcur * cp.z;
   float fx = 0.f, fy = 0.f, fz = 0.f;
-  for_each_neighbor_nr2<kNbrBatch, true>(V, a.nr, a.color, p,
-                                         [&](int, const uint4 rq, const float4 cq) {
+  for_each_neighbor_nv<kNbrBatch, true>(V, a.nv, p, [&](int, const uint4 rq, const float4 cq) {
     const float dx = (float)(int)(recp.x - rq.x);
     const float dy = (float)(int)(recp.y - rq.y);
     const float dz = (float)(int)(recp.z - rq.z);
@@ -448,19 +457,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
   v.y += s * fy;
   v.z += s * fz;
   a.vel[p] = v;
+  if (a.nv_out) st_nv(a.nv_out, p, recp, v);
 }
 
 __global__ void __launch_bounds__(kBlock, kMinBlocksXsph)
     k_xsph(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const uint4 rp = ld_nr(a.nr, p);
-  const float4 vp = __ldg(a.vel + p);
+  uint4 rp;
+  float4 vp;
+  ld_nv(a.nv, p, rp, vp);
   // sums of (v_q - v_p) t^3 / rho_q; the poly6 norm, m and c multiply them
   // once (the padding slots' v_q - v_p is 0)
   float sx = 0.f, sy = 0.f, sz = 0.f;
-  for_each_neighbor_nr2<kNbrBatch, true>(V, a.nr, a.vel, p,
-                                         [&](int, const uint4 rq, const float4 vq) {
+  for_each_neighbor_nv<kNbrBatch, true>(V, a.nv, p, [&](int, const uint4 rq, const float4 vq) {
     const Pair g = pair_nr(P, rp, rq);
     // particles.c:439 evaluates x^2 + y^2 * z^2 (kept unless xsph_exact)
     const float rr = P.xsph_exact ? g.r2 : g.dx * g.dx + g.dy * g.dy * g.dz * g.dz;
@@ -471,7 +481,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksXsph)
     sz = fmaf(vq.z - vp.z, w, sz);
   });
   const float cw = P.c_xsph * P.Wn_m;
-  a.vel_out[p] = make_float4(fmaf(cw, sx, vp.x), fmaf(cw, sy, vp.y), fmaf(cw, sz, vp.z), 0.0f);
+  const float4 vn = make_float4(fmaf(cw, sx, vp.x), fmaf(cw, sy, vp.y), fmaf(cw, sz, vp.z), 0.0f);
+  a.vel_out[p] = vn;
+  if (a.nv_out) st_nv(a.nv_out, p, rp, vn);
   if (a.write_pos) {
     float4 xp, dp;
     ld_pd(a.pd, p, xp, dp);
@@ -489,14 +501,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksVorticity)
     k_vorticity(const DevParams P, const NbrView V, const PassArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const uint4 rp = ld_nr(a.nr, p);
-  const float4 vp = __ldg(a.vel + p);
+  uint4 rp;
+  float4 vp;
+  ld_nv(a.nv, p, rp, vp);
   // sums of (v_q - v_p) x c d with c = (h - r)^2 / r and d in fixed-point
   // units (r too); the spiky norm and 2^-2k multiply them once (the padding slots'
   // v_q - v_p and d are 0)
   float wx = 0.f, wy = 0.f, wz = 0.f;
-  for_each_neighbor_nr2<kNbrBatch, true>(V, a.nr, a.vel, p,
-                                         [&](int, const uint4 rq, const float4 vq) {
+  for_each_neighbor_nv<kNbrBatch, true>(V, a.nv, p, [&](int, const uint4 rq, const float4 vq) {
     const float dx = (float)(int)(rp.x - rq.x);
     const float dy = (float)(int)(rp.y - rq.y);
     const float dz = (float)(int)(rp.z - rq.z);
@@ -711,6 +723,9 @@ void launch_apply_dp(const DevParams& P, const PassArgs& a, cudaStream_t st) {
   else k_apply_dp<false><<<grid_for(P.n), kBlock, 0, st>>>(P, a);
 }
 
+void launch_pack_nv(int n, const uint4* nr, const float4* e, NV* nv, cudaStream_t st) {
+  if (n > 0) k_pack_nv<<<grid_for(n), kBlock, 0, st>>>(n, nr, e, nv);
+}
 void launch_color(const DevParams& P, const NbrView& V, const PassArgs& a, cudaStream_t st) {
   k_color<<<grid_for(P.n), kBlock, 0, st>>>(P, V, a);
 }

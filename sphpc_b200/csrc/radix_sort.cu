@@ -84,21 +84,22 @@ __global__ void __launch_bounds__(kSortThreads, 5)
     (&s_whist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
-  const int64_t tile_base = (int64_t)tile * kSortTile;
-  const int64_t wbase = tile_base + (int64_t)warp * 32 * kSortItems;
+  // n <= kLbValue < 2^30, so every index fits 32 bits
+  const int tile_base = (int)tile * kSortTile;
+  const int wbase = tile_base + warp * 32 * kSortItems;
 
   // the values are loaded only when the tile is staged, so that the ranking
   // holds two arrays of registers, not three
   uint32_t key[kSortItems], rank[kSortItems];
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
-    const int64_t idx = wbase + i * 32 + lane;
+    const int idx = wbase + i * 32 + lane;
     key[i] = idx < n ? __ldg(keys_in + idx) : 0xffffffffu;
   }
   const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
-    const int64_t idx = wbase + i * 32 + lane;
+    const int idx = wbase + i * 32 + lane;
     const uint32_t d = idx < n ? ((key[i] >> shift) & (kRadix - 1)) : (uint32_t)kRadix;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const int leader = __ffs(peers) - 1;
@@ -184,7 +185,7 @@ __global__ void __launch_bounds__(kSortThreads, 5)
   // Stage the tile in digit order.
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
-    const int64_t idx = wbase + i * 32 + lane;
+    const int idx = wbase + i * 32 + lane;
     if (idx < n) {
       const uint32_t d = (key[i] >> shift) & (kRadix - 1);
       const uint32_t lp = s_dstart[d] + s_whist[warp][d] + rank[i];
@@ -193,16 +194,20 @@ __global__ void __launch_bounds__(kSortThreads, 5)
     }
   }
   __syncthreads();
-  const int valid = (int)min((int64_t)kSortTile, (int64_t)n - tile_base);
-  for (int k = t; k < valid; k += kSortThreads) {
-    const uint32_t kk = s_keys[k];
-    const uint32_t d = (kk >> shift) & (kRadix - 1);
-    const uint32_t g = s_gbase[d] + (uint32_t)k - s_dstart[d];
-    if (g < (uint32_t)n) {
-      keys_out[g] = kk;
-      vals_out[g] = s_vals[k];
-    } else {
-      atomicOr(err, 4u);  // inconsistent digit counts: never write out of range
+  const int valid = min(kSortTile, n - tile_base);
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const int k = t + i * kSortThreads;
+    if (k < valid) {
+      const uint32_t kk = s_keys[k];
+      const uint32_t d = (kk >> shift) & (kRadix - 1);
+      const uint32_t g = s_gbase[d] + (uint32_t)k - s_dstart[d];
+      if (g < (uint32_t)n) {
+        keys_out[g] = kk;
+        vals_out[g] = s_vals[k];
+      } else {
+        atomicOr(err, 4u);  // inconsistent digit counts: never write out of range
+      }
     }
   }
 }

@@ -79,6 +79,7 @@ class DeviceSim {
   uint32_t* keys_sorted = nullptr;  // view into keys_by_id or sort.keys_alt
   uint32_t *cellp = nullptr, *nbr = nullptr, *cstart = nullptr;
   float4* xsa = nullptr;
+  NV *nv_a = nullptr, *nv_b = nullptr;  // combined records of the post passes
   uint8_t* ncount = nullptr;
   uint4* gaps = nullptr;
   uint32_t* small = nullptr;  // [0] gap count, [1] explicit count, [2] error bits
@@ -154,7 +155,8 @@ class DeviceSim {
     dfree(color); dfree(omega); dfree(dp); dfree(rho); dfree(lam);
     dfree(color_alt); dfree(omega_alt); dfree(dp_alt); dfree(rho_alt); dfree(lam_alt);
     dfree(ids); dfree(ids_spare); dfree(keys_by_id); dfree(loc_by_id); dfree(cellp);
-    dfree(nbr); dfree(xsa); dfree(cstart); dfree(ncount); dfree(gaps); dfree(small);
+    dfree(nbr); dfree(xsa); dfree(nv_a); dfree(nv_b);
+    dfree(cstart); dfree(ncount); dfree(gaps); dfree(small);
     dfree(resid); dfree(sort.keys_alt); dfree(sort.vals_alt); dfree(sort_aux); dfree(stage);
     mlp_release(mlp);
     for (void* h : pinned) cudaHostUnregister(h);
@@ -184,6 +186,7 @@ class DeviceSim {
     SPHPC_RC(dalloc(&cellp, c)); SPHPC_RC(dalloc(&ncount, c));
     SPHPC_RC(dalloc(&nbr, (size_t)kMaxNeighbors * c));
     SPHPC_RC(dalloc(&xsa, (size_t)c + 2));  // pair blocks: 32 bytes per slot pair
+    SPHPC_RC(dalloc(&nv_a, c)); SPHPC_RC(dalloc(&nv_b, c));
     SPHPC_CK(cudaMemsetAsync(ncount, 0, c, stream));
     SPHPC_RC(dalloc(&small, 8));
     SPHPC_RC(dalloc(&resid, 16));
@@ -803,17 +806,28 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
   a.pd_out = pd_alt;
   a.nr = nr;
   a.nr_out = nullptr;
+  // each pass that gathers the neighbours' velocities (or colours) with their
+  // records reads them from combined 32-byte records {nr, v} written by the
+  // pass before it
   if (solver.surface_tension) {
     Scope sc(this, "surface_tension");
     a.color = color;
+    a.nv_out = nv_a;
     launch_color(P, V, a, stream);
     a.vel = vel;
+    a.nv = nv_a;
+    a.nv_out = nv_b;
     launch_tension(P, V, a, stream);
     launches += 2;
   }
   {
     Scope sc(this, "xsph");
-    a.vel = vel;
+    if (!solver.surface_tension) {
+      launch_pack_nv(n, nr, vel, nv_b, stream);
+      launches += 1;
+    }
+    a.nv = nv_b;
+    a.nv_out = solver.vorticity ? nv_a : nullptr;
     a.vel_out = vel_alt;
     a.write_pos = solver.vorticity ? 0 : 1;
     launch_xsph(P, V, a, stream);
@@ -823,6 +837,8 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     Scope sc(this, "vorticity");
     // the vorticity pass also writes the records {X, |omega|} (into nr_alt)
     // that the confinement pass gathers
+    a.nv = nv_a;
+    a.nv_out = nullptr;
     a.vel = vel_alt;
     a.omega = omega;
     a.nr_out = nr_alt;
@@ -1447,7 +1463,10 @@ int ComputeSurfaceTension(struct Particles* particles, const struct Params* para
   a.nr = s->nr;
   a.color = s->color;
   a.vel = s->vel;
+  a.nv_out = s->nv_a;
   launch_color(P, s->view(), a, s->stream);
+  a.nv = s->nv_a;
+  a.nv_out = nullptr;
   launch_tension(P, s->view(), a, s->stream);
   SPHPC_LAUNCH_DONE();
 }
@@ -1460,9 +1479,11 @@ int ApplyViscosity(struct Particles* particles, const struct Params* params,
   const DevParams P = s->params(*params, nullptr, nullptr);
   launch_pack_w(P, s->pd, nullptr, s->rho, s->stream);
   launch_make_nr(P, s->pd, s->rho, s->nr, s->stream);
+  launch_pack_nv(s->n, s->nr, s->vel, s->nv_a, s->stream);
   PassArgs a{};
   a.pd = s->pd;
   a.nr = s->nr;
+  a.nv = s->nv_a;
   a.vel = s->vel;
   a.vel_out = s->vel_alt;
   launch_xsph(P, s->view(), a, s->stream);
@@ -1477,9 +1498,11 @@ int ComputeVorticity(struct Particles* particles, const struct Params* params,
   SPHPC_NEED_NBR();
   const DevParams P = s->params(*params, nullptr, nullptr);
   launch_make_nr(P, s->pd, nullptr, s->nr, s->stream);
+  launch_pack_nv(s->n, s->nr, s->vel, s->nv_a, s->stream);
   PassArgs a{};
   a.pd = s->pd;
   a.nr = s->nr;
+  a.nv = s->nv_a;
   a.vel = s->vel;
   a.omega = s->omega;
   launch_vorticity(P, s->view(), a, s->stream);

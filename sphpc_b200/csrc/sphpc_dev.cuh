@@ -40,6 +40,15 @@ namespace sphpc {
 
 constexpr int kMaxNeighbors = 60;   // MAX_NEIGHBORS, neighbors.h:6
 
+// 32-byte record for the post-solve passes that gather a second quantity of
+// each neighbour: the 16-byte neighbour record r = {X, Y, Z, w} and a float4
+// e (colour gradient, or velocity), so a neighbour costs one 256-bit gather
+// instead of two 128-bit ones.
+struct __align__(32) NV {
+  uint4 r;
+  float4 e;
+};
+
 // Position record of one particle: step-start x and displacement d = x* - x.
 struct __align__(32) PD {
   float4 x;
@@ -236,6 +245,45 @@ __device__ __forceinline__ void for_each_neighbor_nr2(const NbrView& v,
       r[u] = ld_nr(nr, q[u]);
       e[u] = __ldg(extra + q[u]);
     }
+    int qn[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (kPadSlots || j0 + u < cnt) f(q[u], r[u], e[u]);
+#pragma unroll
+    for (int u = 0; u < B; ++u) q[u] = qn[u];
+  }
+}
+
+__device__ __forceinline__ void ld_nv(const NV* __restrict__ base, int i, uint4& r, float4& e) {
+  asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w), "=f"(e.x), "=f"(e.y), "=f"(e.z), "=f"(e.w)
+      : "l"(base + i));
+}
+
+__device__ __forceinline__ void st_nv(NV* base, int i, const uint4 r, const float4 e) {
+  asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(base + i), "r"(r.x),
+               "r"(r.y), "r"(r.z), "r"(r.w), "f"(e.x), "f"(e.y), "f"(e.z), "f"(e.w)
+               : "memory");
+}
+
+// Batched visit over the 32-byte records {r, e}: f(q, rq, eq), as
+// for_each_neighbor_nr2 but one gather per neighbour.
+template <int B, bool kPadSlots = false, class F>
+__device__ __forceinline__ void for_each_neighbor_nv(const NbrView& v, const NV* __restrict__ nv,
+                                                     int p, F&& f) {
+  const int cnt = (int)__ldg(v.ncount + p);
+  const uint32_t* lst = v.nbr + p;
+  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
+  int q[B];
+#pragma unroll
+  for (int u = 0; u < B; ++u) q[u] = ldq(u);
+  for (int j0 = 0; j0 < cnt; j0 += B) {
+    uint4 r[B];
+    float4 e[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) ld_nv(nv, q[u], r[u], e[u]);
     int qn[B];
 #pragma unroll
     for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
