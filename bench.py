@@ -370,6 +370,26 @@ def run_ours(args, world, rank, local, dist):
             hbm_class[name] = {"bytes_per_particle": per, "avg_launch_ms": tot / cnt,
                                "achieved_gbs": gbs, "frac": gbs / peak}
 
+    # every neighbour stage against the same HBM peak on its algorithmic
+    # bytes, beside its committed ncu DRAM bytes and issue activity (these
+    # stages are bound by instruction issue and the L1 gathers, not by HBM)
+    nbr_stages = {}
+    if prof:
+        peak, kind = peaks()
+        for name in ("build_neighbors", "density_lambda", "position", "surface_tension", "xsph",
+                     "vorticity"):
+            if name not in prof or not prof[name][0]:
+                continue
+            cnt, tot = prof[name]
+            per = STAGE_BYTES[name]
+            gbs = per * n / (tot / cnt / 1e3) / 1e9
+            e = ncu_stage(name)
+            nbr_stages[name] = {"bytes_per_particle": per, "avg_launch_ms": tot / cnt,
+                                "launches_per_step": cnt / args.steps, "achieved_gbs": gbs,
+                                "frac": gbs / peak,
+                                "dram_bytes_per_particle_ncu": e.get("bytes_per_particle"),
+                                "issue_active_ncu": e.get("issue_active_pct")}
+
     # end to end through the C ABI with host buffers, over the same steps of
     # the scene as the headline arm (a fresh particle set, W untimed steps)
     e2e = None
@@ -447,6 +467,7 @@ def run_ours(args, world, rank, local, dist):
         "clocks": clocks,
         "roofline": roof,
         "hbm_class_roofline": hbm_class,
+        "neighbour_stage_roofline": nbr_stages,
         "stage_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()},
         "like_for_like": like,
         "e2e": e2e,
