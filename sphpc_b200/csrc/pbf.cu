@@ -22,10 +22,11 @@ constexpr int kNbrBatch = 4;
 // resident 256-thread blocks per SM asked of the compiler for the neighbour
 // passes (register caps of 40, 48 and 64; more resident warps hide the gather
 // latency better than the registers a larger allocation would keep, as long
-// as the neighbour loop itself does not spill: the position pass spills only
-// in its FP64 epilogue at 40)
+// as the neighbour loop itself does not spill).  The position pass runs at 48:
+// at 40 its FP64 epilogue spills up to 88 bytes a thread through the L1 that
+// its gathers already keep busy (2.4-3.5% slower at 16.7M particles).
 constexpr int kMinBlocksDensity = 6;
-constexpr int kMinBlocksPosition = 6;
+constexpr int kMinBlocksPosition = 5;
 constexpr int kMinBlocksColor = 5;
 constexpr int kMinBlocksVorticity = 5;
 constexpr int kMinBlocksConfinement = 6;
