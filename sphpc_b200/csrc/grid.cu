@@ -308,9 +308,10 @@ __device__ __forceinline__ int walk_27_cells(const DevParams& P, const NbrView& 
 // 128-byte line).  A staged entry is 2 bytes, (row << 12) | offset in the
 // row, with the row starts kept in shared memory, so a thread holds 156
 // bytes of shared memory and the candidate loop only the particle's FP32
-// position: enough blocks stay resident to hide the candidate loads.  A
-// particle with a row of more than 4095 candidates takes the verbatim
-// 27-cell walk.
+// position: enough blocks stay resident to hide the candidate loads.  The
+// candidates of a row are tested two at a time with the packed FP32x2
+// arithmetic of sm_100 (staged_range).  A particle with a row of more than
+// 4095 candidates takes the verbatim 27-cell walk.
 // ---------------------------------------------------------------------------
 constexpr int kStagedBlock = 128;
 constexpr int kRowBits = 12;
