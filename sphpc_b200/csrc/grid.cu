@@ -171,36 +171,54 @@ __device__ __forceinline__ void push_gap(int64_t lo, int64_t hi, uint32_t val, u
   }
 }
 
+// cstart[lo..hi] = v, inline for a short run of cells, else as worklist
+// pieces for k_fill_gaps.
+__device__ __forceinline__ void set_cells(int64_t lo, int64_t hi, uint32_t v,
+                                          uint32_t* __restrict__ cstart, uint4* gaps,
+                                          uint32_t* gap_count) {
+  if (hi - lo + 1 <= kSmallGap) {
+    for (int64_t c = lo; c <= hi; ++c) cstart[c] = v;
+  } else {
+    push_gap(lo, hi, v, gaps, gap_count);
+  }
+}
+
 // start[c] = lower_bound(keys, c): the first slot j of every non-empty key
 // writes j into the cells (key[j-1], key[j]]; long runs of empty cells go to
-// a worklist filled by k_fill_gaps.
+// a worklist filled by k_fill_gaps.  A thread takes four consecutive slots
+// (one 128-bit load of keys and the key before them).
+constexpr int kStartsPerThread = 4;
 __global__ void __launch_bounds__(kBlock)
     k_cell_starts(const uint32_t* __restrict__ keys, int n, uint32_t ncells,
                   uint32_t* __restrict__ cstart, uint4* __restrict__ gaps,
                   uint32_t* __restrict__ gap_count, uint32_t* __restrict__ err) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  const int64_t k = (int64_t)__ldg(keys + j);
-  const int64_t kp = j > 0 ? (int64_t)__ldg(keys + j - 1) : -1;
-  if (k >= (int64_t)ncells) {
-    atomicOr(err, kErrCellRange);
-    return;
+  const int j0 = (blockIdx.x * blockDim.x + threadIdx.x) * kStartsPerThread;
+  if (j0 >= n) return;
+  uint32_t k[kStartsPerThread];
+  if (j0 + kStartsPerThread <= n) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(keys + j0));
+    k[0] = v.x;
+    k[1] = v.y;
+    k[2] = v.z;
+    k[3] = v.w;
+  } else {
+#pragma unroll
+    for (int u = 0; u < kStartsPerThread; ++u) k[u] = j0 + u < n ? __ldg(keys + j0 + u) : 0u;
   }
-  if (k != kp) {
-    const int64_t lo = kp + 1, hi = k;  // inclusive
-    if (hi - lo + 1 <= kSmallGap) {
-      for (int64_t c = lo; c <= hi; ++c) cstart[c] = (uint32_t)j;
-    } else {
-      push_gap(lo, hi, (uint32_t)j, gaps, gap_count);
+  int64_t kp = j0 > 0 ? (int64_t)__ldg(keys + j0 - 1) : -1;
+#pragma unroll
+  for (int u = 0; u < kStartsPerThread; ++u) {
+    const int j = j0 + u;
+    if (j >= n) break;
+    const int64_t kk = (int64_t)k[u];
+    if (kk >= (int64_t)ncells) {
+      atomicOr(err, kErrCellRange);
+      return;
     }
-  }
-  if (j == n - 1) {
-    const int64_t lo = k + 1, hi = (int64_t)ncells;  // includes the sentinel cstart[C]
-    if (hi - lo + 1 <= kSmallGap) {
-      for (int64_t c = lo; c <= hi; ++c) cstart[c] = (uint32_t)n;
-    } else {
-      push_gap(lo, hi, (uint32_t)n, gaps, gap_count);
-    }
+    if (kk != kp) set_cells(kp + 1, kk, (uint32_t)j, cstart, gaps, gap_count);
+    kp = kk;
+    // after the last key: every cell up to the sentinel cstart[C] starts at n
+    if (j == n - 1) set_cells(kk + 1, (int64_t)ncells, (uint32_t)n, cstart, gaps, gap_count);
   }
 }
 
@@ -522,8 +540,9 @@ void launch_cell_starts(const uint32_t* keys_sorted, int n, uint32_t ncells, uin
     return;
   }
   cudaMemsetAsync(gap_count, 0, sizeof(uint32_t), st);
-  k_cell_starts<<<grid_for(n), kBlock, 0, st>>>(keys_sorted, n, ncells, cstart, gaps,
-                                                 gap_count, err);
+  const int threads = (n + kStartsPerThread - 1) / kStartsPerThread;
+  k_cell_starts<<<grid_for(threads), kBlock, 0, st>>>(keys_sorted, n, ncells, cstart, gaps,
+                                                       gap_count, err);
   k_fill_gaps<<<148 * 16, kBlock, 0, st>>>(gaps, gap_count, cstart);
 }
 
