@@ -129,7 +129,9 @@ void launch_confinement(const DevParams& P, const NbrView& V, const PassArgs& a,
 // Pointwise steps.
 void launch_gravity(const DevParams& P, float4* vel, cudaStream_t st);
 void launch_predict(const DevParams& P, PD* pd, const float4* vel, cudaStream_t st);
-void launch_update_velocities(const DevParams& P, const PD* pd, float4* vel, cudaStream_t st);
+// With nr, also nr[p].w = w_src[p] (the records' payload for the post passes).
+void launch_update_velocities(const DevParams& P, const PD* pd, float4* vel, cudaStream_t st,
+                              const float* w_src = nullptr, uint4* nr = nullptr);
 void launch_update_positions(const DevParams& P, PD* pd, cudaStream_t st);
 // d.w and/or the record payload <- src[p] (a per-particle scalar for the
 // neighbour passes; null pd or nr skips it).

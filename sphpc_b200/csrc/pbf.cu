@@ -609,9 +609,11 @@ __global__ void __launch_bounds__(kBlock)
 
 __global__ void __launch_bounds__(kBlock)
     k_update_velocities(const DevParams P, const PD* __restrict__ pd,
-                        float4* __restrict__ vel) {
+                        float4* __restrict__ vel, const float* __restrict__ w_src,
+                        uint4* __restrict__ nr) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.n) return;
+  if (nr) nr[p].w = __float_as_uint(w_src[p]);
   const float4 d = pd[p].d;
   float vx = __double2float_rn(__ddiv_rn((double)d.x, P.dt_d));
   float vy = __double2float_rn(__ddiv_rn((double)d.y, P.dt_d));
@@ -750,8 +752,9 @@ void launch_gravity(const DevParams& P, float4* vel, cudaStream_t st) {
 void launch_predict(const DevParams& P, PD* pd, const float4* vel, cudaStream_t st) {
   k_predict<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, vel);
 }
-void launch_update_velocities(const DevParams& P, const PD* pd, float4* vel, cudaStream_t st) {
-  k_update_velocities<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, vel);
+void launch_update_velocities(const DevParams& P, const PD* pd, float4* vel, cudaStream_t st,
+                              const float* w_src, uint4* nr) {
+  k_update_velocities<<<grid_for(P.n), kBlock, 0, st>>>(P, pd, vel, w_src, nr);
 }
 void launch_update_positions(const DevParams& P, PD* pd, cudaStream_t st) {
   k_update_positions<<<grid_for(P.n), kBlock, 0, st>>>(P, pd);

@@ -785,11 +785,8 @@ int DeviceSim::run_step(const DevParams& P, const Params& prm) {
     // converged (or capped, or no plain pass): velocities from x* and the
     // freshest density
     Scope sc(this, "velocity");
-    if (converged || stalled || iters == 0) {
-      launch_pack_w(P, nullptr, nr, rho, stream);
-      launches += 1;
-    }
-    launch_update_velocities(P, pd, vel, stream);
+    const bool pack = converged || stalled || iters == 0;
+    launch_update_velocities(P, pd, vel, stream, pack ? rho : nullptr, pack ? nr : nullptr);
     launches += 1;
   }
   last_iterations = iters;
