@@ -3,7 +3,7 @@ training target against the FP64 oracle, and the FP64 residual gate."""
 import numpy as np
 import pytest
 
-from helpers import assert_close, oracle_for
+from helpers import assert_close, oracle_for, parity_record
 from sphpc_b200 import Simulation
 from sphpc_b200 import warm_start as ws
 
@@ -160,3 +160,39 @@ def test_network_threshold_skips_mild_steps():
                 # a mild step); after that, and after plain steps, none does
                 assert (features, forward, used) == (1 if pre == 0 else 0, 0, 0), (pre, prof)
             assert sim.device_errors() == 0
+
+
+def test_warm_pass_against_plain_iterations_on_config2():
+    """The evaluation of the learned warm start on the 1,048,576-particle dam
+    break (fixed iteration counts, FP64 residual gate on): from the same state
+    60 steps into the collapse, each step's final positions get an extra
+    density evaluation, and the mean of the FP64 max density error over 5
+    steps is compared between the network's warm pass followed by 2 plain
+    iterations and 2, 3 and 4 plain iterations.  The committed network's pass
+    is worth one plain iteration here: its arm ends where 3 plain iterations
+    end (3.7% against 4.6% with 2 and 3.2% with 4)."""
+    params, norm, meta = ws.load_network()
+    err = {}
+    for arm, its in (("warm+2", 3), ("plain2", 2), ("plain3", 3), ("plain4", 4)):
+        with Simulation("dam_break_1m") as sim:
+            sim.step(60)
+            if arm == "warm+2":
+                sim.mlp_load(params, norm)
+                sim.set_solver(warm_start=1, warm_start_min_error=0.0,
+                               warm_start_scale=float(meta.get("warm_start_scale", 1.0)))
+            # the cap counts every position pass of a step, the warm pass included
+            sim.set_solver(solve_iterations=its, adaptive=0)
+            e = []
+            for _ in range(5):
+                sim.step(1)
+                if arm == "warm+2":
+                    assert sim.last_step_info()["warm_start_used"] == 1
+                sim.find_all_neighbors()
+                sim.compute_densities()
+                e.append(sim.diagnostics()["max_density_error"])
+            assert sim.device_errors() == 0
+            err[arm] = float(np.mean(e))
+    parity_record("warm_pass_vs_plain_iterations_dam_break_1m",
+                  {"steps_before": 60, "steps": 5, "mean_max_density_error": err})
+    assert err["warm+2"] < 0.9 * err["plain2"], err
+    assert err["plain4"] < err["plain3"] < err["plain2"], err
