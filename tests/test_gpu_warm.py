@@ -170,7 +170,8 @@ def test_warm_pass_against_plain_iterations_on_config2():
     steps is compared between the network's warm pass followed by 2 plain
     iterations and 2, 3 and 4 plain iterations.  The committed network's pass
     is worth one plain iteration here: its arm ends where 3 plain iterations
-    end (3.7% against 4.6% with 2 and 3.2% with 4)."""
+    end (4.14% and 4.16% over these 5 steps, against 5.07% with 2 and 3.58%
+    with 4)."""
     params, norm, meta = ws.load_network()
     err = {}
     for arm, its in (("warm+2", 3), ("plain2", 2), ("plain3", 3), ("plain4", 4)):
