@@ -278,8 +278,16 @@ def run_ours(args, world, rank, local, dist):
         overrides["stiffness_k"] = args.stiffness_k
     arms = [a.strip() for a in args.arms.split(",") if a.strip()]
     net = None
+    warm_settings = None
     if not args.no_warm and os.path.exists(args.weights):
         net = ws.load_network(args.weights)
+        # the settings stored with the network unless overridden
+        warm_settings = {
+            "scale": args.warm_scale if args.warm_scale is not None
+            else float(net[2].get("warm_start_scale", 1.0)),
+            "min_error": args.warm_min_error if args.warm_min_error is not None
+            else float(net[2].get("warm_start_min_error", 0.0)),
+            "gate": int(args.warm_gate)}
     stream = torch.cuda.current_stream(dev)
 
     def make_sim(kind):
@@ -291,8 +299,9 @@ def run_ours(args, world, rank, local, dist):
         if kind == "warm":
             sim.mlp_load(net[0], net[1])
             sim.set_solver(warm_start=1, warm_start_source=0,
-                           warm_start_scale=float(net[2].get("warm_start_scale", 1.0)),
-                           warm_start_min_error=float(net[2].get("warm_start_min_error", 0.0)))
+                           warm_start_scale=warm_settings["scale"],
+                           warm_start_min_error=warm_settings["min_error"],
+                           warm_start_gate=warm_settings["gate"])
         elif kind == "carry":
             sim.set_solver(warm_start=1, warm_start_source=1, warm_start_min_error=0.0)
         elif kind == "fixed":
@@ -446,8 +455,10 @@ def run_ours(args, world, rank, local, dist):
                               + (f"; stop when two iterations lower it by < "
                                  f"{100 * args.min_progress:g}%" if args.min_progress > 0 else "")
                               + ")")
-                   + ((", MLP warm start (network skipped at feature-pass error <= "
-                       f"{float(net[2].get('warm_start_min_error', 0.0)):g})")
+                   + ((", MLP warm start (output scale "
+                       f"{warm_settings['scale']:g}, network skipped at feature-pass error <= "
+                       f"{warm_settings['min_error']:g}, residual gate "
+                       f"{'on' if warm_settings['gate'] else 'off'})")
                       if warm is not None else ", plain (no network file)"),
                    "plain": arm_summary(plain),
                    "warm_start": arm_summary(warm),
@@ -568,6 +579,15 @@ def main():
                          "(the reference's 0.95 by default; 1 gives a constant 1)")
     ap.add_argument("--weights", default=os.path.join(ROOT, "sphpc_b200", "weights",
                                                       "warm_start.npz"))
+    ap.add_argument("--warm-scale", type=float, default=None,
+                    help="multiplier on the network's output (default: the one stored "
+                         "with the network)")
+    ap.add_argument("--warm-min-error", type=float, default=None,
+                    help="first-pass max density error below which the network is skipped "
+                         "(default: the one stored with the network)")
+    ap.add_argument("--warm-gate", type=int, default=1,
+                    help="1: discard a warm pass that does not lower the FP64 max density "
+                         "error (the residual gate); 0: keep every warm pass")
     ap.add_argument("--ref-iterations", type=int, default=6)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     args = ap.parse_args()
