@@ -59,3 +59,37 @@ def test_reference_arm_prints_on_rank_zero_only(capsys):
         steps = 1
     bench.run_reference(A, 2, 1)   # a non-zero rank exits without work
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_line_keeps_the_bench_contract(capsys):
+    """`bench.py --impl reference` on rank 0: one JSON line with the bench
+    contract's keys, the reference arm's marker and its CPU baseline, e2e
+    without host-device copies (a one-step, one-iteration sample)."""
+    import json
+
+    sys.path.insert(0, ROOT)
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libsphpc_ref_fast.so")):
+        pytest.skip("the reference's CPU path is not built here")
+    import bench
+
+    class A:
+        config = "dam_break_32k"
+        ref_iterations = 1
+        warmup = 0
+        steps = 1
+    bench.run_reference(A, 1, 0)
+    out = [l for l in capsys.readouterr().out.splitlines() if l.startswith("{")]
+    assert len(out) == 1
+    d = json.loads(out[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["n_gpus"] == 1
+    assert d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
+    assert d["higher_is_better"] is True and d["steps"] == 1 and d["warmup"] == 0
+    assert d["config"]["workload"] == "dam_break_32k"
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] == 1 and cb["value"] == d["value"]
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0
+    assert e["d2h_bytes_per_step"] == 0
