@@ -122,6 +122,26 @@ class Simulation:
             self.host(f)[:] = v
         call("sphpc_update_device", C.byref(self.particles))
 
+    def save_state(self, path: str):
+        """Checkpoint: the particle arrays of struct Particles (the reference's
+        own state, original order, FP64 copies of the device's values) and the
+        solver settings, to an .npz file."""
+        arrays = self.fetch()
+        solver = {f: getattr(self.solver, f) for f, _ in self.solver._fields_}
+        np.savez(path, n=self.n, solver=np.array([solver], dtype=object), **arrays)
+
+    def load_state(self, path: str):
+        """Resume from save_state() into a set of the same configuration: the
+        arrays go to the device and the solver settings are restored, so the
+        steps that follow are those the saved run would have taken (the
+        warm-start's skip rule also reads the previous step's first residual,
+        which is not part of the checkpoint)."""
+        with np.load(path, allow_pickle=True) as z:
+            if int(z["n"]) != self.n:
+                raise ValueError(f"checkpoint of {int(z['n'])} particles, set of {self.n}")
+            self.push({f: z[f] for f in z.files if f not in ("n", "solver")})
+            self.set_solver(**z["solver"][0])
+
     def set_solver(self, **kw):
         for k, v in kw.items():
             setattr(self.solver, k, v)
