@@ -1,4 +1,4 @@
-"""Checkpoint and resume through the C ABI's host arrays (SphSimulation's
+"""Checkpoint and resume through the C ABI's host arrays (struct
 Particles, the reference's own state): a set saved after k steps and loaded
 into a fresh set of the same configuration takes the same next steps as the
 run that was not interrupted, bit for bit."""
