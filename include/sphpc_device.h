@@ -60,6 +60,12 @@ int FindUpperBounds(const unsigned int *const hash_values, const int value_count
 int sphpc_check_sort_wait(int spin_limit, unsigned int *error_bits);
 int sphpc_check_mbarrier_wait(int poll_limit, unsigned int *error_bits);
 
+/* No counterpart in the reference.  Failure injection for the allocation
+ * error paths: after `after` more device allocations of a particle set have
+ * succeeded, the next one fails with SPHPC_ENOMEM (without calling
+ * cudaMalloc) and the injection switches itself off; -1 switches it off. */
+int sphpc_fail_device_alloc(int after);
+
 /* obstacle_cuda.h:23-27 (obstacle_cuda.cu:118-131): pushes every particle
  * whose double position lies inside the obstacle out along the SDF normal.
  * The obstacle must have been uploaded (AllocInitObstacle / _CUDA).  Runs on

@@ -191,6 +191,7 @@ SIGNATURES = {
                                 C.POINTER(C.c_float)], C.c_int),
     "sphpc_mlp_grad": ([C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_void_p],
                        C.c_int),
+    "sphpc_fail_device_alloc": ([C.c_int], C.c_int),
     "sphpc_mlp_dataset_reserve": ([C.c_longlong], C.c_int),
     "sphpc_mlp_dataset_size": ([C.POINTER(C.c_longlong)], C.c_int),
     "sphpc_mlp_dataset_clear": ([], C.c_int),

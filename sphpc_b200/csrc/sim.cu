@@ -5,6 +5,7 @@
 // particles.c:1056-1078).  Its kernels run on one stream; the reference-named
 // step functions launch one stage each, sphpc_step launches the fused step.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -27,9 +28,21 @@ struct Obstacle_CUDA {
 
 namespace sphpc {
 
+// Failure injection for the allocation error paths (sphpc_fail_device_alloc):
+// the number of particle-set device allocations still to succeed before one
+// fails with SPHPC_ENOMEM without calling cudaMalloc; -1: off.
+static std::atomic<long long> g_alloc_fail_after{-1};
+
 template <class T>
 static int dalloc(T** p, size_t n) {
   if (n == 0) n = 1;
+  long long left = g_alloc_fail_after.load();
+  while (left >= 0 && !g_alloc_fail_after.compare_exchange_weak(left, left - 1)) {
+  }
+  if (left == 0) {
+    *p = nullptr;
+    return set_error(SPHPC_ENOMEM, "cudaMalloc(%zu bytes): failure injected", n * sizeof(T));
+  }
   const cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
   if (e != cudaSuccess) {
     *p = nullptr;
@@ -1976,6 +1989,12 @@ static int wait_check(const char* what, cudaError_t e, uint32_t bits, unsigned i
   if (e != cudaSuccess) return set_error(SPHPC_ECUDA, "%s: %s", what, cudaGetErrorString(e));
   if (bits) return set_error(SPHPC_EKERNEL, "%s: the bounded wait gave up (error bits 0x%x)",
                              what, bits);
+  return SPHPC_OK;
+}
+
+int sphpc_fail_device_alloc(int after) {
+  if (after < -1) return set_error(SPHPC_EINVAL, "sphpc_fail_device_alloc: %d < -1", after);
+  g_alloc_fail_after.store(after);
   return SPHPC_OK;
 }
 

@@ -60,3 +60,42 @@ def test_wait_checks_reject_limits_outside_their_range():
     assert lib.sphpc_check_sort_wait((1 << 22) + 1, C.byref(bits)) == EINVAL
     assert lib.sphpc_check_mbarrier_wait(0, C.byref(bits)) == EINVAL
     assert lib.sphpc_check_mbarrier_wait((1 << 20) + 1, C.byref(bits)) == EINVAL
+
+
+ENOMEM = -4
+
+
+def _first_error(config, steps):
+    """Creates a particle set and steps it; the code of the first error, or 0."""
+    from sphpc_b200 import Simulation
+    from sphpc_b200._lib import SphpcError
+    try:
+        with Simulation(config) as sim:
+            sim.step(steps)
+            assert sim.device_errors() == 0
+    except SphpcError as e:
+        return e.code
+    return 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("after", [0, 1, 4, 12])
+def test_device_allocation_failure_is_an_error_and_the_next_set_works(after):
+    """An allocation of the particle set's device copy that fails (injected
+    on the host: the allocation returns the error cudaMalloc would) is
+    reported as SPHPC_ENOMEM by the call that needed it; the partly built set
+    is released, and a set made afterwards steps normally."""
+    lib = _lib.load()
+    try:
+        assert lib.sphpc_fail_device_alloc(after) == 0
+        assert _first_error("small_dam", 1) == ENOMEM
+    finally:
+        lib.sphpc_fail_device_alloc(-1)
+    assert _first_error("small_dam", 2) == 0
+    _sort_still_exact()
+
+
+def test_allocation_injection_rejects_bad_arguments():
+    lib = _lib.load()
+    assert lib.sphpc_fail_device_alloc(-2) == EINVAL
+    assert lib.sphpc_fail_device_alloc(-1) == 0
