@@ -224,38 +224,6 @@ __device__ __forceinline__ void for_each_neighbor_nr(const NbrView& v, const uin
   }
 }
 
-// The same with a second per-neighbour array (velocity, colour) fetched in
-// the same batch: f(q, rq, eq).
-template <int B, bool kPadSlots = false, class F>
-__device__ __forceinline__ void for_each_neighbor_nr2(const NbrView& v,
-                                                      const uint4* __restrict__ nr,
-                                                      const float4* __restrict__ extra, int p,
-                                                      F&& f) {
-  const int cnt = (int)__ldg(v.ncount + p);
-  const uint32_t* lst = v.nbr + p;
-  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
-  int q[B];
-#pragma unroll
-  for (int u = 0; u < B; ++u) q[u] = ldq(u);
-  for (int j0 = 0; j0 < cnt; j0 += B) {
-    uint4 r[B];
-    float4 e[B];
-#pragma unroll
-    for (int u = 0; u < B; ++u) {
-      r[u] = ld_nr(nr, q[u]);
-      e[u] = __ldg(extra + q[u]);
-    }
-    int qn[B];
-#pragma unroll
-    for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
-#pragma unroll
-    for (int u = 0; u < B; ++u)
-      if (kPadSlots || j0 + u < cnt) f(q[u], r[u], e[u]);
-#pragma unroll
-    for (int u = 0; u < B; ++u) q[u] = qn[u];
-  }
-}
-
 __device__ __forceinline__ void ld_nv(const NV* __restrict__ base, int i, uint4& r, float4& e) {
   asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
       : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w), "=f"(e.x), "=f"(e.y), "=f"(e.z), "=f"(e.w)
@@ -269,7 +237,7 @@ __device__ __forceinline__ void st_nv(NV* base, int i, const uint4 r, const floa
 }
 
 // Batched visit over the 32-byte records {r, e}: f(q, rq, eq), as
-// for_each_neighbor_nr2 but one gather per neighbour.
+// for_each_neighbor_nr with one 256-bit gather per neighbour.
 template <int B, bool kPadSlots = false, class F>
 __device__ __forceinline__ void for_each_neighbor_nv(const NbrView& v, const NV* __restrict__ nv,
                                                      int p, F&& f) {
