@@ -186,36 +186,47 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksFeatures)
   if (p < P.n) {
     float4 xp, dp;
     ld_pd(a.pd, p, xp, dp);
-    float rho = P.W0m, comp = 0.0f;
+    // Only what varies per pair stays in the loop: the Kahan sum of t^3
+    // (t = h^2 - r^2), the sums of c d with c = (h - r)^2 / r and of c^2 r^2,
+    // the neighbour offsets and displacements; the kernel norms and the mass
+    // multiply the sums once afterwards, as in the density pass.
+    float st = 0.0f, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
     float ox = 0.f, oy = 0.f, oz = 0.f, ux = 0.f, uy = 0.f, uz = 0.f, rmin2 = P.h2;
     int cnt = 0;
     for_each_neighbor_pd<kNbrBatch>(V, a.pd, p, [&](int, const float4 xq, const float4 dq) {
       const Pair g = pair_geom(xp, dp, xq, dq);
-      const float t = P.h2 - g.r2;
-      const float w = t > 0.0f ? P.Wn_m * t * t * t : 0.0f;
-      const float y = w - comp;
-      const float s = rho + y;
-      comp = (s - rho) - y;
-      rho = s;
+      const float t = fmaxf(P.h2 - g.r2, 0.0f);
+      const float y = t * t * t - comp;
+      const float s = st + y;
+      comp = (s - st) - y;
+      st = s;
       float r, rinv;
       floored_r(P, g.r2, r, rinv);
-      const float hm = P.h - r;
-      const float c = hm > 0.0f ? P.DWn_m * hm * hm * rinv : 0.0f;
-      const float gx = c * g.dx, gy = c * g.dy, gz = c * g.dz;
-      sgx += gx;
-      sgy += gy;
-      sgz += gz;
-      sC += gx * gx + gy * gy + gz * gz;
+      const float hm = fmaxf(P.h - r, 0.0f);
+      const float c = hm * hm * rinv;
+      sgx = fmaf(c, g.dx, sgx);
+      sgy = fmaf(c, g.dy, sgy);
+      sgz = fmaf(c, g.dz, sgz);
+      sC = fmaf(c * c, g.r2, sC);
       ox -= g.dx;
       oy -= g.dy;
       oz -= g.dz;
-      ux += dq.x - dp.x;
-      uy += dq.y - dp.y;
-      uz += dq.z - dp.z;
+      ux += dq.x;
+      uy += dq.y;
+      uz += dq.z;
       rmin2 = fminf(rmin2, g.r2);
       ++cnt;
     });
+    // sum_q (d_q - d_p) from sum_q d_q
+    ux = fmaf(-(float)cnt, dp.x, ux);
+    uy = fmaf(-(float)cnt, dp.y, uy);
+    uz = fmaf(-(float)cnt, dp.z, uz);
+    sgx *= P.DWn_m;
+    sgy *= P.DWn_m;
+    sgz *= P.DWn_m;
+    sC *= P.DWn_m * P.DWn_m;
+    const float rho = fmaf(P.Wn_m, st - comp, P.W0m);
     a.rho[p] = rho;
     const float C = (float)fmax(__ddiv_rn((double)rho, P.rho0_d) - 1.0, 0.0);
     const float s_pairs = sC * P.inv_rho0_sq;
