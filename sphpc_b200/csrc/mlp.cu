@@ -731,7 +731,14 @@ static void pack_bf16(const MlpDevice& d, cudaStream_t st) {
   k_to_bf16<<<(n2 + 255) / 256, 256, 0, st>>>(d.params + kOffW3, d.wbf + n1 + n2, n2);
 }
 
+static int set_mlp_attrs();
+
+// Uploads the parameters and the normalisation, and readies the network's
+// kernels on this device (their shared-memory opt-in, which also makes the
+// runtime load them), so that the first step that runs the network does not
+// pay for that.
 int mlp_upload(MlpDevice& d, const float* params, const float* norm, cudaStream_t st) {
+  SPHPC_RC(set_mlp_attrs());
   cudaError_t e = cudaSuccess;
   if (!d.params) e = cudaMalloc(&d.params, sizeof(float) * kMlpParams);
   if (e == cudaSuccess && !d.norm) e = cudaMalloc(&d.norm, sizeof(float) * kMlpNorm);

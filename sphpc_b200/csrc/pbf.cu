@@ -78,6 +78,16 @@ __device__ __forceinline__ void floored_r_fx(const DevParams& P, float r2f, floa
   r = r2c * rinv;
 }
 
+// 1/x by the hardware's approximate reciprocal (PTX rcp.approx.ftz.f32, at
+// most 1 ulp from the rounded quotient): one instruction where the correctly
+// rounded reciprocal takes a refinement sequence.  Used for the neighbour
+// densities of the post passes (x near rho0, never subnormal).
+__device__ __forceinline__ float rcp_fast(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 __device__ __forceinline__ void block_resid(double e, double* resid) {
   // max and sum of the per-particle density error over the block (FP64).
   double m = e, s = e;
@@ -113,34 +123,48 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
   if (p < P.n) {
     const uint4 rp = ld_nr(a.nr, p);
     // The loop keeps only what varies per pair: the density sums t^3 with
-    // t = h^2 - r^2 (Kahan-compensated) and the gradient sums c d with
-    // c = (h - r)^2 / r and d the pair difference, both in fixed-point units;
-    // the kernel norms, the mass and 2^-2k multiply the sums once afterwards.
+    // t = h^2 - r^2 and the gradient sums c d with c = (h - r)^2 / r and d
+    // the pair difference, both in fixed-point units; the kernel norms, the
+    // mass and 2^-2k multiply the sums once afterwards.  The density sum is
+    // Kahan-compensated per batch: a batch's four terms are added pairwise
+    // (relative error at most 2 ulp of the batch sum, all terms >= 0) and the
+    // batch sum enters the compensated running sum.  Padding slots past the
+    // count are the pair (p, p): their density term is masked, their gradient
+    // terms carry d = 0.
     float st = 0.0f, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
-    for_each_neighbor_nr<kNbrBatch>(V, a.nr, p, [&](int, const uint4 rq) {
-      const float fx = (float)(int)(rp.x - rq.x);
-      const float fy = (float)(int)(rp.y - rq.y);
-      const float fz = (float)(int)(rp.z - rq.z);
-      const float r2f = fx * fx + fy * fy + fz * fz;
+    for_each_batch_nr<kNbrBatch>(V, a.nr, p, [&](const uint4 (&rq)[kNbrBatch], int nvalid) {
+      float t3[kNbrBatch];
+#pragma unroll
+      for (int u = 0; u < kNbrBatch; ++u) {
+        const float fx = (float)(int)(rp.x - rq[u].x);
+        const float fy = (float)(int)(rp.y - rq[u].y);
+        const float fz = (float)(int)(rp.z - rq[u].z);
+        const float r2f = fx * fx + fy * fy + fz * fz;
+        if (MODE != 2) {
+          float t = fmaxf(fmaf(-P.fx_inv2, r2f, P.h2), 0.0f);
+          t = u < nvalid ? t : 0.0f;
+          t3[u] = t * t * t;
+        }
+        if (MODE != 1) {
+          // in fixed-point units: c_f = (h_f - r_f)^2 / r_f = 2^k c
+          float r2c, r, rinv;
+          floored_r_fx(P, r2f, r2c, r, rinv);
+          const float hm = fmaxf(P.h_fx - r, 0.0f);
+          const float c = hm * hm * rinv;
+          // |c d|^2 = c^2 |d|^2: three fused accumulations and one for the norm
+          sgx = fmaf(c, fx, sgx);
+          sgy = fmaf(c, fy, sgy);
+          sgz = fmaf(c, fz, sgz);
+          sC = fmaf(c * c, r2f, sC);
+        }
+      }
       if (MODE != 2) {
-        const float t = fmaxf(fmaf(-P.fx_inv2, r2f, P.h2), 0.0f);
-        const float y = t * t * t - comp;
+        static_assert(kNbrBatch == 4, "pairwise batch sum of four terms");
+        const float y = ((t3[0] + t3[1]) + (t3[2] + t3[3])) - comp;
         const float s = st + y;
         comp = (s - st) - y;
         st = s;
-      }
-      if (MODE != 1) {
-        // in fixed-point units: c_f = (h_f - r_f)^2 / r_f = 2^k c
-        float r2c, r, rinv;
-        floored_r_fx(P, r2f, r2c, r, rinv);
-        const float hm = fmaxf(P.h_fx - r, 0.0f);
-        const float c = hm * hm * rinv;
-        // |c d|^2 = c^2 |d|^2: three fused accumulations and one for the norm
-        sgx = fmaf(c, fx, sgx);
-        sgy = fmaf(c, fy, sgy);
-        sgz = fmaf(c, fz, sgz);
-        sC = fmaf(c * c, r2f, sC);
       }
     });
     float rho;
@@ -186,37 +210,46 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksFeatures)
   if (p < P.n) {
     float4 xp, dp;
     ld_pd(a.pd, p, xp, dp);
-    // Only what varies per pair stays in the loop: the Kahan sum of t^3
+    // Only what varies per pair stays in the loop: the sum of t^3
     // (t = h^2 - r^2), the sums of c d with c = (h - r)^2 / r and of c^2 r^2,
     // the neighbour offsets and displacements; the kernel norms and the mass
-    // multiply the sums once afterwards, as in the density pass.
+    // multiply the sums once afterwards, as in the density pass.  The t^3
+    // sum is Kahan-compensated per batch of four neighbours, as there.
     float st = 0.0f, comp = 0.0f;
     float sgx = 0.f, sgy = 0.f, sgz = 0.f, sC = 0.f;
     float ox = 0.f, oy = 0.f, oz = 0.f, ux = 0.f, uy = 0.f, uz = 0.f, rmin2 = P.h2;
     int cnt = 0;
-    for_each_neighbor_pd<kNbrBatch>(V, a.pd, p, [&](int, const float4 xq, const float4 dq) {
-      const Pair g = pair_geom(xp, dp, xq, dq);
-      const float t = fmaxf(P.h2 - g.r2, 0.0f);
-      const float y = t * t * t - comp;
+    for_each_batch_pd<kNbrBatch>(V, a.pd, p, [&](const float4 (&xq)[kNbrBatch],
+                                                 const float4 (&dq)[kNbrBatch], int nvalid) {
+      float yb = 0.0f;
+#pragma unroll
+      for (int u = 0; u < kNbrBatch; ++u) {
+        if (u < nvalid) {
+          const Pair g = pair_geom(xp, dp, xq[u], dq[u]);
+          const float t = fmaxf(P.h2 - g.r2, 0.0f);
+          yb += t * t * t;
+          float r, rinv;
+          floored_r(P, g.r2, r, rinv);
+          const float hm = fmaxf(P.h - r, 0.0f);
+          const float c = hm * hm * rinv;
+          sgx = fmaf(c, g.dx, sgx);
+          sgy = fmaf(c, g.dy, sgy);
+          sgz = fmaf(c, g.dz, sgz);
+          sC = fmaf(c * c, g.r2, sC);
+          ox -= g.dx;
+          oy -= g.dy;
+          oz -= g.dz;
+          ux += dq[u].x;
+          uy += dq[u].y;
+          uz += dq[u].z;
+          rmin2 = fminf(rmin2, g.r2);
+          ++cnt;
+        }
+      }
+      const float y = yb - comp;
       const float s = st + y;
       comp = (s - st) - y;
       st = s;
-      float r, rinv;
-      floored_r(P, g.r2, r, rinv);
-      const float hm = fmaxf(P.h - r, 0.0f);
-      const float c = hm * hm * rinv;
-      sgx = fmaf(c, g.dx, sgx);
-      sgy = fmaf(c, g.dy, sgy);
-      sgz = fmaf(c, g.dz, sgz);
-      sC = fmaf(c * c, g.r2, sC);
-      ox -= g.dx;
-      oy -= g.dy;
-      oz -= g.dz;
-      ux += dq.x;
-      uy += dq.y;
-      uz += dq.z;
-      rmin2 = fminf(rmin2, g.r2);
-      ++cnt;
     });
     // sum_q (d_q - d_p) from sum_q d_q
     ux = fmaf(-(float)cnt, dp.x, ux);
@@ -408,7 +441,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksColor)
     float r2c, r, rinv;
     floored_r_fx(P, fx * fx + fy * fy + fz * fz, r2c, r, rinv);
     const float t = fmaxf(fmaf(-P.fx_inv2, r2c, P.h2), 0.0f);
-    const float c = t * t * r * (rinv * __frcp_rn(nr_w(rq)));
+    const float c = t * t * r * (rinv * rcp_fast(nr_w(rq)));
     cx = fmaf(c, fx, cx);
     cy = fmaf(c, fy, cy);
     cz = fmaf(c, fz, cz);
@@ -419,18 +452,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksColor)
   if (a.nv_out) st_nv(a.nv_out, p, rp, col);
 }
 
-__device__ __forceinline__ float cohesion(const DevParams& P, float r) {
-  // Akinci cohesion spline, particles.c:54-65
-  const float hr = P.h - r;
-  float c;
-  if (r > P.h)
-    c = 0.0f;
-  else if (r <= 0.5f * P.h) {
-    const float h3 = P.h * P.h * P.h;
-    c = 2.0f * hr * hr * hr * r * r * r - h3 * h3 * (1.0f / 64.0f);
-  } else
-    c = hr * hr * hr * r * r * r;
-  return P.C_norm * c;
+// Akinci cohesion spline (particles.c:54-65) without its norm: with
+// y = ((h - r) r)^3, 2y - h^6/64 for r <= h/2, y up to h, 0 beyond (h6_64 =
+// h^6/64); selects, no branches.
+__device__ __forceinline__ float cohesion_unnormed(const DevParams& P, float r, float h6_64) {
+  const float hr = (P.h - r) * r;
+  const float y = hr * hr * hr;
+  float c = r <= 0.5f * P.h ? fmaf(2.0f, y, -h6_64) : y;
+  return r > P.h ? 0.0f : c;
 }
 
 __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
@@ -445,7 +474,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
   const float kcur = -P.gamma * P.m;
   // colour of each neighbour fetched with its record; the self terms of the
   // padding slots vanish (d = 0, c_p - c_q = 0)
-  const float kcoh_fx = kcoh * P.fx_inv;  // for d in fixed-point units (exact)
+  // the spline's norm and 2^-k for d in fixed-point units (exact)
+  const float kcoh_fx = kcoh * P.C_norm * P.fx_inv;
+  const float h3 = P.h * P.h * P.h;
+  const float h6_64 = h3 * h3 * (1.0f / 64.0f);
   const float two_rho0 = 2.0f * P.rho0;
   // kcur (c_p - c_q) = kcur c_p - kcur c_q
   const float kpx = kcur * cp.x, kpy = kcur * cp.y, kpz = kcur * cp.z;
@@ -457,8 +489,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
     const float r2 = (dx * dx + dy * dy + dz * dz) * P.fx_inv2;
     float r, rinv;
     floored_r(P, r2, r, rinv);
-    const float coh = kcoh_fx * cohesion(P, r) * rinv;
-    const float K = two_rho0 * __frcp_rn(rp + nr_w(rq));
+    const float coh = kcoh_fx * cohesion_unnormed(P, r, h6_64) * rinv;
+    const float K = two_rho0 * rcp_fast(rp + nr_w(rq));
     fx = fmaf(K, fmaf(coh, dx, fmaf(-kcur, cq.x, kpx)), fx);
     fy = fmaf(K, fmaf(coh, dy, fmaf(-kcur, cq.y, kpy)), fy);
     fz = fmaf(K, fmaf(coh, dz, fmaf(-kcur, cq.z, kpz)), fz);
@@ -487,7 +519,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksXsph)
     // particles.c:439 evaluates x^2 + y^2 * z^2 (kept unless xsph_exact)
     const float rr = P.xsph_exact ? g.r2 : g.dx * g.dx + g.dy * g.dy * g.dz * g.dz;
     const float t = fmaxf(P.h2 - rr, 0.0f);
-    const float w = t * t * t * __frcp_rn(nr_w(rq));
+    const float w = t * t * t * rcp_fast(nr_w(rq));
     sx = fmaf(vq.x - vp.x, w, sx);
     sy = fmaf(vq.y - vp.y, w, sy);
     sz = fmaf(vq.z - vp.z, w, sz);

@@ -224,6 +224,29 @@ __device__ __forceinline__ void for_each_neighbor_nr(const NbrView& v, const uin
   }
 }
 
+// The same batched visit with the whole batch handed to f(r[B], nvalid):
+// r[u] is the record of list entry j0 + u for u < nvalid = min(B, cnt - j0)
+// and the particle's own record past the count (the pair (p, p), difference
+// 0), so a body can combine the batch's terms before adding them to a sum.
+template <int B, class F>
+__device__ __forceinline__ void for_each_batch_nr(const NbrView& v, const uint4* __restrict__ nr,
+                                                  int p, F&& f) {
+  const int cnt = (int)__ldg(v.ncount + p);
+  const uint32_t* lst = v.nbr + p;
+  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
+  int q[B];
+#pragma unroll
+  for (int u = 0; u < B; ++u) q[u] = ldq(u);
+  for (int j0 = 0; j0 < cnt; j0 += B) {
+    uint4 r[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) r[u] = ld_nr(nr, q[u]);
+#pragma unroll
+    for (int u = 0; u < B; ++u) q[u] = ldq(j0 + B + u);
+    f(r, cnt - j0);
+  }
+}
+
 __device__ __forceinline__ void ld_nv(const NV* __restrict__ base, int i, uint4& r, float4& e) {
   asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
       : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w), "=f"(e.x), "=f"(e.y), "=f"(e.z), "=f"(e.w)
@@ -263,10 +286,12 @@ __device__ __forceinline__ void for_each_neighbor_nv(const NbrView& v, const NV*
   }
 }
 
-// Batched visit over the 32-byte particle records: f(q, xq, dq).
+// Batched visit over the 32-byte particle records with the batch handed to
+// f(x[B], d[B], nvalid), nvalid = min(B, cnt - j0); slots past the count
+// hold the particle's own record and are the body's to skip.
 template <int B, class F>
-__device__ __forceinline__ void for_each_neighbor_pd(const NbrView& v, const PD* __restrict__ pd,
-                                                     int p, F&& f) {
+__device__ __forceinline__ void for_each_batch_pd(const NbrView& v, const PD* __restrict__ pd,
+                                                  int p, F&& f) {
   const int cnt = (int)__ldg(v.ncount + p);
   const uint32_t* lst = v.nbr + p;
   auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
@@ -277,14 +302,9 @@ __device__ __forceinline__ void for_each_neighbor_pd(const NbrView& v, const PD*
     float4 x[B], d[B];
 #pragma unroll
     for (int u = 0; u < B; ++u) ld_pd(pd, q[u], x[u], d[u]);
-    int qn[B];
 #pragma unroll
-    for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
-#pragma unroll
-    for (int u = 0; u < B; ++u)
-      if (j0 + u < cnt) f(q[u], x[u], d[u]);
-#pragma unroll
-    for (int u = 0; u < B; ++u) q[u] = qn[u];
+    for (int u = 0; u < B; ++u) q[u] = ldq(j0 + B + u);
+    f(x, d, cnt - j0);
   }
 }
 

@@ -105,6 +105,33 @@ def test_find_all_neighbors_bit_exact(config, steps):
         assert sim.device_errors() == 0
 
 
+def test_find_all_neighbors_bit_exact_with_the_band_open(tmp_path):
+    """A box so long (20,000 along x, 10,000 h) that FP32 rounding of its
+    largest coordinates could move r^2 across the pre-test band: the host
+    then opens the band and every candidate pair is decided by the FP64 test.
+    The buckets must still equal the oracle's."""
+    from sphpc_b200.scenes import config_path
+    text = open(config_path("small_dam")).read().replace("max_x = 48.0", "max_x = 20000.0")
+    assert "max_x = 20000.0" in text
+    ini = tmp_path / "long_box.ini"
+    ini.write_text(text)
+    assert not _lib.load().sphpc_neighbor_pretest_fp32_safe(C.c_double(20000.0), C.c_double(2.0))
+    with Simulation(str(ini)) as sim:
+        sim.step(4)
+        sim.apply_gravity()
+        sim.predict_positions()
+        sim.find_all_neighbors()
+        st = sim.fetch()
+        o = oracle_for(sim, st)
+        o.call("find_all_neighbors")
+        cnt, nbr = sim.neighbor_buckets()
+        ocnt, onbr = o.neighbor_lists()
+        np.testing.assert_array_equal(cnt, ocnt)
+        for i in range(sim.n):
+            np.testing.assert_array_equal(nbr[i, :cnt[i]], onbr[i, :cnt[i]], err_msg=str(i))
+        assert sim.device_errors() == 0
+
+
 def test_neighbor_cap_60_truncates_in_reference_order():
     """A compressed clump where every particle has more than 60 candidates
     within h: buckets are truncated at 60 in the reference's order."""
