@@ -318,18 +318,18 @@ __device__ __forceinline__ int walk_27_cells(const DevParams& P, const NbrView& 
 // Staged neighbour build (FillNeighbors, neighbors.c:217-298): one thread per
 // particle walks its 9 (dz, dy) slot rows in the reference's order (rows of
 // cells cx-1..cx+1 are contiguous slot ranges, cells in dx order, particles
-// in ascending original index).  The candidates of a row are tested eight at
-// a time into a hit mask (masked_row: packed FP32x2 arithmetic of sm_100 on
-// the pair-block positions, no branch or store per candidate), and the hits
-// are appended in slot order to the thread's own column of a shared-memory
-// staging area; the bucket is written out at the end as column entries of
+// in ascending original index), appending every candidate without branches
+// to its own column of a shared-memory staging area -- store the entry,
+// advance the count on a hit; the particle itself is skipped by splitting
+// its own row -- and writes its bucket out at the end as column entries of
 // nbr[60][n] (for each entry index, a warp's 32 consecutive slots are one
 // 128-byte line).  A staged entry is 2 bytes, (row << 12) | offset in the
 // row, with the row starts kept in shared memory, so a thread holds 156
 // bytes of shared memory and the candidate loop only the particle's FP32
-// position: enough blocks stay resident to hide the candidate loads.  A
-// particle with a row of more than 4095 candidates takes the verbatim
-// 27-cell walk.
+// position: enough blocks stay resident to hide the candidate loads.  The
+// candidates of a row are tested two at a time with the packed FP32x2
+// arithmetic of sm_100 (staged_range).  A particle with a row of more than
+// 4095 candidates takes the verbatim 27-cell walk.
 // ---------------------------------------------------------------------------
 constexpr int kStagedBlock = 128;
 constexpr int kRowBits = 12;
@@ -350,82 +350,81 @@ __device__ __forceinline__ bool staged_exact(const DevParams& P, const PD* __res
   return r2 < P.h2d;
 }
 
-// r^2 of the two slots of the pair block at even slot j from particle
-// position (pxx, pyy, pzz) duplicated in both halves: packed FP32x2
-// arithmetic, each half rounded as the scalar form (x_p - x_q, then
-// (dx^2 + dy^2) + dz^2 by fused multiply-adds).
-__device__ __forceinline__ uint64_t pair_r2(const float4* __restrict__ xsa, int j, uint64_t pxx,
-                                            uint64_t pyy, uint64_t pzz) {
-  uint64_t x0, y0, z0;
-  ld_pair(xsa, j, x0, y0, z0);
-  uint64_t d = f2_sub(pxx, x0);
-  uint64_t s = f2_mul(d, d);
-  d = f2_sub(pyy, y0);
-  s = f2_fma(d, d, s);
-  d = f2_sub(pzz, z0);
-  return f2_fma(d, d, s);
+// Test and append of one candidate slot j with FP32 r^2 = r2 (the exact
+// FP64 test decides inside the band): the entry is stored at the thread's
+// next staging slot and the count advances on a hit.
+__device__ __forceinline__ void staged_one(const DevParams& P, const PD* __restrict__ pd, int p,
+                                           int j, float r2, uint32_t entry,
+                                           uint16_t* __restrict__ stg, int& cnt) {
+  bool hit = r2 <= P.bld_h2hi;
+  if (hit && r2 >= P.bld_h2lo) hit = staged_exact(P, pd, p, j);
+  stg[cnt * kStagedBlock] = (uint16_t)entry;
+  cnt += hit ? 1 : 0;
 }
 
-// Tests the slots [b, e) of row r against particle p and appends the hits in
-// slot order, entries (r << kRowBits) | (j - b).  The slots go by groups of
-// eight from the even slot at or below b: four pair blocks (the last block
-// holding a slot of the row is reloaded past the row's end, so every load
-// stays inside the row), their outcomes gathered into an 8-bit hit mask
-// (r^2 <= the band's top) without branches or stores; one check per group,
-// the smallest |r^2 - c| against the band's half width w (c and w its centre
-// and half width, w widened by 2^-10), says whether any of its slots lies in
-// the band [bld_h2lo, bld_h2hi], and only such a group decides those slots by
-// the exact FP64 test.  Slots outside [b, e) and, in p's own row (SELF), p
-// itself are masked out; then the mask's hits go to the thread's staging
-// column.  Returns false once the bucket holds kMaxNeighbors entries.
-template <bool SELF>
-__device__ __forceinline__ bool masked_row(const DevParams& P, const PD* __restrict__ pd,
-                                           const float4* __restrict__ xsa, uint64_t pxx,
-                                           uint64_t pyy, uint64_t pzz, float bc, float bw,
-                                           int p, int r, int b, int e,
-                                           uint16_t* __restrict__ stg, int& cnt) {
+// r^2 of one slot from the FP32 positions (the ragged ends of a range).
+__device__ __forceinline__ float staged_r2(const float4* __restrict__ xsa, int j, float px,
+                                           float py, float pz) {
+  const float4 q = xsa_load(xsa, j);
+  const float fx = px - q.x, fy = py - q.y, fz = pz - q.z;
+  return fx * fx + fy * fy + fz * fz;
+}
+
+// Appends the candidates of slots [ja, jb) of row r (starting at slot rb),
+// entries (r << kRowBits) | (j - rb).  The slots of an even-aligned pair are
+// tested together with packed FP32x2 arithmetic (each lane rounds as the
+// scalar form would: x_p - x_q, then (dx^2 + dy^2) + dz^2 by fused
+// multiply-adds), two pairs per batch while four more entries fit below the
+// cap; an odd first or last slot is tested alone.
+__device__ __forceinline__ void staged_range(const DevParams& P, const PD* __restrict__ pd,
+                                             const float4* __restrict__ xsa, uint64_t pxx,
+                                             uint64_t pyy, uint64_t pzz, float px, float py,
+                                             float pz, int p, int r, int rb, int ja, int jb,
+                                             uint16_t* __restrict__ stg, int& cnt) {
   const uint32_t tag = (uint32_t)r << kRowBits;
-  const int jlast = (e - 1) & ~1;
-  for (int g0 = b & ~1; g0 < e; g0 += 8) {
-    uint32_t hm = 0u;
-    float amin = __int_as_float(0x7f800000);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const uint64_t s = pair_r2(xsa, min(g0 + 2 * u, jlast), pxx, pyy, pzz);
-      const float slo = f2_lo(s), shi = f2_hi(s);
-      if (slo <= P.bld_h2hi) hm |= 1u << (2 * u);
-      if (shi <= P.bld_h2hi) hm |= 2u << (2 * u);
-      amin = fminf(amin, fminf(fabsf(slo - bc), fabsf(shi - bc)));
-    }
-    // the group's slots that belong to [b, e) (and are not p)
-    const int lim = e - g0;
-    uint32_t vm = lim >= 8 ? 0xFFu : (1u << lim) - 1u;
-    if (g0 < b) vm &= ~1u;
-    if (SELF) {
-      const unsigned sp = (unsigned)(p - g0);
-      if (sp < 8u) vm &= ~(1u << sp);
-    }
-    hm &= vm;
-    if (amin <= bw) {
-      // a slot of the group lies in the band: those decide by the FP64 test
-#pragma unroll 1
-      for (int k = 0; k < 8; ++k) {
-        if (!((vm >> k) & 1u)) continue;
-        const int j = g0 + k;
-        const uint64_t s = pair_r2(xsa, j & ~1, pxx, pyy, pzz);
-        const float sj = (j & 1) ? f2_hi(s) : f2_lo(s);
-        if (sj >= P.bld_h2lo && sj <= P.bld_h2hi && !staged_exact(P, pd, p, j))
-          hm &= ~(1u << k);
-      }
-    }
-    while (hm) {
-      const int k = __ffs(hm) - 1;
-      hm &= hm - 1u;
-      stg[cnt * kStagedBlock] = (uint16_t)(tag | (uint32_t)(g0 + k - b));
-      if (++cnt == kMaxNeighbors) return false;
-    }
+  int j = ja;
+  if ((j & 1) && j < jb && cnt < kMaxNeighbors) {
+    staged_one(P, pd, p, j, staged_r2(xsa, j, px, py, pz), tag | (uint32_t)(j - rb), stg, cnt);
+    ++j;
   }
-  return true;
+  for (; j + 4 <= jb && cnt <= kMaxNeighbors - 4; j += 4) {
+    // pair blocks of slots j, j+1 and j+2, j+3
+    uint64_t x0, y0, z0, x1, y1, z1;
+    ld_pair(xsa, j, x0, y0, z0);
+    ld_pair(xsa, j + 2, x1, y1, z1);
+    uint64_t d = f2_sub(pxx, x0);
+    uint64_t s0 = f2_mul(d, d);
+    d = f2_sub(pyy, y0);
+    s0 = f2_fma(d, d, s0);
+    d = f2_sub(pzz, z0);
+    s0 = f2_fma(d, d, s0);
+    d = f2_sub(pxx, x1);
+    uint64_t s1 = f2_mul(d, d);
+    d = f2_sub(pyy, y1);
+    s1 = f2_fma(d, d, s1);
+    d = f2_sub(pzz, z1);
+    s1 = f2_fma(d, d, s1);
+    const uint32_t e = tag | (uint32_t)(j - rb);
+    staged_one(P, pd, p, j, f2_lo(s0), e, stg, cnt);
+    staged_one(P, pd, p, j + 1, f2_hi(s0), e + 1, stg, cnt);
+    staged_one(P, pd, p, j + 2, f2_lo(s1), e + 2, stg, cnt);
+    staged_one(P, pd, p, j + 3, f2_hi(s1), e + 3, stg, cnt);
+  }
+  for (; j + 2 <= jb && cnt <= kMaxNeighbors - 2; j += 2) {
+    uint64_t x0, y0, z0;
+    ld_pair(xsa, j, x0, y0, z0);
+    uint64_t d = f2_sub(pxx, x0);
+    uint64_t s0 = f2_mul(d, d);
+    d = f2_sub(pyy, y0);
+    s0 = f2_fma(d, d, s0);
+    d = f2_sub(pzz, z0);
+    s0 = f2_fma(d, d, s0);
+    const uint32_t e = tag | (uint32_t)(j - rb);
+    staged_one(P, pd, p, j, f2_lo(s0), e, stg, cnt);
+    staged_one(P, pd, p, j + 1, f2_hi(s0), e + 1, stg, cnt);
+  }
+  for (; j < jb && cnt < kMaxNeighbors; ++j)
+    staged_one(P, pd, p, j, staged_r2(xsa, j, px, py, pz), tag | (uint32_t)(j - rb), stg, cnt);
 }
 
 // 9 blocks of 128 threads per SM: 56 registers, no spills (a tighter cap
@@ -470,22 +469,18 @@ __global__ void __launch_bounds__(kStagedBlock, 9)
   if (regular) {
     const float4 xf = xsa_load(xsa, p);
     const uint64_t pxx = f2_dup(xf.x), pyy = f2_dup(xf.y), pzz = f2_dup(xf.z);
-    // centre and half width of the FP64-decided band, the width widened by
-    // 2^-10 so that FP32 rounding of |r^2 - c| cannot leave out a slot of
-    // the band (an open band, bld_h2hi = inf, makes both infinite: every
-    // group is decided exactly)
-    const float bc = 0.5f * P.bld_h2lo + 0.5f * P.bld_h2hi;
-    const float bw = (0.5f * P.bld_h2hi - 0.5f * P.bld_h2lo) * (1.0f + 0x1p-10f);
     for (int r = 0; r < 9 && count < kMaxNeighbors; ++r) {
       const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
       if ((unsigned)z >= (unsigned)P.nz || (unsigned)y >= (unsigned)P.ny) continue;
       const uint32_t rk = (uint32_t)z * P.nxny + (uint32_t)y * (uint32_t)P.nx;
       const int b = rowb[r * kStagedBlock];
       const int e = (int)__ldg(V.cstart + rk + xhi + 1);
-      const bool more =
-          r == 4 ? masked_row<true>(P, pd, xsa, pxx, pyy, pzz, bc, bw, p, r, b, e, stg, count)
-                 : masked_row<false>(P, pd, xsa, pxx, pyy, pzz, bc, bw, p, r, b, e, stg, count);
-      if (!more) break;
+      if (r == 4) {
+        staged_range(P, pd, xsa, pxx, pyy, pzz, xf.x, xf.y, xf.z, p, r, b, b, p, stg, count);
+        staged_range(P, pd, xsa, pxx, pyy, pzz, xf.x, xf.y, xf.z, p, r, b, p + 1, e, stg, count);
+      } else {
+        staged_range(P, pd, xsa, pxx, pyy, pzz, xf.x, xf.y, xf.z, p, r, b, b, e, stg, count);
+      }
     }
     for (int t = 0; t < count; ++t) {
       const uint32_t en = stg[t * kStagedBlock];
