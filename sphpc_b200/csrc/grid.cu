@@ -281,19 +281,25 @@ __device__ __forceinline__ bool is_neighbor(const BuildCtx& c, const PD* __restr
                                             const float4* __restrict__ xsa, int j) {
   const float4 q = xsa_load(xsa, j);
   const float fx = c.xf.x - q.x, fy = c.xf.y - q.y, fz = c.xf.z - q.z;
-  const float r2f = fx * fx + fy * fy + fz * fz;
+  const float r2f = norm2(fx, fy, fz);
   if (r2f < c.h2lo) return true;
   if (r2f > c.h2hi) return false;
   return exact_neighbor(c, pd, j);
 }
 
+// Address of list entry t of particle p in the four-entry blocks nbr4[15][n].
+__device__ __forceinline__ size_t nbr_index(int n, int p, int t) {
+  return (((size_t)(t >> 2) * n + p) << 2) + (t & 3);
+}
+
 // FillNeighbors' 27-cell walk (neighbors.c:247-295) verbatim, for a
 // particle whose neighbour cells are not cx-1..cx+1 (FP64 rounding at a cell
-// face): its bucket goes to out[count * stride]; returns the count.
+// face): its bucket goes to list entries 0..count-1 of p in nbr, the last
+// block's entries past the count are set to p; returns the count.
 __device__ __forceinline__ int walk_27_cells(const DevParams& P, const NbrView& V, const BuildCtx& c,
                                           const PD* __restrict__ pd,
                                           const float4* __restrict__ xsa, int p,
-                                          uint32_t* __restrict__ out, size_t stride) {
+                                          uint32_t* __restrict__ nbr) {
   int count = 0;
   for (int dz = -1; dz <= 1; ++dz)
     for (int dy = -1; dy <= 1; ++dy)
@@ -308,9 +314,10 @@ __device__ __forceinline__ int walk_27_cells(const DevParams& P, const NbrView& 
         const int b = (int)__ldg(V.cstart + key);
         const int e = (int)__ldg(V.cstart + key + 1);
         for (int j = b; j < e && count < kMaxNeighbors; ++j) {
-          if (j != p && is_neighbor(c, pd, xsa, j)) out[(size_t)(count++) * stride] = (uint32_t)j;
+          if (j != p && is_neighbor(c, pd, xsa, j)) nbr[nbr_index(V.n, p, count++)] = (uint32_t)j;
         }
       }
+  for (int t = count; t & 3; ++t) nbr[nbr_index(V.n, p, t)] = (uint32_t)p;
   return count;
 }
 
@@ -321,9 +328,10 @@ __device__ __forceinline__ int walk_27_cells(const DevParams& P, const NbrView& 
 // in ascending original index), appending every candidate without branches
 // to its own column of a shared-memory staging area -- store the entry,
 // advance the count on a hit; the particle itself is skipped by splitting
-// its own row -- and writes its bucket out at the end as column entries of
-// nbr[60][n] (for each entry index, a warp's 32 consecutive slots are one
-// 128-byte line).  A staged entry is 2 bytes, (row << 12) | offset in the
+// its own row -- and writes its bucket out at the end as four-entry blocks
+// of nbr4[15][n] (for each block index, a warp's 32 consecutive slots are
+// four whole 128-byte lines), the last block's entries past the count set to
+// p.  A staged entry is 2 bytes, (row << 12) | offset in the
 // row, with the row starts kept in shared memory, so a thread holds 156
 // bytes of shared memory and the candidate loop only the particle's FP32
 // position: enough blocks stay resident to hide the candidate loads.  The
@@ -367,7 +375,7 @@ __device__ __forceinline__ float staged_r2(const float4* __restrict__ xsa, int j
                                            float py, float pz) {
   const float4 q = xsa_load(xsa, j);
   const float fx = px - q.x, fy = py - q.y, fz = pz - q.z;
-  return fx * fx + fy * fy + fz * fz;
+  return norm2(fx, fy, fz);
 }
 
 // Appends the candidates of slots [ja, jb) of row r (starting at slot rb),
@@ -427,8 +435,9 @@ __device__ __forceinline__ void staged_range(const DevParams& P, const PD* __res
     staged_one(P, pd, p, j, staged_r2(xsa, j, px, py, pz), tag | (uint32_t)(j - rb), stg, cnt);
 }
 
-// 9 blocks of 128 threads per SM: 56 registers, no spills (a tighter cap
-// spills and gains nothing).
+// 9 blocks of 128 threads per SM: 56 registers (8 bytes spilled since the
+// four-entry write-out, no slower at 16.7M particles than without; a tighter
+// cap spills more and gains nothing).
 __global__ void __launch_bounds__(kStagedBlock, 9)
     k_build_staged(const DevParams P, const NbrView V, const PD* __restrict__ pd,
                    const float4* __restrict__ xsa, const uint32_t* __restrict__ cellp,
@@ -439,7 +448,6 @@ __global__ void __launch_bounds__(kStagedBlock, 9)
   if (p >= P.n) return;
   uint16_t* stg = s_stage + threadIdx.x;
   int* rowb = s_rowb + threadIdx.x;
-  const size_t stride = (size_t)P.n;
   BuildCtx c;
   ld_pd(pd, p, c.xp, c.dp);
   c.xs = xstar_d(c.xp.x, c.dp.x);
@@ -482,26 +490,38 @@ __global__ void __launch_bounds__(kStagedBlock, 9)
         staged_range(P, pd, xsa, pxx, pyy, pzz, xf.x, xf.y, xf.z, p, r, b, b, e, stg, count);
       }
     }
-    for (int t = 0; t < count; ++t) {
+    // one 16-byte block of four entries per store; the last block's entries
+    // past the count are p
+    uint4* out = reinterpret_cast<uint4*>(nbr) + p;
+    auto entry = [&](int t) {
       const uint32_t en = stg[t * kStagedBlock];
-      nbr[(size_t)t * stride + p] =
-          (uint32_t)(rowb[(en >> kRowBits) * kStagedBlock] + (int)(en & kRowMax));
-    }
+      return t < count ? (uint32_t)(rowb[(en >> kRowBits) * kStagedBlock] + (int)(en & kRowMax))
+                       : (uint32_t)p;
+    };
+#pragma unroll 1
+    for (int t0 = 0; t0 < count; t0 += 4, out += P.n)
+      *out = make_uint4(entry(t0), entry(t0 + 1), entry(t0 + 2), entry(t0 + 3));
   } else {
     c.xf = xsa_load(xsa, p);
     c.h2lo = P.bld_h2lo;
     c.h2hi = P.bld_h2hi;
     c.h2d = P.h2d;
-    count = walk_27_cells(P, V, c, pd, xsa, p, nbr + p, stride);
+    count = walk_27_cells(P, V, c, pd, xsa, p, nbr);
   }
   ncount[p] = (uint8_t)count;
 }
 
 __global__ void __launch_bounds__(kBlock)
     k_export_buckets(const NbrView V, const uint32_t* __restrict__ ids,
-                     uint32_t* __restrict__ nbr, int32_t* __restrict__ count) {
+                     uint32_t* __restrict__ nbr, int32_t* __restrict__ count,
+                     uint32_t* __restrict__ err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= V.n) return;
+  // the list's last block must hold p past the count (the batched visits
+  // read those entries as the pair (p, p))
+  const int c0 = (int)__ldg(V.ncount + p);
+  for (int t = c0; t & 3; ++t)
+    if (nbr_entry(V, p, t) != (uint32_t)p) atomicOr(err, kErrNbrTail);
   const uint32_t idp = __ldg(ids + p);
   uint32_t* out = nbr + (size_t)idp * kMaxNeighbors;
   int cnt = 0;
@@ -554,8 +574,8 @@ void launch_build_neighbors(const DevParams& P, const NbrView& V, const PD* pd,
 }
 
 void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr, int32_t* count,
-                           cudaStream_t st) {
-  k_export_buckets<<<grid_for(V.n), kBlock, 0, st>>>(V, ids, nbr, count);
+                           uint32_t* err, cudaStream_t st) {
+  k_export_buckets<<<grid_for(V.n), kBlock, 0, st>>>(V, ids, nbr, count, err);
 }
 
 }  // namespace sphpc

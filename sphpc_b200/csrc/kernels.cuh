@@ -51,14 +51,17 @@ void launch_cell_starts(const uint32_t* keys_sorted, int n, uint32_t ncells, uin
                         uint4* gaps, uint32_t* gap_count, uint32_t* err, cudaStream_t st);
 
 // Neighbour build (FillNeighbors, neighbors.c:217-298): per particle, its
-// bucket of neighbour slots nbr[j][p] and its size ncount[p].
+// bucket of neighbour slots (four-entry blocks nbr4[j / 4][p], entries past
+// the count in the last block set to p) and its size ncount[p].
 void launch_build_neighbors(const DevParams& P, const NbrView& V, const PD* pd,
                             const float4* xsa, const uint32_t* cellp, uint32_t* nbr,
                             uint8_t* ncount, cudaStream_t st);
 
-// Export the buckets in original-index space: nbr[id*60 + j], count[id].
+// Export the buckets in original-index space: nbr[id*60 + j], count[id];
+// raises kErrNbrTail in err if a list's last block does not hold p past the
+// count.
 void launch_export_buckets(const NbrView& V, const uint32_t* ids, uint32_t* nbr, int32_t* count,
-                           cudaStream_t st);
+                           uint32_t* err, cudaStream_t st);
 
 // ---- PBF passes (pbf.cu) ----
 

@@ -45,10 +45,10 @@ __device__ __forceinline__ void ld_rw(const PD* base, int i, float4& x, float4& 
 // exact, its conversion to FP32 rounds like any FP32 difference.
 __device__ __forceinline__ Pair pair_nr(const DevParams& P, const uint4 a, const uint4 b) {
   Pair g;
-  g.dx = (float)(int)(a.x - b.x) * P.fx_inv;
-  g.dy = (float)(int)(a.y - b.y) * P.fx_inv;
-  g.dz = (float)(int)(a.z - b.z) * P.fx_inv;
-  g.r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
+  g.dx = __fmul_rn((float)(int)(a.x - b.x), P.fx_inv);
+  g.dy = __fmul_rn((float)(int)(a.y - b.y), P.fx_inv);
+  g.dz = __fmul_rn((float)(int)(a.z - b.z), P.fx_inv);
+  g.r2 = norm2(g.dx, g.dy, g.dz);
   return g;
 }
 
@@ -58,7 +58,7 @@ __device__ __forceinline__ Pair pair_geom(const float4 xp, const float4 dp, cons
   g.dx = (xp.x - xq.x) + (dp.x - dq.x);
   g.dy = (xp.y - xq.y) + (dp.y - dq.y);
   g.dz = (xp.z - xq.z) + (dp.z - dq.z);
-  g.r2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
+  g.r2 = norm2(g.dx, g.dy, g.dz);
   return g;
 }
 
@@ -66,16 +66,21 @@ __device__ __forceinline__ Pair pair_geom(const float4 xp, const float4 dp, cons
 __device__ __forceinline__ void floored_r(const DevParams& P, float r2, float& r, float& rinv) {
   const float r2c = fmaxf(r2, P.rmin * P.rmin);
   rinv = rsqrtf(r2c);
-  r = r2c * rinv;
+  r = __fmul_rn(r2c, rinv);
 }
 
 // The same in fixed-point units (r2f = |d|^2 of the record difference):
-// r_f = r 2^k and rinv_f = 2^-k / r, so the loops need no rescaling of r^2.
+// r2c = max(r2f, r_min^2) and rinv_f = 2^-k / r, so the loops need no
+// rescaling of r^2; r_f = r 2^k is r2c rinv (fx_r), and h_f - r_f, floored at
+// 0, one fused multiply-add (fx_hm).
 __device__ __forceinline__ void floored_r_fx(const DevParams& P, float r2f, float& r2c,
-                                             float& r, float& rinv) {
+                                             float& rinv) {
   r2c = fmaxf(r2f, P.rmin2_fx);
   rinv = rsqrtf(r2c);
-  r = r2c * rinv;
+}
+__device__ __forceinline__ float fx_r(float r2c, float rinv) { return __fmul_rn(r2c, rinv); }
+__device__ __forceinline__ float fx_hm(const DevParams& P, float r2c, float rinv) {
+  return fmaxf(fmaf(-r2c, rinv, P.h_fx), 0.0f);
 }
 
 // 1/x by the hardware's approximate reciprocal (PTX rcp.approx.ftz.f32, at
@@ -140,28 +145,34 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
         const float fx = (float)(int)(rp.x - rq[u].x);
         const float fy = (float)(int)(rp.y - rq[u].y);
         const float fz = (float)(int)(rp.z - rq[u].z);
-        const float r2f = fx * fx + fy * fy + fz * fz;
+        const float r2f = norm2(fx, fy, fz);
         if (MODE != 2) {
           float t = fmaxf(fmaf(-P.fx_inv2, r2f, P.h2), 0.0f);
           t = u < nvalid ? t : 0.0f;
-          t3[u] = t * t * t;
+          t3[u] = t;
         }
         if (MODE != 1) {
           // in fixed-point units: c_f = (h_f - r_f)^2 / r_f = 2^k c
-          float r2c, r, rinv;
-          floored_r_fx(P, r2f, r2c, r, rinv);
-          const float hm = fmaxf(P.h_fx - r, 0.0f);
-          const float c = hm * hm * rinv;
+          float r2c, rinv;
+          floored_r_fx(P, r2f, r2c, rinv);
+          const float hm = fx_hm(P, r2c, rinv);
+          const float c = __fmul_rn(__fmul_rn(hm, hm), rinv);
           // |c d|^2 = c^2 |d|^2: three fused accumulations and one for the norm
           sgx = fmaf(c, fx, sgx);
           sgy = fmaf(c, fy, sgy);
           sgz = fmaf(c, fz, sgz);
-          sC = fmaf(c * c, r2f, sC);
+          sC = fmaf(__fmul_rn(c, c), r2f, sC);
         }
       }
       if (MODE != 2) {
-        static_assert(kNbrBatch == 4, "pairwise batch sum of four terms");
-        const float y = ((t3[0] + t3[1]) + (t3[2] + t3[3])) - comp;
+        static_assert(kNbrBatch == 4, "batch sum of four terms");
+        // t0^3 + t1^3 + t2^3 + t3^3 as a chain of fused multiply-adds
+        const float* t = t3;
+        const float yb = fmaf(__fmul_rn(t[0], t[0]), t[0],
+                              fmaf(__fmul_rn(t[1], t[1]), t[1],
+                                   fmaf(__fmul_rn(t[2], t[2]), t[2],
+                                        __fmul_rn(__fmul_rn(t[3], t[3]), t[3]))));
+        const float y = yb - comp;
         const float s = st + y;
         comp = (s - st) - y;
         st = s;
@@ -177,7 +188,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksDensity)
       // ComputeLambda's constraint (particles.c:616-617) in FP64
       const float C = (float)fmax(__ddiv_rn((double)rho, P.rho0_d) - 1.0, 0.0);
       const float g = P.DWn_m * P.fx_inv2;  // gradient scale (2^-2k is exact)
-      sC += sgx * sgx + sgy * sgy + sgz * sgz;
+      sC = __fadd_rn(sC, norm2(sgx, sgy, sgz));
       sC *= (g * g) * P.inv_rho0_sq;
       const float lam = -C / (sC + P.lambda_eps);
       if (a.nr_out) a.nr_out[p] = make_uint4(rp.x, rp.y, rp.z, __float_as_uint(lam));
@@ -227,15 +238,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksFeatures)
         if (u < nvalid) {
           const Pair g = pair_geom(xp, dp, xq[u], dq[u]);
           const float t = fmaxf(P.h2 - g.r2, 0.0f);
-          yb += t * t * t;
+          yb = fmaf(__fmul_rn(t, t), t, yb);
           float r, rinv;
           floored_r(P, g.r2, r, rinv);
           const float hm = fmaxf(P.h - r, 0.0f);
-          const float c = hm * hm * rinv;
+          const float c = __fmul_rn(__fmul_rn(hm, hm), rinv);
           sgx = fmaf(c, g.dx, sgx);
           sgy = fmaf(c, g.dy, sgy);
           sgz = fmaf(c, g.dz, sgz);
-          sC = fmaf(c * c, g.r2, sC);
+          sC = fmaf(__fmul_rn(c, c), g.r2, sC);
           ox -= g.dx;
           oy -= g.dy;
           oz -= g.dz;
@@ -263,7 +274,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksFeatures)
     a.rho[p] = rho;
     const float C = (float)fmax(__ddiv_rn((double)rho, P.rho0_d) - 1.0, 0.0);
     const float s_pairs = sC * P.inv_rho0_sq;
-    sC += sgx * sgx + sgy * sgy + sgz * sgz;
+    sC = __fadd_rn(sC, norm2(sgx, sgy, sgz));
     sC *= P.inv_rho0_sq;
     const float lam = -C / (sC + P.lambda_eps);
     const double xs = xstar_d(xp.x, dp.x), ys = xstar_d(xp.y, dp.y), zs = xstar_d(xp.z, dp.z);
@@ -271,7 +282,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksFeatures)
     err = fmax((double)rho / (double)P.rho0 - 1.0, 0.0);
     if (p < limit) {
       const float inv_h = 1.0f / P.h;
-      const float s_self = (sgx * sgx + sgy * sgy + sgz * sgz) * P.inv_rho0_sq;
+      const float s_self = __fmul_rn(norm2(sgx, sgy, sgz), P.inv_rho0_sq);
       const float inv_cnt = cnt > 0 ? 1.0f / (float)cnt : 0.0f;
       const float sc = inv_h * inv_cnt;
       float sdf = 4.0f;
@@ -287,7 +298,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksFeatures)
                fmin(fmin(ys - P.bmin[1], P.bmax[1] - ys), fmin(zs - P.bmin[2], P.bmax[2] - zs)));
       const float fw = fminf(fmaxf((float)(wall / P.hd), 0.0f), 4.0f);
       const float vg = (P.gaxis == 0 ? dp.x : (P.gaxis == 1 ? dp.y : dp.z)) * inv_h;
-      const float f[16] = {rho * P.inv_rho0 - 1.0f, C, lam, s_pairs, s_self, (float)cnt,
+      const float f[16] = {fmaf(rho, P.inv_rho0, -1.0f), C, lam, s_pairs, s_self, (float)cnt,
                            ox * sc, oy * sc, oz * sc, ux * sc, uy * sc, uz * sc,
                            sdf, sqrtf(rmin2) * inv_h, fw, vg};
       if (RAW) {
@@ -319,7 +330,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksFeatures)
 __global__ void k_accum_lambda(const uint4* __restrict__ rec, float s, float* __restrict__ target,
                                int limit) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < limit) target[p] += s * __uint_as_float(rec[p].w);
+  if (p < limit) target[p] = fmaf(s, __uint_as_float(rec[p].w), target[p]);
 }
 
 template <int MODE, int SCORR_N, bool SDF>
@@ -341,9 +352,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksPosition)
     const float fy = (float)(int)(rp.y - rq.y);
     const float fz = (float)(int)(rp.z - rq.z);
     // in fixed-point units: c_f = s (h_f - r_f)^2 / r_f = 2^k c
-    float r2c, r, rinv;
-    floored_r_fx(P, fx * fx + fy * fy + fz * fz, r2c, r, rinv);
-    const float hm = fmaxf(P.h_fx - r, 0.0f);
+    float r2c, rinv;
+    floored_r_fx(P, norm2(fx, fy, fz), r2c, rinv);
+    const float hm = fx_hm(P, r2c, rinv);
     float s = lp + nr_w(rq);
     if (SCORR_N != 0) {
       // W(r) / W(dq) = u^3 with u = (h^2 - r^2) / (h^2 - dq^2), u <= 1.05
@@ -355,11 +366,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksPosition)
       } else {
         const float ratio = u * u * u;
         float sc = -P.scorr_k;
-        for (int e = 0; e < P.scorr_n; ++e) sc *= ratio;
-        s += sc;
+        for (int e = 0; e < P.scorr_n; ++e) sc = __fmul_rn(sc, ratio);
+        s = __fadd_rn(s, sc);
       }
     }
-    const float c = s * hm * hm * rinv;
+    const float c = __fmul_rn(__fmul_rn(__fmul_rn(s, hm), hm), rinv);
     ax = fmaf(c, fx, ax);
     ay = fmaf(c, fy, ay);
     az = fmaf(c, fz, az);
@@ -438,10 +449,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksColor)
     const float fy = (float)(int)(rp.y - rq.y);
     const float fz = (float)(int)(rp.z - rq.z);
     // r and 1/r in fixed-point units (their product is unit-free)
-    float r2c, r, rinv;
-    floored_r_fx(P, fx * fx + fy * fy + fz * fz, r2c, r, rinv);
+    float r2c, rinv;
+    floored_r_fx(P, norm2(fx, fy, fz), r2c, rinv);
     const float t = fmaxf(fmaf(-P.fx_inv2, r2c, P.h2), 0.0f);
-    const float c = t * t * r * (rinv * rcp_fast(nr_w(rq)));
+    const float c = __fmul_rn(__fmul_rn(__fmul_rn(t, t), fx_r(r2c, rinv)),
+                              __fmul_rn(rinv, rcp_fast(nr_w(rq))));
     cx = fmaf(c, fx, cx);
     cy = fmaf(c, fy, cy);
     cz = fmaf(c, fz, cz);
@@ -486,7 +498,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
     const float dx = (float)(int)(recp.x - rq.x);
     const float dy = (float)(int)(recp.y - rq.y);
     const float dz = (float)(int)(recp.z - rq.z);
-    const float r2 = (dx * dx + dy * dy + dz * dz) * P.fx_inv2;
+    const float r2 = __fmul_rn(norm2(dx, dy, dz), P.fx_inv2);
     float r, rinv;
     floored_r(P, r2, r, rinv);
     const float coh = kcoh_fx * cohesion_unnormed(P, r, h6_64) * rinv;
@@ -497,9 +509,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksTension)
   });
   float4 v = a.vel[p];
   const float s = P.dt / rp;
-  v.x += s * fx;
-  v.y += s * fy;
-  v.z += s * fz;
+  v.x = fmaf(s, fx, v.x);
+  v.y = fmaf(s, fy, v.y);
+  v.z = fmaf(s, fz, v.z);
   a.vel[p] = v;
   if (a.nv_out) st_nv(a.nv_out, p, recp, v);
 }
@@ -517,9 +529,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksXsph)
   for_each_neighbor_nv<kNbrBatch, true>(V, a.nv, p, [&](int, const uint4 rq, const float4 vq) {
     const Pair g = pair_nr(P, rp, rq);
     // particles.c:439 evaluates x^2 + y^2 * z^2 (kept unless xsph_exact)
-    const float rr = P.xsph_exact ? g.r2 : g.dx * g.dx + g.dy * g.dy * g.dz * g.dz;
+    const float rr =
+        P.xsph_exact ? g.r2
+                     : fmaf(g.dx, g.dx, __fmul_rn(__fmul_rn(__fmul_rn(g.dy, g.dy), g.dz), g.dz));
     const float t = fmaxf(P.h2 - rr, 0.0f);
-    const float w = t * t * t * rcp_fast(nr_w(rq));
+    const float w = __fmul_rn(__fmul_rn(__fmul_rn(t, t), t), rcp_fast(nr_w(rq)));
     sx = fmaf(vq.x - vp.x, w, sx);
     sy = fmaf(vq.y - vp.y, w, sy);
     sz = fmaf(vq.z - vp.z, w, sz);
@@ -556,21 +570,21 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksVorticity)
     const float dx = (float)(int)(rp.x - rq.x);
     const float dy = (float)(int)(rp.y - rq.y);
     const float dz = (float)(int)(rp.z - rq.z);
-    float r2c, r, rinv;
-    floored_r_fx(P, dx * dx + dy * dy + dz * dz, r2c, r, rinv);
-    const float hm = fmaxf(P.h_fx - r, 0.0f);
-    const float c = hm * hm * rinv;
-    const float gx = c * dx, gy = c * dy, gz = c * dz;
+    float r2c, rinv;
+    floored_r_fx(P, norm2(dx, dy, dz), r2c, rinv);
+    const float hm = fx_hm(P, r2c, rinv);
+    const float c = __fmul_rn(__fmul_rn(hm, hm), rinv);
+    const float gx = __fmul_rn(c, dx), gy = __fmul_rn(c, dy), gz = __fmul_rn(c, dz);
     const float ux = vq.x - vp.x, uy = vq.y - vp.y, uz = vq.z - vp.z;
-    wx += uy * gz - uz * gy;
-    wy += uz * gx - ux * gz;
-    wz += ux * gy - uy * gx;
+    wx = __fadd_rn(wx, fmaf(uy, gz, -__fmul_rn(uz, gy)));
+    wy = __fadd_rn(wy, fmaf(uz, gx, -__fmul_rn(ux, gz)));
+    wz = __fadd_rn(wz, fmaf(ux, gy, -__fmul_rn(uy, gx)));
   });
   const float sw = P.DWn * P.fx_inv2;
   wx *= sw;
   wy *= sw;
   wz *= sw;
-  const float wm = sqrtf(wx * wx + wy * wy + wz * wz);
+  const float wm = sqrtf(norm2(wx, wy, wz));
   a.omega[p] = make_float4(wx, wy, wz, wm);
   if (a.nr_out) a.nr_out[p] = make_uint4(rp.x, rp.y, rp.z, __float_as_uint(wm));
 }
@@ -590,11 +604,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksConfinement)
     const float dx = (float)(int)(rp.x - rq.x);
     const float dy = (float)(int)(rp.y - rq.y);
     const float dz = (float)(int)(rp.z - rq.z);
-    float r2c, r, rinv;
-    floored_r_fx(P, dx * dx + dy * dy + dz * dz, r2c, r, rinv);
-    const float hm = fmaxf(P.h_fx - r, 0.0f);
+    float r2c, rinv;
+    floored_r_fx(P, norm2(dx, dy, dz), r2c, rinv);
+    const float hm = fx_hm(P, r2c, rinv);
     const float wq = OW ? nr_w(rq) : __ldg(a.omega + q).w;
-    const float c = hm * hm * rinv * wq;
+    const float c = __fmul_rn(__fmul_rn(__fmul_rn(hm, hm), rinv), wq);
     ex = fmaf(c, dx, ex);
     ey = fmaf(c, dy, ey);
     ez = fmaf(c, dz, ez);
@@ -603,14 +617,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksConfinement)
   ex *= se;
   ey *= se;
   ez *= se;
-  const float em = fmaxf(sqrtf(ex * ex + ey * ey + ez * ez), P.rmin);
+  const float em = fmaxf(sqrtf(norm2(ex, ey, ez)), P.rmin);
   const float nx = ex / em, ny = ey / em, nz = ez / em;
   const float4 w = __ldg(a.omega + p);
   const float s = P.dt * P.vort_eps / P.m;
   float4 v = a.vel[p];
-  v.x += s * (ny * w.z - nz * w.y);
-  v.y += s * (nz * w.x - nx * w.z);
-  v.z += s * (nx * w.y - ny * w.x);
+  v.x = fmaf(s, fmaf(ny, w.z, -__fmul_rn(nz, w.y)), v.x);
+  v.y = fmaf(s, fmaf(nz, w.x, -__fmul_rn(nx, w.z)), v.y);
+  v.z = fmaf(s, fmaf(nx, w.y, -__fmul_rn(ny, w.x)), v.z);
   a.vel[p] = v;
   if (a.write_pos) {
     float4 xp, dp;

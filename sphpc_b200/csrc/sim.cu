@@ -1333,7 +1333,7 @@ int sphpc_get_neighbor_buckets(const struct Particles* particles, unsigned int* 
     dfree(d_nbr);
     return rc;
   }
-  launch_export_buckets(s->view(), s->ids, d_nbr, d_cnt, s->stream);
+  launch_export_buckets(s->view(), s->ids, d_nbr, d_cnt, s->err(), s->stream);
   cudaError_t e = cudaMemcpyAsync(indices, d_nbr, sizeof(uint32_t) * s->n * kMaxNeighbors,
                                   cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess)

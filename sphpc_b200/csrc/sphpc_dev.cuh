@@ -20,9 +20,11 @@
 //   ids[n]   u32     original particle index of each slot
 //   cellp[n] u32     packed grid cell (cx | cy<<bx | cz<<(bx+by)) of x* at
 //                    neighbour-build time
-//   nbr[60][n] u32   neighbour slots of every particle in the reference's
-//                    bucket order (column j of all particles contiguous, so a
-//                    warp reads one 128-byte line per neighbour index)
+//   nbr4[15][n] uint4  neighbour slots of every particle in the reference's
+//                    bucket order, four per block (block b of all particles
+//                    contiguous, so a warp reads four 128-byte lines per
+//                    block); the last block's entries past the count are p
+//                    (nbr_entry, nbr_block)
 //   ncount[n] u8     bucket sizes
 //   cstart[C+1] u32  start slot of every cell (lower bound), cstart[C] = n
 //
@@ -104,11 +106,20 @@ __device__ __forceinline__ uint4 ld_nr(const uint4* __restrict__ base, int i) {
 
 __device__ __forceinline__ float nr_w(const uint4 r) { return __uint_as_float(r.w); }
 
+// |(x, y, z)|^2 as fma(z, z, fma(y, y, x x)).  The neighbour sums spell out
+// every fused multiply-add (fmaf) and every product or sum that must not be
+// fused (__fmul_rn, __fadd_rn), so their rounding is the same in every build
+// of the library, whatever contractions the compiler would choose.
+__device__ __forceinline__ float norm2(float x, float y, float z) {
+  return fmaf(z, z, fmaf(y, y, __fmul_rn(x, x)));
+}
+
 // Error bits raised by kernels (host reads them back).
 enum : uint32_t {
   kErrSortSpin = 1u << 1,          // radix-sort look-back wait gave up
   kErrCellRange = 1u << 2,         // a particle hashed outside the grid
   kErrScanSpin = 1u << 3,
+  kErrNbrTail = 1u << 5,           // a list block's entries past the count are not p
 };
 
 struct DevParams {
@@ -165,7 +176,7 @@ struct DevParams {
 
 // View of the per-step neighbour structure.
 struct NbrView {
-  const uint32_t* __restrict__ nbr;     // [kMaxNeighbors][n]
+  const uint32_t* __restrict__ nbr;     // [kMaxNeighbors / 4][n] blocks of 4 entries
   const uint8_t* __restrict__ ncount;   // [n]
   const uint32_t* __restrict__ cstart;  // [C+1]
   int n;
@@ -182,45 +193,55 @@ __device__ __forceinline__ void unpack_cell(const NbrView& v, uint32_t cp, int& 
   cz = (int)(cp >> (v.bx + v.by));
 }
 
+// Neighbour lists, nbr4[15][n] (uint4): block b of particle p holds its list
+// entries 4b .. 4b+3 (column b of all particles contiguous, so a warp reads
+// four whole 128-byte lines per block index); the entries of the last block
+// past the count hold p itself.  Entry j of particle p:
+__device__ __forceinline__ uint32_t nbr_entry(const NbrView& v, int p, int j) {
+  return __ldg(v.nbr + (((size_t)(j >> 2) * v.n + p) << 2) + (j & 3));
+}
+__device__ __forceinline__ uint4 nbr_block(const NbrView& v, int p, int b) {
+  return __ldg(reinterpret_cast<const uint4*>(v.nbr) + (size_t)b * v.n + p);
+}
+
 // Visits the neighbour slots of particle p in the reference's bucket order
 // (FillNeighbors, neighbors.c:247-295: dz, dy, dx, then ascending sorted
 // index), as stored by the neighbour build.
 template <class F>
 __device__ __forceinline__ void for_each_neighbor(const NbrView& v, int p, F&& f) {
   const int cnt = (int)__ldg(v.ncount + p);
-  const uint32_t* lst = v.nbr + p;
 #pragma unroll 2
-  for (int j = 0; j < cnt; ++j) f((int)__ldg(lst + (size_t)j * v.n));
+  for (int j = 0; j < cnt; ++j) f((int)nbr_entry(v, p, j));
 }
 
-// The same visit with each neighbour's 16-byte record loaded for f(q, rq):
-// list entries and records are fetched in batches of B, and the list
-// entries of the next batch are loaded before the bodies of this one run, so
-// a batch waits only for its record gathers (the list read from HBM overlaps
-// the previous batch).  Batch slots past the count load the particle's own
-// record and are skipped, or, with kPadSlots, visited as the pair (p, p)
-// (for bodies whose every term carries the pair difference, which is 0).
+// The batched visits below take a batch of four list entries per 128-bit
+// load (one block) and load the next block before the bodies of this batch
+// run, so a batch waits only for its record gathers (the list read from HBM
+// overlaps the previous batch).  The entries of the last block past the count
+// are p: those slots load the particle's own record and are skipped, or, with
+// kPadSlots, visited as the pair (p, p) (for bodies whose every term carries
+// the pair difference, which is 0).
+#define SPHPC_NBR_BATCH_HEAD                                      \
+  static_assert(B == 4, "a batch is one four-entry list block"); \
+  const int cnt = (int)__ldg(v.ncount + p);                      \
+  uint4 blk = cnt > 0 ? nbr_block(v, p, 0) : make_uint4(p, p, p, p)
+#define SPHPC_NBR_BATCH_NEXT(j0)                                                         \
+  const int q[4] = {(int)blk.x, (int)blk.y, (int)blk.z, (int)blk.w};                    \
+  if ((j0) + 4 < cnt) blk = nbr_block(v, p, ((j0) >> 2) + 1)
+
+// Each neighbour's 16-byte record loaded for f(q, rq).
 template <int B, bool kPadSlots = false, class F>
 __device__ __forceinline__ void for_each_neighbor_nr(const NbrView& v, const uint4* __restrict__ nr,
                                                      int p, F&& f) {
-  const int cnt = (int)__ldg(v.ncount + p);
-  const uint32_t* lst = v.nbr + p;
-  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
-  int q[B];
+  SPHPC_NBR_BATCH_HEAD;
+  for (int j0 = 0; j0 < cnt; j0 += 4) {
+    SPHPC_NBR_BATCH_NEXT(j0);
+    uint4 r[4];
 #pragma unroll
-  for (int u = 0; u < B; ++u) q[u] = ldq(u);
-  for (int j0 = 0; j0 < cnt; j0 += B) {
-    uint4 r[B];
+    for (int u = 0; u < 4; ++u) r[u] = ld_nr(nr, q[u]);
 #pragma unroll
-    for (int u = 0; u < B; ++u) r[u] = ld_nr(nr, q[u]);
-    int qn[B];
-#pragma unroll
-    for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
-#pragma unroll
-    for (int u = 0; u < B; ++u)
+    for (int u = 0; u < 4; ++u)
       if (kPadSlots || j0 + u < cnt) f(q[u], r[u]);
-#pragma unroll
-    for (int u = 0; u < B; ++u) q[u] = qn[u];
   }
 }
 
@@ -231,18 +252,12 @@ __device__ __forceinline__ void for_each_neighbor_nr(const NbrView& v, const uin
 template <int B, class F>
 __device__ __forceinline__ void for_each_batch_nr(const NbrView& v, const uint4* __restrict__ nr,
                                                   int p, F&& f) {
-  const int cnt = (int)__ldg(v.ncount + p);
-  const uint32_t* lst = v.nbr + p;
-  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
-  int q[B];
+  SPHPC_NBR_BATCH_HEAD;
+  for (int j0 = 0; j0 < cnt; j0 += 4) {
+    SPHPC_NBR_BATCH_NEXT(j0);
+    uint4 r[4];
 #pragma unroll
-  for (int u = 0; u < B; ++u) q[u] = ldq(u);
-  for (int j0 = 0; j0 < cnt; j0 += B) {
-    uint4 r[B];
-#pragma unroll
-    for (int u = 0; u < B; ++u) r[u] = ld_nr(nr, q[u]);
-#pragma unroll
-    for (int u = 0; u < B; ++u) q[u] = ldq(j0 + B + u);
+    for (int u = 0; u < 4; ++u) r[u] = ld_nr(nr, q[u]);
     f(r, cnt - j0);
   }
 }
@@ -264,25 +279,16 @@ __device__ __forceinline__ void st_nv(NV* base, int i, const uint4 r, const floa
 template <int B, bool kPadSlots = false, class F>
 __device__ __forceinline__ void for_each_neighbor_nv(const NbrView& v, const NV* __restrict__ nv,
                                                      int p, F&& f) {
-  const int cnt = (int)__ldg(v.ncount + p);
-  const uint32_t* lst = v.nbr + p;
-  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
-  int q[B];
+  SPHPC_NBR_BATCH_HEAD;
+  for (int j0 = 0; j0 < cnt; j0 += 4) {
+    SPHPC_NBR_BATCH_NEXT(j0);
+    uint4 r[4];
+    float4 e[4];
 #pragma unroll
-  for (int u = 0; u < B; ++u) q[u] = ldq(u);
-  for (int j0 = 0; j0 < cnt; j0 += B) {
-    uint4 r[B];
-    float4 e[B];
+    for (int u = 0; u < 4; ++u) ld_nv(nv, q[u], r[u], e[u]);
 #pragma unroll
-    for (int u = 0; u < B; ++u) ld_nv(nv, q[u], r[u], e[u]);
-    int qn[B];
-#pragma unroll
-    for (int u = 0; u < B; ++u) qn[u] = ldq(j0 + B + u);
-#pragma unroll
-    for (int u = 0; u < B; ++u)
+    for (int u = 0; u < 4; ++u)
       if (kPadSlots || j0 + u < cnt) f(q[u], r[u], e[u]);
-#pragma unroll
-    for (int u = 0; u < B; ++u) q[u] = qn[u];
   }
 }
 
@@ -292,21 +298,18 @@ __device__ __forceinline__ void for_each_neighbor_nv(const NbrView& v, const NV*
 template <int B, class F>
 __device__ __forceinline__ void for_each_batch_pd(const NbrView& v, const PD* __restrict__ pd,
                                                   int p, F&& f) {
-  const int cnt = (int)__ldg(v.ncount + p);
-  const uint32_t* lst = v.nbr + p;
-  auto ldq = [&](int j) { return j < cnt ? (int)__ldg(lst + (size_t)j * v.n) : p; };
-  int q[B];
+  SPHPC_NBR_BATCH_HEAD;
+  for (int j0 = 0; j0 < cnt; j0 += 4) {
+    SPHPC_NBR_BATCH_NEXT(j0);
+    float4 x[4], d[4];
 #pragma unroll
-  for (int u = 0; u < B; ++u) q[u] = ldq(u);
-  for (int j0 = 0; j0 < cnt; j0 += B) {
-    float4 x[B], d[B];
-#pragma unroll
-    for (int u = 0; u < B; ++u) ld_pd(pd, q[u], x[u], d[u]);
-#pragma unroll
-    for (int u = 0; u < B; ++u) q[u] = ldq(j0 + B + u);
+    for (int u = 0; u < 4; ++u) ld_pd(pd, q[u], x[u], d[u]);
     f(x, d, cnt - j0);
   }
 }
+
+#undef SPHPC_NBR_BATCH_HEAD
+#undef SPHPC_NBR_BATCH_NEXT
 
 // ---------------------------------------------------------------------------
 // Canonical double predicted position and the reference's box clamp.
