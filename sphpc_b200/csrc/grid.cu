@@ -370,6 +370,31 @@ __device__ __forceinline__ void staged_one(const DevParams& P, const PD* __restr
   cnt += hit ? 1 : 0;
 }
 
+// Test and append of the four candidates j .. j+3 with FP32 r^2 = r2[u]:
+// one branch for the group, taken only when a candidate lies in the band
+// (the exact FP64 test then decides those), then four branch-free appends.
+__device__ __forceinline__ void staged_four(const DevParams& P, const PD* __restrict__ pd, int p,
+                                            int j, const float (&r2)[4], uint32_t entry,
+                                            uint16_t* __restrict__ stg, int& cnt) {
+  bool hit[4];
+  bool band = false;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    hit[u] = r2[u] <= P.bld_h2hi;
+    band |= hit[u] && r2[u] >= P.bld_h2lo;
+  }
+  if (band) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (hit[u] && r2[u] >= P.bld_h2lo) hit[u] = staged_exact(P, pd, p, j + u);
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    stg[cnt * kStagedBlock] = (uint16_t)(entry + u);
+    cnt += hit[u] ? 1 : 0;
+  }
+}
+
 // r^2 of one slot from the FP32 positions (the ragged ends of a range).
 __device__ __forceinline__ float staged_r2(const float4* __restrict__ xsa, int j, float px,
                                            float py, float pz) {
@@ -412,11 +437,8 @@ __device__ __forceinline__ void staged_range(const DevParams& P, const PD* __res
     s1 = f2_fma(d, d, s1);
     d = f2_sub(pzz, z1);
     s1 = f2_fma(d, d, s1);
-    const uint32_t e = tag | (uint32_t)(j - rb);
-    staged_one(P, pd, p, j, f2_lo(s0), e, stg, cnt);
-    staged_one(P, pd, p, j + 1, f2_hi(s0), e + 1, stg, cnt);
-    staged_one(P, pd, p, j + 2, f2_lo(s1), e + 2, stg, cnt);
-    staged_one(P, pd, p, j + 3, f2_hi(s1), e + 3, stg, cnt);
+    const float r2[4] = {f2_lo(s0), f2_hi(s0), f2_lo(s1), f2_hi(s1)};
+    staged_four(P, pd, p, j, r2, tag | (uint32_t)(j - rb), stg, cnt);
   }
   for (; j + 2 <= jb && cnt <= kMaxNeighbors - 2; j += 2) {
     uint64_t x0, y0, z0;
